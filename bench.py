@@ -1,0 +1,393 @@
+"""Benchmark: histories/s of a 100-beamlet 6 MV Dij on a 128^3 CT-like phantom.
+
+Workload (the batched-Dij configuration the headline metric is quoted on):
+a 128^3 phantom at 2.5 mm (water plus 6-12 seeded random ellipsoids of density
+U(0.2, 1.9)), a 10x10 lattice of 5x5 mm beamlets of the Ali-Rogers Varian 6 MV
+spectrum at SAD 100 cm, per-beamlet history counts log-uniform in 1e4-1e6
+(seeded; ~2e7 histories in total), 10 batches, full electron transport with
+Goudsmit-Saunderson multiple scattering, truncation 1e-3.  One step is one whole
+Dij: transport, fold, finalize, truncation and CSC assembly.
+
+``python bench.py [--gpus N --steps K --warmup W] [--impl b200|reference]``
+prints one JSON line.  ``value`` is histories/s over the device-resident step
+(CUDA events on the stream the engine runs on, max over ranks); ``e2e`` is the
+same metric through ``B200Engine.run_dij`` from host data, with the grid, table
+and GS uploads and the CSC readback inside the timed region.  Under torchrun each
+rank computes its own Dij (weak scaling, no data-path collective); the books and
+timings meet in one all-reduce after the timed region.
+
+``--impl reference`` times the CPU oracle (the C restatement of the reference's
+transport, all host threads) on bounded samples of the same workload.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "histories/s and s per 100-beamlet Dij at 2% sigma: plain MC vs MC+denoiser"
+N_BATCHES = 10
+SEED = 20260726
+
+
+def workload(rank: int = 0):
+    from pyradmc_b200 import phantoms
+    from pyradmc_b200.model import AnalyticWaterTables
+
+    grid = phantoms.ellipsoid_phantom(seed=SEED)
+    source = phantoms.beamlet_fan(grid)
+    counts = phantoms.log_uniform_counts(source.n_beamlets, n_batches=N_BATCHES, seed=SEED)
+    xs = AnalyticWaterTables(geometry_densities=grid.max_density_by_material())
+    return grid, xs, source, counts
+
+
+def config_dict(counts, l2_note):
+    return {
+        "workload": "dij_128cube_100beamlets_6MV",
+        "phantom": "128^3 at 2.5 mm, water + seeded ellipsoids rho U(0.2,1.9)",
+        "beamlets": 100,
+        "beamlet_mm": 5,
+        "spectrum": "Ali-Rogers varian-6mv, e_min 0.1 MeV",
+        "histories_per_dij": int(np.sum(counts)),
+        "histories_per_beamlet": "log-uniform 1e4-1e6",
+        "n_batches": N_BATCHES,
+        "msc": "gs",
+        "truncation": 1e-3,
+        "l2": l2_note,
+    }
+
+
+# ---- clocks -----------------------------------------------------------------------
+class ClockSampler:
+    """nvidia-smi samples during the timed region (every 200 ms)."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int) -> None:
+        self.index = index
+        self.proc = None
+        self.lines: list[str] = []
+        self._t = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self._t = threading.Thread(target=self._read, daemon=True)
+            self._t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        if self._t is not None:
+            self._t.join(timeout=2)
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[5:9], strict=True):
+                if flag.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---- distributed plumbing ---------------------------------------------------------------
+def dist_setup(n_gpus: int):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device(f"cuda:{local}"))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def all_max(world, values):
+    if world == 1:
+        return list(values)
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor(values, dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return t.tolist()
+
+
+def all_sum(world, values):
+    if world == 1:
+        return list(values)
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor(values, dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return t.tolist()
+
+
+# ---- the CPU baseline -----------------------------------------------------------------
+def cpu_baseline(grid, xs, source, counts, target_seconds=15.0):
+    """The C oracle on all host cores, on a bounded sample of the same Dij."""
+    import oracle
+
+    tab = xs.build_tables(0.2, 0.05, source.max_energy * (1 + 1e-6))
+    gs = xs.gs_grid_for(tab, [0])
+    threads = oracle.max_threads()
+    sample = 20
+
+    def run(per_col):
+        t0 = time.perf_counter()
+        oracle.run(grid, tab, gs, source, counts=list(counts), n_batches=1, seed=SEED,
+                   forward=False, n_threads=threads, max_histories=per_col)
+        return time.perf_counter() - t0
+
+    elapsed = run(sample)
+    if elapsed < target_seconds:
+        sample = int(sample * min(200.0, target_seconds / max(elapsed, 1e-3)))
+        elapsed = run(sample)
+    done = int(np.sum(np.minimum(counts, sample)))
+    return {
+        "value": done / elapsed,
+        "unit": "histories/s",
+        "cores": threads,
+        "kind": "port",
+        "sample": f"{sample} histories of each of the 100 beamlets ({done} histories, "
+                  f"{elapsed:.1f} s), same phantom/spectrum/physics, one batch",
+    }
+
+
+def reference_arm(args, world, rank):
+    if rank != 0:
+        return 0
+    grid, xs, source, counts = workload()
+    import oracle
+
+    tab = xs.build_tables(0.2, 0.05, source.max_energy * (1 + 1e-6))
+    gs = xs.gs_grid_for(tab, [0])
+    threads = oracle.max_threads()
+    per_col = 200  # bounded sample per beamlet per step
+    times, done = [], int(np.sum(np.minimum(counts, per_col)))
+    for step in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        oracle.run(grid, tab, gs, source, counts=list(counts), n_batches=1, seed=SEED + step,
+                   forward=False, n_threads=threads, max_histories=per_col)
+        if step >= args.warmup:
+            times.append(time.perf_counter() - t0)
+    total = sum(times)
+    value = done * len(times) / total
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "histories/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * total / len(times), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": config_dict(counts, "n/a (CPU)"),
+        "cpu_baseline": {"value": value, "unit": "histories/s", "cores": threads, "kind": "port",
+                         "sample": f"{per_col} histories of each beamlet per step ({done})"},
+        "e2e": {"value": value, "unit": "histories/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---- the B200 arm ---------------------------------------------------------------------
+def algorithmic_bytes(c: dict) -> float:
+    """Transport bytes by event (the per-event figures stated in DESIGN.md)."""
+    pops = c["queue_pushes"]
+    return (13.0 * c["photon_flights"] + 32.0 * c["photon_interactions"]
+            + 77.0 * c["electron_substeps"] + 16.0 * c["deposits"]
+            + 48.0 * c["queue_pushes"] + 48.0 * pops)
+
+
+def b200_arm(args, world, rank, local):
+    import torch
+
+    from pyradmc_b200 import B200Engine, phantoms
+
+    device = f"cuda:{local}"
+    torch.cuda.set_device(local)
+    grid, xs, source, counts = workload(rank)
+    engine = B200Engine(grid, xs, device=device)
+    stream = torch.cuda.Stream(device=device)  # an explicit stream: the legacy default is 0
+    torch.cuda.set_stream(stream)
+    engine.use_stream(stream.cuda_stream)
+    kw = dict(n_histories_per_beamlet=counts, n_batches=N_BATCHES, seed=SEED + rank)
+    histories = int(np.sum(counts))
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=device)  # > 126 MB L2
+
+    for _ in range(args.warmup):
+        dij = engine.run_dij(source, **kw)
+    peaks_path = ROOT / "MEASURED_PEAKS.json"
+    peaks = json.loads(peaks_path.read_text()) if peaks_path.exists() else {}
+    hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
+
+    # device-resident steps
+    step_ms, counters = [], []
+    with ClockSampler(local) as clocks:
+        barrier(world)
+        torch.cuda.synchronize()
+        for _ in range(args.steps):
+            flush.fill_(1)
+            start = torch.cuda.Event(enable_timing=True)
+            end = torch.cuda.Event(enable_timing=True)
+            start.record(stream)
+            dij = engine.run_dij(source, **kw)
+            end.record(stream)
+            end.synchronize()
+            step_ms.append(start.elapsed_time(end))
+            counters.append(engine.last_counters())
+        torch.cuda.synchronize()
+        barrier(world)
+    total_ms = all_max(world, [sum(step_ms)])[0]
+    value = world * histories * args.steps / (total_ms / 1e3)
+
+    # end to end from host data: uploads and readback inside the timed region
+    e2e_ms, h2d, d2h = [], [], []
+    barrier(world)
+    torch.cuda.synchronize()
+    for _ in range(args.steps):
+        engine.drop_uploads()
+        before = engine.last_counters()
+        t0 = time.perf_counter()
+        dij = engine.run_dij(source, **kw)
+        dense_ok = dij.indptr[-1] == dij.indices.size
+        e2e_ms.append(1e3 * (time.perf_counter() - t0))
+        after = engine.last_counters()
+        h2d.append(after["h2d_bytes_total"] - before["h2d_bytes_total"])
+        d2h.append(after["d2h_bytes_total"] - before["d2h_bytes_total"])
+        assert dense_ok
+    torch.cuda.synchronize()
+    barrier(world)
+    e2e_total = all_max(world, [sum(e2e_ms)])[0]
+    e2e_value = world * histories * args.steps / (e2e_total / 1e3)
+
+    c = counters[-1]
+    transport_s = c["transport_ms"] / 1e3
+    achieved = algorithmic_bytes(c) / transport_s / 1e9
+    sigma = phantoms.per_beamlet_sigma(dij)
+    s_per_dij = total_ms / args.steps / 1e3
+    s_at_2pct = s_per_dij * (sigma / 0.02) ** 2
+    totals = all_sum(world, [dij.energy_deposited, dij.energy_escaped, dij.energy_emitted])
+    if rank != 0:
+        return 0
+    clock = clocks.summary()
+    base = cpu_baseline(grid, xs, source, counts) if world == 1 else None
+    traffic_path = ROOT / "profiles" / "transport_traffic.json"
+    traffic = None
+    if traffic_path.exists():
+        t = json.loads(traffic_path.read_text())
+        traffic = t.get("bytes_per_history", 0.0) * histories if t.get("bytes_per_history") else None
+    line = {
+        "metric": METRIC,
+        "value": value,
+        "unit": "histories/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": total_ms / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32 transport, int64 scoring, f64 statistics",
+        "data": "synthetic (seeded phantom and beamlet counts)",
+        "config": config_dict(counts, "256 MB buffer written between timed steps (flush)"),
+        "s_per_dij": s_per_dij,
+        "per_beamlet_sigma": sigma,
+        "s_per_dij_at_2pct_sigma": s_at_2pct,
+        "denoiser": None,
+        "e2e": {"value": e2e_value, "unit": "histories/s",
+                "h2d_bytes_per_step": int(np.median(h2d)), "d2h_bytes_per_step": int(np.median(d2h))},
+        "roofline": {
+            "bound": "hbm",
+            "kernel": "photon_kernel+electron_kernel (transport graph)",
+            "achieved": achieved,
+            "peak": hbm_peak,
+            "unit": "GB/s",
+            "frac": achieved / hbm_peak,
+            "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
+            "traffic": traffic,
+            "algorithmic_bytes": algorithmic_bytes(c),
+            "transport_ms": c["transport_ms"],
+            "reduce_ms": c["reduce_ms"],
+        },
+        "gpu_launches": int(sum(x["kernel_launches"] for x in counters)),
+        "counters": {k: c[k] for k in ("photon_flights", "photon_interactions", "electron_substeps",
+                                       "deposits", "queue_pushes", "primaries", "rounds")},
+        "energy_balance": (totals[0] + totals[1]) / totals[2],
+        "clocks": clock,
+        "cpu_baseline": base,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main() -> int:
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=("b200", "reference"), default="b200")
+    args = ap.parse_args()
+    world, rank, local = dist_setup(args.gpus)
+    try:
+        if args.impl == "reference":
+            return reference_arm(args, world, rank)
+        return b200_arm(args, world, rank, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,279 @@
+/*
+ * pyradmc_b200.h — C-ABI of the B200 Monte Carlo dose backend (libpmc_b200.so).
+ *
+ * The library replaces the device side of pyRadMC's Warp backend
+ * (pyradmc/backends/warp/engine.py, pyradmc/backends/warp/kernels.py): photon
+ * Woodcock transport, Class II condensed-history electron transport with
+ * Goudsmit-Saunderson multiple scattering, int64 fixed-point beamlet-tagged
+ * scoring, the per-batch float64 fold, finalize, and the truncation + CSC
+ * compaction of the dose-influence matrix.  Everything here is plain C types:
+ * host pointers and sizes in, host buffers out.  A Python host binds it with
+ * ctypes (pyradmc_b200/engine.py); any other FFI can bind it the same way.
+ *
+ * Conventions
+ *   - Every entry point returns 0 (PMC_OK) or a negative PMC_ERR_* code; the
+ *     message of the last failure is pmc_last_error(engine).
+ *   - Host buffers are caller-owned.  Device memory is engine-owned.
+ *   - One engine per host thread; calls on one engine are not re-entrant.  All
+ *     device work of a call is ordered on the engine's own CUDA stream, and a
+ *     call returns only after that work has finished.
+ *   - No call waits without bound: every device loop carries a step cap and a
+ *     round cap, and a tripped cap is reported as PMC_ERR_STEP_CAP.
+ */
+#ifndef PYRADMC_B200_H
+#define PYRADMC_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PMC_ABI_VERSION 1
+
+/* Return codes.  The Python host maps them onto the reference's exceptions:
+ * INVALID -> ValueError (engine.py:512-550), MAJORANT and QUEUE_OVERFLOW ->
+ * RuntimeError (engine.py:685-690, engine.py:347-351). */
+#define PMC_OK 0
+#define PMC_ERR_INVALID (-1)
+#define PMC_ERR_MAJORANT (-2)
+#define PMC_ERR_QUEUE_OVERFLOW (-3)
+#define PMC_ERR_STEP_CAP (-4)
+#define PMC_ERR_CUDA (-5)
+#define PMC_ERR_OOM (-6)
+#define PMC_ERR_STATE (-7)
+
+/* Particle kinds: pyradmc/transport/particles.py:23-25. */
+#define PMC_PHOTON 0
+#define PMC_ELECTRON 1
+#define PMC_POSITRON 2
+
+/* Primary generators.  PENCIL/PARALLEL/SPECTRAL mirror the Warp generators
+ * generate_pencil_beam (kernels.py:1888), generate_parallel_beam (:2035) and
+ * generate_spectral_beam (:2071); UPLOAD mirrors generate_from_upload (:1922),
+ * the host pre-sampling route of Source.sample_batch. */
+#define PMC_SRC_PENCIL 0
+#define PMC_SRC_PARALLEL 1
+#define PMC_SRC_SPECTRAL 2
+#define PMC_SRC_UPLOAD 3
+
+/* Beamlet generators: generate_beamlet_lattice (kernels.py:2248) and
+ * generate_spectral_beamlets (kernels.py:2322). */
+#define PMC_BEAMLET_LATTICE 0
+#define PMC_BEAMLET_SPECTRAL 1
+
+typedef struct pmc_engine pmc_engine;
+
+/* Flattened cross-section tables: the fields of CrossSectionTables
+ * (pyradmc/data/tables.py:140-219).  Per-material arrays are row-major
+ * [n_materials][n_points] float64; the engine casts to float32 on upload, as
+ * WarpEngine._upload_tables does (engine.py:3368-3429). */
+typedef struct pmc_tables_desc {
+    int32_t n_materials;
+    int32_t n_points;
+    double photon_log_e_min, photon_inv_dlog;
+    double electron_log_e_min, electron_inv_dlog;
+    double range_log_r_min, range_inv_dlog;
+    const double* mu_compton;
+    const double* mu_photo;
+    const double* mu_pair;
+    const double* mu_rayleigh;
+    const double* majorant; /* [n_points] */
+    const double* stopping_restricted;
+    const double* stopping_radiative;
+    const double* moller;
+    const double* csda_range;
+    const double* scattering_power;
+    const double* log_eta;
+    const double* restricted_range;
+    const double* energy_of_restricted_range;
+    int32_t n_coherent;
+    const double* coherent_x;          /* [n_coherent] */
+    const double* coherent_cumulative; /* [n_materials][n_coherent] */
+} pmc_tables_desc;
+
+/* Scoring geometry: a rectilinear grid (pyradmc/scoring/grid.py:67).  A
+ * deposit outside it is booked to the unscored ledger (kernels.py:536-585). */
+typedef struct pmc_scoring_desc {
+    int32_t nx, ny, nz;
+    double origin[3];
+    double spacing[3];
+    const double* voxel_mass; /* [nx*ny*nz] grams, C order */
+} pmc_scoring_desc;
+
+/* Open-field primary source (WarpEngine.run, engine.py:454). */
+typedef struct pmc_source_desc {
+    int32_t type; /* PMC_SRC_* */
+    int32_t kind; /* PMC_PHOTON or PMC_ELECTRON for the analytic beams */
+    double energy;
+    double position[3]; /* pencil */
+    double direction[3];
+    double z0, x_lo, x_extent, y_lo, y_extent; /* parallel */
+    /* spectral fan (geometry/source.py:479 _DivergentFan.emit_through) */
+    int32_t n_bins;
+    const double* edges; /* [n_bins+1] */
+    const double* cdf;   /* [n_bins] */
+    double focal[3], center[3], u_axis[3], v_axis[3];
+    double width_u, width_v;
+    /* upload: one record per history, in history order */
+    const int32_t* up_kind; /* PMC_PHOTON / PMC_ELECTRON / PMC_POSITRON */
+    const float* up_energy;
+    const float* up_pos;    /* [n][3] */
+    const float* up_dir;    /* [n][3] */
+    const float* up_weight;
+} pmc_source_desc;
+
+/* Beamlet source for run_dij (engine.py:948). */
+typedef struct pmc_beamlet_desc {
+    int32_t type; /* PMC_BEAMLET_* */
+    int32_t n_beamlets;
+    double energy, z0;                     /* lattice */
+    const double* x_lo;                    /* [n_beamlets] */
+    const double* x_extent;
+    const double* y_lo;
+    const double* y_extent;
+    int32_t n_bins;                        /* spectral beamlets */
+    const double* edges;
+    const double* cdf;
+    double focal[3], u_axis[3], v_axis[3];
+    double width_u, width_v;
+    const double* centers; /* [n_beamlets][3] */
+    /* Optional [n_beamlets] first global history of each beamlet; NULL means the
+     * exclusive prefix sum of counts.  Lets a caller run a range of beamlets
+     * (one device's share) with the streams the whole matrix would use. */
+    const int64_t* history_offsets;
+} pmc_beamlet_desc;
+
+/* Run options: the keyword arguments of WarpEngine.run / run_dij plus the
+ * scheduling knobs.  Scheduling knobs never change a result (bit-inert). */
+typedef struct pmc_run_params {
+    int64_t n_histories; /* run: total histories (divisible by n_batches) */
+    int32_t n_batches;
+    uint64_t seed;
+    double pcut, ecut;
+    int32_t transport_electrons;
+    int32_t msc_gs; /* 1 Goudsmit-Saunderson, 0 Gaussian hinge */
+    double step_energy_fraction;
+    double deposit_resolution; /* <= 0: single midpoint deposit */
+    int32_t dose_to_water;
+    int32_t photon_split_n; /* Compton splitting of primaries; 1 = off */
+    double truncation;      /* run_dij */
+    int32_t correlated;     /* run_dij */
+    int32_t beamlet_group_size; /* 0: auto */
+    /* scheduling */
+    int64_t chunk_size; /* new primaries admitted per transport round; 0: auto */
+    int32_t queue_factor;
+    int32_t block_size;     /* transport threads per block; 0: auto */
+    int32_t blocks_per_sm;  /* transport blocks per SM; 0: auto */
+    int32_t use_graph;      /* drain each batch inside one CUDA graph */
+    int64_t max_steps;      /* per-particle step cap; 0: default */
+} pmc_run_params;
+
+/* Exact integer energy books of a call, in quanta of 1e-9 MeV
+ * (kernels.py:96 ENERGY_QUANTUM_MEV). */
+typedef struct pmc_books {
+    int64_t deposited;
+    int64_t escaped;
+    int64_t unscored;
+    int64_t emitted; /* booked per primary by the spectral/upload routes */
+    int64_t majorant_violations;
+} pmc_books;
+
+/* Device event counters of the last call (for the roofline figures). */
+typedef struct pmc_counters {
+    int64_t photon_flights;
+    int64_t photon_interactions;
+    int64_t electron_substeps;
+    int64_t deposits;
+    int64_t queue_pushes;
+    int64_t primaries;
+    int64_t rounds;
+    int64_t transport_launches; /* graph launches (or host-loop rounds) */
+    int64_t reduce_launches;
+    int64_t kernel_launches;    /* every kernel of this library the call ran */
+    double transport_ms; /* device time of the transport kernels */
+    double reduce_ms;    /* device time of fold/finalize/truncation */
+    int64_t h2d_bytes_total; /* host-to-device bytes over the engine's life */
+    int64_t d2h_bytes_total; /* device-to-host bytes over the engine's life */
+} pmc_counters;
+
+int pmc_abi_version(void);
+int pmc_device_count(void);
+
+/* Engine lifetime.  Replaces the per-call uploads WarpEngine performs
+ * (_upload_grid engine.py:3336, _upload_tables :3368) with a resident engine. */
+int pmc_create(pmc_engine** out, int device_ordinal);
+void pmc_destroy(pmc_engine* engine);
+const char* pmc_last_error(const pmc_engine* engine);
+
+/* Transport grid: VoxelGrid (geometry/grid.py:227).  density float32 and
+ * material uint8 per voxel, C order (x slowest), as _upload_grid casts them. */
+int pmc_upload_grid(pmc_engine* engine, int32_t nx, int32_t ny, int32_t nz,
+                    const double origin[3], const double spacing[3],
+                    const float* density, const uint8_t* material);
+
+/* Cross-section tables (data/tables.py:222 build_cross_section_tables). */
+int pmc_upload_tables(pmc_engine* engine, const pmc_tables_desc* tables);
+
+/* Goudsmit-Saunderson node grid (data/goudsmit_saunderson.py:1108
+ * build_gs_grid): values [n_eta][n_theta2][n_u] float32, window origin
+ * (ix0, iy0), bins_per_log nodes per natural log. */
+int pmc_upload_gs(pmc_engine* engine, const float* values, int32_t ix0, int32_t iy0,
+                  int32_t n_eta, int32_t n_theta2, int32_t n_u, double bins_per_log);
+
+/* Scoring geometry; a call with NULL restores "score on the transport grid"
+ * (ScoringGrid.for_grid, scoring/grid.py:113). */
+int pmc_set_scoring(pmc_engine* engine, const pmc_scoring_desc* scoring);
+
+/* Open-field run: WarpEngine.run (engine.py:454).  dose and dose_sigma are
+ * caller buffers of n_scoring_voxels float64 (MeV/g per emitted history). */
+int pmc_run_forward(pmc_engine* engine, const pmc_source_desc* source,
+                    const pmc_run_params* params, double* dose, double* dose_sigma,
+                    pmc_books* books);
+
+/* Dij: WarpEngine.run_dij (engine.py:948).  counts[j] is beamlet j's history
+ * count (each divisible by n_batches); equal counts reproduce the reference
+ * mapping h = j * n_per + r (backends/ref/engine.py:410-442).  The CSC result
+ * stays on the engine; *nnz receives its entry count. */
+int pmc_run_dij(pmc_engine* engine, const pmc_beamlet_desc* source, const int64_t* counts,
+                const pmc_run_params* params, int64_t* nnz, pmc_books* books);
+
+/* Copy the CSC of the last pmc_run_dij into caller buffers:
+ * indptr[n_beamlets+1], indices[nnz], dose[nnz], sigma[nnz]
+ * (DijResult fields, scoring/dij.py:195-229). */
+int pmc_dij_fetch(pmc_engine* engine, int64_t* indptr, int64_t* indices, double* dose,
+                  double* sigma);
+
+int pmc_get_counters(const pmc_engine* engine, pmc_counters* counters);
+
+/* Run the engine's work on the caller's CUDA stream (a cudaStream_t passed as
+ * void*), e.g. to bracket it with the caller's own events; NULL restores the
+ * engine's private stream. */
+int pmc_set_stream(pmc_engine* engine, void* stream);
+
+/* Progress: fn(user, histories) is called from the calling thread after each
+ * completed batch of pmc_run_forward and each completed beamlet group of
+ * pmc_run_dij, with the histories that completed (progress.py:71 tick).  A
+ * NULL fn disables it. */
+typedef void (*pmc_progress_fn)(void* user, int64_t histories);
+int pmc_set_progress(pmc_engine* engine, pmc_progress_fn fn, void* user);
+
+/* Device reduction entry points, exposed on their own for the parity tests
+ * against the host scorers.  All pointers are host buffers.
+ *   fold:   BatchedBeamletScorer.end_batch (scoring/dij.py:155-174) over
+ *           batches of int64 quanta maps [n_batches][n_cols][n_vox];
+ *   finalize + truncate + compact: BatchedBeamletScorer.finalize
+ *           (scoring/dij.py:176-191) then DijAssembler.add_block (:351-366). */
+int pmc_reduce_dense(pmc_engine* engine, const int64_t* quanta, int32_t n_batches,
+                     int32_t n_cols, int64_t n_vox, const double* voxel_mass,
+                     const double* histories_per_batch, double* mean, double* sigma,
+                     int64_t* total_quanta);
+int pmc_truncate_dense(pmc_engine* engine, const double* mean, const double* sigma,
+                       int32_t n_cols, int64_t n_vox, double truncation, int64_t* counts,
+                       int64_t* nnz);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PYRADMC_B200_H */

@@ -1,0 +1,39 @@
+"""pyradmc_b200: a B200-native Monte Carlo dose backend for pyRadMC.
+
+``B200Engine`` is a drop-in for pyRadMC's ``WarpEngine(device="cuda:0")``: the
+same ``run`` / ``run_dij`` calls, with the transport, scoring, batch statistics
+and Dij compaction running as hand-written sm_100a CUDA behind the C-ABI of
+``include/pyradmc_b200.h``.
+"""
+
+from pyradmc_b200.engine import B200Engine
+from pyradmc_b200.model import (
+    AnalyticWaterTables,
+    BeamletGridSource,
+    DijResult,
+    ParallelBeamSource,
+    PencilBeamSource,
+    ScoringGrid,
+    SpectralBeamletSource,
+    SpectralBeamSource,
+    Spectrum,
+    TransportResult,
+    VoxelGrid,
+    ali_rogers_varian_6mv,
+)
+
+__all__ = [
+    "AnalyticWaterTables",
+    "B200Engine",
+    "BeamletGridSource",
+    "DijResult",
+    "ParallelBeamSource",
+    "PencilBeamSource",
+    "ScoringGrid",
+    "SpectralBeamSource",
+    "SpectralBeamletSource",
+    "Spectrum",
+    "TransportResult",
+    "VoxelGrid",
+    "ali_rogers_varian_6mv",
+]

@@ -1,0 +1,261 @@
+"""ctypes binding of ``libpmc_b200.so`` (the C-ABI of ``include/pyradmc_b200.h``).
+
+The structures below mirror the header field for field.  Loading fails loudly:
+there is no CPU fallback anywhere in this package — a missing or unbuildable
+library raises, it never degrades to another implementation.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import threading
+from pathlib import Path
+
+from pyradmc_b200.build import LIBRARY, build
+
+PMC_OK = 0
+PMC_ERR_INVALID = -1
+PMC_ERR_MAJORANT = -2
+PMC_ERR_QUEUE_OVERFLOW = -3
+PMC_ERR_STEP_CAP = -4
+PMC_ERR_CUDA = -5
+PMC_ERR_OOM = -6
+PMC_ERR_STATE = -7
+
+PMC_PHOTON, PMC_ELECTRON, PMC_POSITRON = 0, 1, 2
+PMC_SRC_PENCIL, PMC_SRC_PARALLEL, PMC_SRC_SPECTRAL, PMC_SRC_UPLOAD = 0, 1, 2, 3
+PMC_BEAMLET_LATTICE, PMC_BEAMLET_SPECTRAL = 0, 1
+
+_dp = C.POINTER(C.c_double)
+_fp = C.POINTER(C.c_float)
+_ip = C.POINTER(C.c_int32)
+_lp = C.POINTER(C.c_int64)
+_u8p = C.POINTER(C.c_uint8)
+_d3 = C.c_double * 3
+
+
+class TablesDesc(C.Structure):
+    _fields_ = [
+        ("n_materials", C.c_int32),
+        ("n_points", C.c_int32),
+        ("photon_log_e_min", C.c_double),
+        ("photon_inv_dlog", C.c_double),
+        ("electron_log_e_min", C.c_double),
+        ("electron_inv_dlog", C.c_double),
+        ("range_log_r_min", C.c_double),
+        ("range_inv_dlog", C.c_double),
+        ("mu_compton", _dp),
+        ("mu_photo", _dp),
+        ("mu_pair", _dp),
+        ("mu_rayleigh", _dp),
+        ("majorant", _dp),
+        ("stopping_restricted", _dp),
+        ("stopping_radiative", _dp),
+        ("moller", _dp),
+        ("csda_range", _dp),
+        ("scattering_power", _dp),
+        ("log_eta", _dp),
+        ("restricted_range", _dp),
+        ("energy_of_restricted_range", _dp),
+        ("n_coherent", C.c_int32),
+        ("coherent_x", _dp),
+        ("coherent_cumulative", _dp),
+    ]
+
+
+class ScoringDesc(C.Structure):
+    _fields_ = [
+        ("nx", C.c_int32),
+        ("ny", C.c_int32),
+        ("nz", C.c_int32),
+        ("origin", _d3),
+        ("spacing", _d3),
+        ("voxel_mass", _dp),
+    ]
+
+
+class SourceDesc(C.Structure):
+    _fields_ = [
+        ("type", C.c_int32),
+        ("kind", C.c_int32),
+        ("energy", C.c_double),
+        ("position", _d3),
+        ("direction", _d3),
+        ("z0", C.c_double),
+        ("x_lo", C.c_double),
+        ("x_extent", C.c_double),
+        ("y_lo", C.c_double),
+        ("y_extent", C.c_double),
+        ("n_bins", C.c_int32),
+        ("edges", _dp),
+        ("cdf", _dp),
+        ("focal", _d3),
+        ("center", _d3),
+        ("u_axis", _d3),
+        ("v_axis", _d3),
+        ("width_u", C.c_double),
+        ("width_v", C.c_double),
+        ("up_kind", _ip),
+        ("up_energy", _fp),
+        ("up_pos", _fp),
+        ("up_dir", _fp),
+        ("up_weight", _fp),
+    ]
+
+
+class BeamletDesc(C.Structure):
+    _fields_ = [
+        ("type", C.c_int32),
+        ("n_beamlets", C.c_int32),
+        ("energy", C.c_double),
+        ("z0", C.c_double),
+        ("x_lo", _dp),
+        ("x_extent", _dp),
+        ("y_lo", _dp),
+        ("y_extent", _dp),
+        ("n_bins", C.c_int32),
+        ("edges", _dp),
+        ("cdf", _dp),
+        ("focal", _d3),
+        ("u_axis", _d3),
+        ("v_axis", _d3),
+        ("width_u", C.c_double),
+        ("width_v", C.c_double),
+        ("centers", _dp),
+        ("history_offsets", _lp),
+    ]
+
+
+class RunParams(C.Structure):
+    _fields_ = [
+        ("n_histories", C.c_int64),
+        ("n_batches", C.c_int32),
+        ("seed", C.c_uint64),
+        ("pcut", C.c_double),
+        ("ecut", C.c_double),
+        ("transport_electrons", C.c_int32),
+        ("msc_gs", C.c_int32),
+        ("step_energy_fraction", C.c_double),
+        ("deposit_resolution", C.c_double),
+        ("dose_to_water", C.c_int32),
+        ("photon_split_n", C.c_int32),
+        ("truncation", C.c_double),
+        ("correlated", C.c_int32),
+        ("beamlet_group_size", C.c_int32),
+        ("chunk_size", C.c_int64),
+        ("queue_factor", C.c_int32),
+        ("block_size", C.c_int32),
+        ("blocks_per_sm", C.c_int32),
+        ("use_graph", C.c_int32),
+        ("max_steps", C.c_int64),
+    ]
+
+
+class Books(C.Structure):
+    _fields_ = [
+        ("deposited", C.c_int64),
+        ("escaped", C.c_int64),
+        ("unscored", C.c_int64),
+        ("emitted", C.c_int64),
+        ("majorant_violations", C.c_int64),
+    ]
+
+
+class Counters(C.Structure):
+    _fields_ = [
+        ("photon_flights", C.c_int64),
+        ("photon_interactions", C.c_int64),
+        ("electron_substeps", C.c_int64),
+        ("deposits", C.c_int64),
+        ("queue_pushes", C.c_int64),
+        ("primaries", C.c_int64),
+        ("rounds", C.c_int64),
+        ("transport_launches", C.c_int64),
+        ("reduce_launches", C.c_int64),
+        ("kernel_launches", C.c_int64),
+        ("transport_ms", C.c_double),
+        ("reduce_ms", C.c_double),
+        ("h2d_bytes_total", C.c_int64),
+        ("d2h_bytes_total", C.c_int64),
+    ]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+# Every symbol the header declares, with its ctypes signature.
+SIGNATURES: dict[str, tuple[object, list]] = {
+    "pmc_abi_version": (C.c_int, []),
+    "pmc_device_count": (C.c_int, []),
+    "pmc_create": (C.c_int, [C.POINTER(C.c_void_p), C.c_int]),
+    "pmc_destroy": (None, [C.c_void_p]),
+    "pmc_last_error": (C.c_char_p, [C.c_void_p]),
+    "pmc_upload_grid": (
+        C.c_int,
+        [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, _dp, _dp, _fp, _u8p],
+    ),
+    "pmc_upload_tables": (C.c_int, [C.c_void_p, C.POINTER(TablesDesc)]),
+    "pmc_upload_gs": (
+        C.c_int,
+        [C.c_void_p, _fp, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_double],
+    ),
+    "pmc_set_scoring": (C.c_int, [C.c_void_p, C.POINTER(ScoringDesc)]),
+    "pmc_run_forward": (
+        C.c_int,
+        [C.c_void_p, C.POINTER(SourceDesc), C.POINTER(RunParams), _dp, _dp, C.POINTER(Books)],
+    ),
+    "pmc_run_dij": (
+        C.c_int,
+        [C.c_void_p, C.POINTER(BeamletDesc), _lp, C.POINTER(RunParams), _lp, C.POINTER(Books)],
+    ),
+    "pmc_dij_fetch": (C.c_int, [C.c_void_p, _lp, _lp, _dp, _dp]),
+    "pmc_get_counters": (C.c_int, [C.c_void_p, C.POINTER(Counters)]),
+    "pmc_set_progress": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "pmc_set_stream": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "pmc_reduce_dense": (
+        C.c_int,
+        [C.c_void_p, _lp, C.c_int32, C.c_int32, C.c_int64, _dp, _dp, _dp, _dp, _lp],
+    ),
+    "pmc_truncate_dense": (
+        C.c_int,
+        [C.c_void_p, _dp, _dp, C.c_int32, C.c_int64, C.c_double, _lp, _lp],
+    ),
+}
+
+PROGRESS_FN = C.CFUNCTYPE(None, C.c_void_p, C.c_int64)
+
+_lib: C.CDLL | None = None
+_lock = threading.Lock()
+
+
+def library_path() -> Path:
+    return LIBRARY
+
+
+def load(build_if_missing: bool = True) -> C.CDLL:
+    """Load (building first if needed) the shared library and bind every symbol."""
+    global _lib
+    with _lock:
+        if _lib is not None:
+            return _lib
+        if build_if_missing:
+            build()
+        if not LIBRARY.exists():
+            raise RuntimeError(
+                f"the B200 backend library {LIBRARY} is missing; build it with "
+                "`python -m pyradmc_b200.build` (there is no CPU fallback)"
+            )
+        lib = C.CDLL(str(LIBRARY))
+        for name, (restype, argtypes) in SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.restype = restype
+            fn.argtypes = argtypes
+        _lib = lib
+        return lib
+
+
+def ptr(array, ctype):
+    """ctypes pointer to a contiguous numpy array (or None)."""
+    if array is None:
+        return None
+    return array.ctypes.data_as(C.POINTER(ctype))

@@ -1,0 +1,76 @@
+"""Build the sm_100a shared library of the B200 backend, in-tree.
+
+``python -m pyradmc_b200.build`` compiles ``csrc/pmc_runtime.cu`` (which includes
+every kernel header) with nvcc for ``sm_100a`` into ``_lib/libpmc_b200.so``.  The
+library is rebuilt only when a source is newer than it, unless ``force`` is set.
+"""
+
+from __future__ import annotations
+
+import os
+import subprocess
+import sys
+from pathlib import Path
+
+PACKAGE = Path(__file__).resolve().parent
+CSRC = PACKAGE / "csrc"
+LIBDIR = PACKAGE / "_lib"
+LIBRARY = LIBDIR / "libpmc_b200.so"
+INCLUDE = PACKAGE.parent / "include"
+
+ARCH_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a"]
+NVCC_FLAGS = [
+    "-O3",
+    "-lineinfo",
+    "-std=c++17",
+    "--expt-relaxed-constexpr",
+    "-Xcompiler",
+    "-fPIC",
+    "-shared",
+    "-lcudart",
+]
+
+
+def nvcc() -> str:
+    """Locate nvcc: $CUDA_HOME/bin, /usr/local/cuda/bin, then PATH."""
+    for root in (os.environ.get("CUDA_HOME"), "/usr/local/cuda"):
+        if root and (Path(root) / "bin" / "nvcc").exists():
+            return str(Path(root) / "bin" / "nvcc")
+    return "nvcc"
+
+
+def sources() -> list[Path]:
+    """Every file the library depends on."""
+    return sorted(CSRC.glob("*.cu")) + sorted(CSRC.glob("*.cuh")) + sorted(INCLUDE.glob("*.h"))
+
+
+def needs_build() -> bool:
+    if not LIBRARY.exists():
+        return True
+    built = LIBRARY.stat().st_mtime
+    return any(src.stat().st_mtime > built for src in sources())
+
+
+def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) -> Path:
+    """Compile the library if it is missing or stale; return its path."""
+    if not force and not needs_build():
+        return LIBRARY
+    LIBDIR.mkdir(exist_ok=True)
+    tmp = LIBRARY.with_suffix(f".so.tmp{os.getpid()}")
+    cmd = [nvcc(), *ARCH_FLAGS, *NVCC_FLAGS, f"-I{INCLUDE}", str(CSRC / "pmc_runtime.cu"), "-o", str(tmp)]
+    if ptxas_info:
+        cmd.insert(1, "-Xptxas=-v")
+    if verbose:
+        print(" ".join(cmd), file=sys.stderr)
+    proc = subprocess.run(cmd, capture_output=True, text=True)
+    if proc.returncode != 0:
+        tmp.unlink(missing_ok=True)
+        raise RuntimeError(f"nvcc failed ({proc.returncode}):\n{proc.stdout}\n{proc.stderr}")
+    if ptxas_info or verbose:
+        sys.stderr.write(proc.stderr)
+    tmp.replace(LIBRARY)
+    return LIBRARY
+
+
+if __name__ == "__main__":
+    build(force="--force" in sys.argv, verbose=True, ptxas_info="--ptxas" in sys.argv)

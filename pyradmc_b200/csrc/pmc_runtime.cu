@@ -1,0 +1,1188 @@
+// pmc_runtime.cu — the engine behind the C-ABI of include/pyradmc_b200.h.
+//
+// Host orchestration of WarpEngine.run / run_dij (pyradmc/backends/warp/
+// engine.py:454-1572), re-planned for one resident B200 engine:
+//   * uploads persist across calls; buffers grow on demand and are reused;
+//   * a batch is one launch of a CUDA graph whose conditional WHILE node runs
+//     [photon kernel -> electron kernel] until the device reports no work left
+//     (the Warp engine read every queue count back to the host, engine.py:
+//     2766-2831);
+//   * the fold, finalize, truncation and CSC compaction (including its prefix
+//     sum) run on the device; only the kept CSC entries cross to the host.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/pyradmc_b200.h"
+#include "pmc_common.cuh"
+#include "pmc_reduce.cuh"
+#include "pmc_transport.cuh"
+
+using namespace pmc;
+
+namespace {
+
+constexpr long long kDefaultMaxSteps = 10000000LL;  // per particle
+constexpr long long kMaxRounds = 1000000LL;         // per batch
+
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+};
+
+}  // namespace
+
+struct pmc_engine {
+    int device = 0;
+    cudaStream_t stream = nullptr;        // the stream every call runs on
+    cudaStream_t own_stream = nullptr;    // the engine's private stream
+    std::string error;
+    int sm_count = 0;
+
+    // transport grid
+    bool has_grid = false;
+    int max_material = 0;
+    GridInfo gi{};
+    float2* d_vox = nullptr;
+    std::vector<double> default_mass;  // density * volume for the default scoring grid
+
+    // scoring grid
+    GridInfo si{};
+    bool custom_scoring = false;
+    double* d_mass = nullptr;
+    long long mass_len = 0;
+
+    // tables
+    bool has_tables = false;
+    bool has_gs = false;
+    Tables tab{};
+    std::vector<void*> table_allocs;
+    float4* d_gs4 = nullptr;
+
+    // transport buffers
+    DevBuf q[4];
+    unsigned int q_capacity = 0;
+    DevBuf edep, s1, s2;
+    Sched* d_sched = nullptr;
+    Counters* d_counters = nullptr;
+    GenDesc* d_gen = nullptr;
+    unsigned long long* d_total_q = nullptr;
+    unsigned long long* d_colmax = nullptr;
+    long long colmax_len = 0;
+    DevBuf tile_counts, tile_offsets, col_counts, out_idx, out_dose, out_sigma, col_nhist;
+    unsigned long long* d_nnz = nullptr;
+    std::vector<void*> run_allocs;  // per-call generator arrays
+
+    // graph of the drain loop
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t graph_exec = nullptr;
+    cudaGraphConditionalHandle cond = 0;
+    int graph_grid[2] = {0, 0};
+    int graph_block = 0;
+    TransportParams graph_params{};
+
+    // results of the last Dij
+    std::vector<long long> dij_indptr;
+    std::vector<long long> dij_indices;
+    std::vector<double> dij_dose;
+    std::vector<double> dij_sigma;
+
+    pmc_counters counters{};
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    unsigned long long h2d_bytes = 0;  // cumulative over the engine's life
+    unsigned long long d2h_bytes = 0;
+    pmc_progress_fn progress = nullptr;
+    void* progress_user = nullptr;
+};
+
+namespace {
+
+int fail(pmc_engine* e, int code, const char* fmt, ...) {
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    if (e) e->error = buf;
+    return code;
+}
+
+#define PMC_CUDA(e, call)                                                                  \
+    do {                                                                                   \
+        cudaError_t _st = (call);                                                          \
+        if (_st != cudaSuccess) {                                                          \
+            return fail((e), _st == cudaErrorMemoryAllocation ? PMC_ERR_OOM : PMC_ERR_CUDA, \
+                        "CUDA error %s at %s:%d: %s", cudaGetErrorName(_st), __FILE__,     \
+                        __LINE__, cudaGetErrorString(_st));                                \
+        }                                                                                  \
+    } while (0)
+
+int ensure(pmc_engine* e, DevBuf& b, size_t bytes) {
+    if (b.bytes >= bytes && b.p) return PMC_OK;
+    if (b.p) cudaFree(b.p);
+    b.p = nullptr;
+    b.bytes = 0;
+    PMC_CUDA(e, cudaMalloc(&b.p, std::max<size_t>(bytes, 16)));
+    b.bytes = std::max<size_t>(bytes, 16);
+    return PMC_OK;
+}
+
+template <typename T>
+int upload_vec(pmc_engine* e, const std::vector<T>& v, const T** out) {
+    void* p = nullptr;
+    PMC_CUDA(e, cudaMalloc(&p, std::max<size_t>(v.size() * sizeof(T), 16)));
+    if (!v.empty()) PMC_CUDA(e, cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+    e->h2d_bytes += (unsigned long long)(v.size() * sizeof(T));
+    e->run_allocs.push_back(p);
+    *out = (const T*)p;
+    return PMC_OK;
+}
+
+void free_run_allocs(pmc_engine* e) {
+    for (void* p : e->run_allocs) cudaFree(p);
+    e->run_allocs.clear();
+}
+
+void free_tables(pmc_engine* e) {
+    for (void* p : e->table_allocs) cudaFree(p);
+    e->table_allocs.clear();
+    e->has_tables = false;
+}
+
+void destroy_graph(pmc_engine* e) {
+    if (e->graph_exec) cudaGraphExecDestroy(e->graph_exec);
+    if (e->graph) cudaGraphDestroy(e->graph);
+    e->graph_exec = nullptr;
+    e->graph = nullptr;
+    e->cond = 0;
+}
+
+GridInfo make_grid(int nx, int ny, int nz, const double o[3], const double s[3]) {
+    // Bounds computed in float64 and stored as float32, as the Warp GridInfo
+    // struct does (engine.py:3336-3345).
+    GridInfo g{};
+    g.x_lo = (float)o[0];
+    g.y_lo = (float)o[1];
+    g.z_lo = (float)o[2];
+    g.x_hi = (float)(o[0] + nx * s[0]);
+    g.y_hi = (float)(o[1] + ny * s[1]);
+    g.z_hi = (float)(o[2] + nz * s[2]);
+    g.sx = (float)s[0];
+    g.sy = (float)s[1];
+    g.sz = (float)s[2];
+    g.nx = nx;
+    g.ny = ny;
+    g.nz = nz;
+    g.n_voxels = (long long)nx * ny * nz;
+    return g;
+}
+
+int transport_launch_shape(pmc_engine* e, const pmc_run_params* p, int* grid_ph, int* grid_el,
+                           int* block) {
+    int bs = p->block_size > 0 ? p->block_size : 256;
+    if (bs % 32 != 0 || bs > 256) return fail(e, PMC_ERR_INVALID, "block_size must be a multiple of 32 and <= 256");
+    int per_sm_ph = 0, per_sm_el = 0;
+    PMC_CUDA(e, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_ph, photon_kernel, bs, 0));
+    PMC_CUDA(e, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_el, electron_kernel, bs, 0));
+    if (p->blocks_per_sm > 0) {
+        per_sm_ph = std::min(per_sm_ph, p->blocks_per_sm);
+        per_sm_el = std::min(per_sm_el, p->blocks_per_sm);
+    }
+    per_sm_ph = std::max(per_sm_ph, 1);
+    per_sm_el = std::max(per_sm_el, 1);
+    *grid_ph = per_sm_ph * e->sm_count;
+    *grid_el = per_sm_el * e->sm_count;
+    *block = bs;
+    return PMC_OK;
+}
+
+// The drain graph: WHILE(remaining) { photon_kernel; electron_kernel }.
+int build_graph(pmc_engine* e, const TransportParams& P, int grid_ph, int grid_el, int block) {
+    destroy_graph(e);
+    PMC_CUDA(e, cudaGraphCreate(&e->graph, 0));
+    PMC_CUDA(e, cudaGraphConditionalHandleCreate(&e->cond, e->graph, 1, cudaGraphCondAssignDefault));
+    cudaGraphNodeParams cp{};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = e->cond;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t cnode;
+    PMC_CUDA(e, cudaGraphAddNode(&cnode, e->graph, nullptr, 0, &cp));
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+
+    e->graph_params = P;
+    void* args[] = {&e->graph_params};
+    cudaKernelNodeParams kp{};
+    kp.func = (void*)photon_kernel;
+    kp.gridDim = dim3(grid_ph);
+    kp.blockDim = dim3(block);
+    kp.sharedMemBytes = 0;
+    kp.kernelParams = args;
+    cudaGraphNode_t n_ph, n_el;
+    PMC_CUDA(e, cudaGraphAddKernelNode(&n_ph, body, nullptr, 0, &kp));
+    kp.func = (void*)electron_kernel;
+    kp.gridDim = dim3(grid_el);
+    PMC_CUDA(e, cudaGraphAddKernelNode(&n_el, body, &n_ph, 1, &kp));
+    PMC_CUDA(e, cudaGraphInstantiate(&e->graph_exec, e->graph, 0));
+    e->graph_grid[0] = grid_ph;
+    e->graph_grid[1] = grid_el;
+    e->graph_block = block;
+    return PMC_OK;
+}
+
+__global__ void init_batch_kernel(Sched* S, int batch, unsigned long long block_end,
+                                  unsigned long long budget, long long max_rounds,
+                                  unsigned long long cond) {
+    S->p_in = 0;
+    S->e_in = 0;
+    for (int i = 0; i < 4; ++i) {
+        S->count[i] = 0u;
+        S->head[i] = 0u;
+    }
+    S->cursor = 0ull;
+    S->block_end = block_end;
+    S->budget = budget;
+    S->limit = budget < block_end ? budget : block_end;
+    S->blocks_done = 0u;
+    S->remaining = 1;
+    S->batch = batch;
+    S->rounds = 0;
+    S->max_rounds = max_rounds;
+    S->cond_handle = cond;
+}
+
+struct SchedHost {
+    Sched s;
+};
+
+int read_sched(pmc_engine* e, Sched* out) {
+    PMC_CUDA(e, cudaMemcpyAsync(out, e->d_sched, sizeof(Sched), cudaMemcpyDeviceToHost, e->stream));
+        e->d2h_bytes += (unsigned long long)(sizeof(Sched));
+    PMC_CUDA(e, cudaStreamSynchronize(e->stream));
+    return PMC_OK;
+}
+
+int check_flags(pmc_engine* e, const Sched& s) {
+    if (s.flags & kFlagOverflow)
+        return fail(e, PMC_ERR_QUEUE_OVERFLOW,
+                    "particle queue overflow (capacity %u). Lower chunk_size or raise queue_factor.",
+                    e->q_capacity);
+    if (s.flags & kFlagStepCap)
+        return fail(e, PMC_ERR_STEP_CAP,
+                    "a particle exceeded the per-particle step cap; transport stopped early");
+    if (s.flags & kFlagRoundCap)
+        return fail(e, PMC_ERR_STEP_CAP, "a batch exceeded the transport round cap");
+    return PMC_OK;
+}
+
+struct RunPlan {
+    int grid_ph = 0, grid_el = 0, block = 0;
+    unsigned long long budget = 0;
+    long long max_steps = 0;
+};
+
+int prepare_transport(pmc_engine* e, const pmc_run_params* p, RunPlan* plan) {
+    if (!e->has_grid) return fail(e, PMC_ERR_STATE, "no transport grid uploaded");
+    if (!e->has_tables) return fail(e, PMC_ERR_STATE, "no cross-section tables uploaded");
+    if (p->msc_gs && !e->has_gs)
+        return fail(e, PMC_ERR_STATE, "msc_model='gs' needs the Goudsmit-Saunderson grid");
+    if (p->n_batches < 1) return fail(e, PMC_ERR_INVALID, "need at least one batch, got %d", p->n_batches);
+    if (e->max_material >= e->tab.n_materials)
+        return fail(e, PMC_ERR_INVALID, "material index %d beyond the cross-section source (%d materials)",
+                    e->max_material, e->tab.n_materials);
+    int rc = transport_launch_shape(e, p, &plan->grid_ph, &plan->grid_el, &plan->block);
+    if (rc) return rc;
+    const unsigned long long resident =
+        (unsigned long long)std::max(plan->grid_ph, plan->grid_el) * plan->block;
+    plan->budget = p->chunk_size > 0 ? (unsigned long long)p->chunk_size : 4ull * resident;
+    const int qf = p->queue_factor > 0 ? p->queue_factor : 16;
+    const unsigned long long cap64 = plan->budget * (unsigned long long)qf;
+    if (cap64 > 0x7fffffffull)
+        return fail(e, PMC_ERR_INVALID, "chunk_size * queue_factor exceeds the queue index range");
+    const unsigned int cap = (unsigned int)cap64;
+    if (cap > e->q_capacity) {
+        for (int i = 0; i < 4; ++i) {
+            rc = ensure(e, e->q[i], (size_t)cap * sizeof(Slot));
+            if (rc) return rc;
+        }
+        e->q_capacity = cap;
+    }
+    plan->max_steps = p->max_steps > 0 ? p->max_steps : kDefaultMaxSteps;
+    return PMC_OK;
+}
+
+TransportParams make_params(pmc_engine* e, const pmc_run_params* p, const RunPlan& plan) {
+    TransportParams P{};
+    P.gi = e->gi;
+    P.si = e->si;
+    P.vox = e->d_vox;
+    P.tab = e->tab;
+    for (int i = 0; i < 4; ++i) P.q[i] = (Slot*)e->q[i].p;
+    P.capacity = e->q_capacity;
+    P.sched = e->d_sched;
+    P.gen = e->d_gen;
+    P.edep = (unsigned long long*)e->edep.p;
+    P.counters = e->d_counters;
+    P.seed_lo = (uint32_t)(p->seed & 0xffffffffull);
+    P.seed_hi = (uint32_t)(p->seed >> 32);
+    P.pcut = (float)p->pcut;
+    P.ecut = (float)p->ecut;
+    P.step_fraction = (float)p->step_energy_fraction;
+    P.deposit_resolution = (float)p->deposit_resolution;
+    P.transport_electrons = p->transport_electrons ? 1 : 0;
+    P.msc_gs = p->msc_gs ? 1 : 0;
+    P.dose_to_water = p->dose_to_water ? 1 : 0;
+    P.split_n = p->photon_split_n > 1 ? p->photon_split_n : 1;
+    P.max_steps = plan.max_steps;
+    return P;
+}
+
+// Transport one statistical batch of the current group into e->edep.
+int run_batch(pmc_engine* e, const pmc_run_params* p, const RunPlan& plan, TransportParams& P,
+              int batch, unsigned long long block) {
+    if (block == 0) return PMC_OK;
+    const bool graph = p->use_graph != 0;
+    if (graph) {
+        const bool same = e->graph_exec && e->graph_grid[0] == plan.grid_ph &&
+                          e->graph_grid[1] == plan.grid_el && e->graph_block == plan.block &&
+                          std::memcmp(&e->graph_params, &P, sizeof P) == 0;
+        if (!same) {
+            int rc = build_graph(e, P, plan.grid_ph, plan.grid_el, plan.block);
+            if (rc) return rc;
+        }
+    }
+    init_batch_kernel<<<1, 1, 0, e->stream>>>(e->d_sched, batch, block, plan.budget, kMaxRounds,
+                                              graph ? (unsigned long long)e->cond : 0ull);
+    PMC_CUDA(e, cudaGetLastError());
+    e->counters.kernel_launches += 1;
+    if (graph) {
+        PMC_CUDA(e, cudaGraphLaunch(e->graph_exec, e->stream));
+        e->counters.transport_launches += 1;
+        return PMC_OK;
+    }
+    for (long long round = 0; round < kMaxRounds; ++round) {
+        photon_kernel<<<plan.grid_ph, plan.block, 0, e->stream>>>(P);
+        electron_kernel<<<plan.grid_el, plan.block, 0, e->stream>>>(P);
+        PMC_CUDA(e, cudaGetLastError());
+        e->counters.transport_launches += 2;
+        Sched s;
+        int rc = read_sched(e, &s);
+        if (rc) return rc;
+        if (!s.remaining) break;
+    }
+    return PMC_OK;
+}
+
+int launch_fold(pmc_engine* e, long long n_vox, int group, const double* d_col_nhist) {
+    const long long n_total = n_vox * group;
+    const int blocks = (int)std::min<long long>((n_total + kReduceThreads - 1) / kReduceThreads,
+                                                (long long)e->sm_count * 16);
+    fold_kernel<<<std::max(blocks, 1), kReduceThreads, 0, e->stream>>>(
+        (unsigned long long*)e->edep.p, e->d_mass, d_col_nhist, n_vox, n_total, (double*)e->s1.p,
+        (double*)e->s2.p, e->d_total_q);
+    PMC_CUDA(e, cudaGetLastError());
+    e->counters.reduce_launches += 1;
+    return PMC_OK;
+}
+
+int ensure_colmax(pmc_engine* e, int group) {
+    if (group > e->colmax_len) {
+        if (e->d_colmax) cudaFree(e->d_colmax);
+        PMC_CUDA(e, cudaMalloc(&e->d_colmax, sizeof(unsigned long long) * group));
+        e->colmax_len = group;
+    }
+    return PMC_OK;
+}
+
+int launch_finalize(pmc_engine* e, long long n_vox, int group, int n_batches) {
+    int rc = ensure_colmax(e, group);
+    if (rc) return rc;
+    PMC_CUDA(e, cudaMemsetAsync(e->d_colmax, 0, sizeof(unsigned long long) * group, e->stream));
+    const int n_tiles = (int)((n_vox + kTileVoxels - 1) / kTileVoxels);
+    finalize_kernel<<<dim3(n_tiles, group), kReduceThreads, 0, e->stream>>>(
+        (double*)e->s1.p, (double*)e->s2.p, n_vox, n_batches, e->d_colmax);
+    PMC_CUDA(e, cudaGetLastError());
+    e->counters.reduce_launches += 1;
+    return PMC_OK;
+}
+
+// Truncate + compact the finalized group held in s1 (mean) / s2 (sigma) and
+// append its columns to the host CSC.
+int truncate_group(pmc_engine* e, long long n_vox, int group, double truncation) {
+    const int n_tiles = (int)((n_vox + kTileVoxels - 1) / kTileVoxels);
+    const long long n_tc = (long long)n_tiles * group;
+    int rc = ensure(e, e->tile_counts, sizeof(unsigned int) * n_tc);
+    if (!rc) rc = ensure(e, e->tile_offsets, sizeof(unsigned long long) * n_tc);
+    if (!rc) rc = ensure(e, e->col_counts, sizeof(long long) * group);
+    if (rc) return rc;
+    count_kept_kernel<<<dim3(n_tiles, group), kReduceThreads, 0, e->stream>>>(
+        (const double*)e->s1.p, n_vox, n_tiles, truncation, e->d_colmax,
+        (unsigned int*)e->tile_counts.p);
+    scan_tiles_kernel<<<1, 1024, 0, e->stream>>>(
+        (const unsigned int*)e->tile_counts.p, n_tc, (unsigned long long*)e->tile_offsets.p, group,
+        n_tiles, (long long*)e->col_counts.p, e->d_nnz);
+    PMC_CUDA(e, cudaGetLastError());
+    unsigned long long nnz = 0;
+    std::vector<long long> counts(group);
+    PMC_CUDA(e, cudaMemcpyAsync(&nnz, e->d_nnz, sizeof nnz, cudaMemcpyDeviceToHost, e->stream));
+        e->d2h_bytes += (unsigned long long)(sizeof nnz);
+    PMC_CUDA(e, cudaMemcpyAsync(counts.data(), e->col_counts.p, sizeof(long long) * group, cudaMemcpyDeviceToHost, e->stream));
+        e->d2h_bytes += (unsigned long long)(sizeof(long long) * group);
+    PMC_CUDA(e, cudaStreamSynchronize(e->stream));
+    rc = ensure(e, e->out_idx, sizeof(long long) * nnz);
+    if (!rc) rc = ensure(e, e->out_dose, sizeof(double) * nnz);
+    if (!rc) rc = ensure(e, e->out_sigma, sizeof(double) * nnz);
+    if (rc) return rc;
+    if (nnz > 0) {
+        compact_kernel<<<dim3(n_tiles, group), kReduceThreads, 0, e->stream>>>(
+            (const double*)e->s1.p, (const double*)e->s2.p, n_vox, n_tiles, truncation,
+            e->d_colmax, (const unsigned long long*)e->tile_offsets.p, (long long*)e->out_idx.p,
+            (double*)e->out_dose.p, (double*)e->out_sigma.p);
+        PMC_CUDA(e, cudaGetLastError());
+    }
+    e->counters.reduce_launches += nnz > 0 ? 3 : 2;
+    const size_t old = e->dij_indices.size();
+    e->dij_indices.resize(old + nnz);
+    e->dij_dose.resize(old + nnz);
+    e->dij_sigma.resize(old + nnz);
+    if (nnz > 0) {
+        PMC_CUDA(e, cudaMemcpyAsync(e->dij_indices.data() + old, e->out_idx.p, sizeof(long long) * nnz, cudaMemcpyDeviceToHost, e->stream));
+        e->d2h_bytes += (unsigned long long)(sizeof(long long) * nnz);
+        PMC_CUDA(e, cudaMemcpyAsync(e->dij_dose.data() + old, e->out_dose.p, sizeof(double) * nnz, cudaMemcpyDeviceToHost, e->stream));
+        e->d2h_bytes += (unsigned long long)(sizeof(double) * nnz);
+        PMC_CUDA(e, cudaMemcpyAsync(e->dij_sigma.data() + old, e->out_sigma.p, sizeof(double) * nnz, cudaMemcpyDeviceToHost, e->stream));
+        e->d2h_bytes += (unsigned long long)(sizeof(double) * nnz);
+        PMC_CUDA(e, cudaStreamSynchronize(e->stream));
+    }
+    for (int c = 0; c < group; ++c) e->dij_indptr.push_back(e->dij_indptr.back() + counts[c]);
+    return PMC_OK;
+}
+
+int ensure_dense(pmc_engine* e, long long n_entries) {
+    const size_t b = sizeof(double) * (size_t)n_entries;
+    int rc = ensure(e, e->edep, b);
+    if (!rc) rc = ensure(e, e->s1, b);
+    if (!rc) rc = ensure(e, e->s2, b);
+    return rc;
+}
+
+int reset_counters(pmc_engine* e) {
+    std::memset(&e->counters, 0, sizeof e->counters);
+    PMC_CUDA(e, cudaMemsetAsync(e->d_counters, 0, sizeof(Counters), e->stream));
+    PMC_CUDA(e, cudaMemsetAsync(e->d_sched, 0, sizeof(Sched), e->stream));
+    return PMC_OK;
+}
+
+int finish_counters(pmc_engine* e, pmc_books* books) {
+    Counters c{};
+    Sched s{};
+    PMC_CUDA(e, cudaMemcpyAsync(&c, e->d_counters, sizeof c, cudaMemcpyDeviceToHost, e->stream));
+        e->d2h_bytes += (unsigned long long)(sizeof c);
+    PMC_CUDA(e, cudaMemcpyAsync(&s, e->d_sched, sizeof s, cudaMemcpyDeviceToHost, e->stream));
+        e->d2h_bytes += (unsigned long long)(sizeof s);
+    PMC_CUDA(e, cudaStreamSynchronize(e->stream));
+    e->counters.rounds = s.total_rounds;
+    e->counters.kernel_launches += 2 * s.total_rounds + e->counters.reduce_launches;
+    e->counters.photon_flights = (int64_t)c.flights;
+    e->counters.photon_interactions = (int64_t)c.interactions;
+    e->counters.electron_substeps = (int64_t)c.substeps;
+    e->counters.deposits = (int64_t)c.deposits;
+    e->counters.queue_pushes = (int64_t)c.pushes;
+    e->counters.primaries = (int64_t)c.primaries;
+    if (books) {
+        books->escaped = c.escaped;
+        books->unscored = c.unscored;
+        books->emitted = c.emitted;
+        books->majorant_violations = c.violations;
+        if (c.deposited != 0) books->deposited = c.deposited;  // dose-to-water physical book
+    }
+    if (c.violations != 0)
+        return fail(e, PMC_ERR_MAJORANT,
+                    "Woodcock majorant violated in the kernel despite table headroom. The geometry "
+                    "contains material or density the majorant declaration did not cover.");
+    return PMC_OK;
+}
+
+int upload_f32(pmc_engine* e, const std::vector<float>& v, const float** out) {
+    return upload_vec(e, v, out);
+}
+
+int fill_gen_spectrum(pmc_engine* e, GenDesc& G, int n_bins, const double* edges,
+                      const double* cdf) {
+    if (n_bins < 1 || !edges || !cdf) return fail(e, PMC_ERR_INVALID, "spectral source without a spectrum");
+    std::vector<float> ed(edges, edges + n_bins + 1), cd(cdf, cdf + n_bins);
+    G.n_bins = n_bins;
+    int rc = upload_f32(e, ed, &G.edges);
+    if (!rc) rc = upload_f32(e, cd, &G.cdf);
+    return rc;
+}
+
+}  // namespace
+
+// ============================================================================
+// C-ABI
+// ============================================================================
+extern "C" {
+
+int pmc_abi_version(void) { return PMC_ABI_VERSION; }
+
+int pmc_device_count(void) {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) return 0;
+    return n;
+}
+
+int pmc_create(pmc_engine** out, int device_ordinal) {
+    if (!out) return PMC_ERR_INVALID;
+    *out = nullptr;
+    pmc_engine* e = new pmc_engine();
+    e->device = device_ordinal;
+    cudaError_t st = cudaSetDevice(device_ordinal);
+    if (st == cudaSuccess) st = cudaStreamCreateWithFlags(&e->own_stream, cudaStreamNonBlocking);
+    e->stream = e->own_stream;
+    if (st == cudaSuccess) st = cudaDeviceGetAttribute(&e->sm_count, cudaDevAttrMultiProcessorCount, device_ordinal);
+    if (st == cudaSuccess) st = cudaMalloc(&e->d_sched, sizeof(Sched));
+    if (st == cudaSuccess) st = cudaMalloc(&e->d_counters, sizeof(Counters));
+    if (st == cudaSuccess) st = cudaMalloc(&e->d_gen, sizeof(GenDesc));
+    if (st == cudaSuccess) st = cudaMalloc(&e->d_total_q, sizeof(unsigned long long));
+    if (st == cudaSuccess) st = cudaMalloc(&e->d_nnz, sizeof(unsigned long long));
+    for (int i = 0; i < 4 && st == cudaSuccess; ++i) st = cudaEventCreate(&e->ev[i]);
+    if (st != cudaSuccess) {
+        pmc_destroy(e);
+        return PMC_ERR_CUDA;
+    }
+    *out = e;
+    return PMC_OK;
+}
+
+void pmc_destroy(pmc_engine* e) {
+    if (!e) return;
+    cudaSetDevice(e->device);
+    if (e->stream) cudaStreamSynchronize(e->stream);
+    destroy_graph(e);
+    free_run_allocs(e);
+    free_tables(e);
+    if (e->d_gs4) cudaFree(e->d_gs4);
+    if (e->d_vox) cudaFree(e->d_vox);
+    if (e->d_mass) cudaFree(e->d_mass);
+    for (DevBuf* b : {&e->q[0], &e->q[1], &e->q[2], &e->q[3], &e->edep, &e->s1, &e->s2,
+                      &e->tile_counts, &e->tile_offsets, &e->col_counts, &e->out_idx,
+                      &e->out_dose, &e->out_sigma, &e->col_nhist})
+        if (b->p) cudaFree(b->p);
+    for (void* p : {(void*)e->d_sched, (void*)e->d_counters, (void*)e->d_gen,
+                    (void*)e->d_total_q, (void*)e->d_colmax, (void*)e->d_nnz})
+        if (p) cudaFree(p);
+    for (cudaEvent_t ev : e->ev)
+        if (ev) cudaEventDestroy(ev);
+    if (e->own_stream) cudaStreamDestroy(e->own_stream);
+    delete e;
+}
+
+const char* pmc_last_error(const pmc_engine* e) { return e ? e->error.c_str() : "no engine"; }
+
+int pmc_upload_grid(pmc_engine* e, int32_t nx, int32_t ny, int32_t nz, const double origin[3],
+                    const double spacing[3], const float* density, const uint8_t* material) {
+    if (!e) return PMC_ERR_INVALID;
+    if (nx < 1 || ny < 1 || nz < 1) return fail(e, PMC_ERR_INVALID, "empty grid shape");
+    if (!origin || !spacing || !density || !material) return fail(e, PMC_ERR_INVALID, "null grid array");
+    for (int i = 0; i < 3; ++i)
+        if (!(spacing[i] > 0.0)) return fail(e, PMC_ERR_INVALID, "non-positive spacing");
+    PMC_CUDA(e, cudaSetDevice(e->device));
+    const long long n = (long long)nx * ny * nz;
+    std::vector<float2> vox((size_t)n);
+    e->default_mass.resize((size_t)n);
+    const double volume = spacing[0] * spacing[1] * spacing[2];
+    int max_mat = 0;
+    for (long long i = 0; i < n; ++i) {
+        if (!(density[i] > 0.0f)) return fail(e, PMC_ERR_INVALID, "non-positive voxel density; vacuum is not supported");
+        max_mat = std::max(max_mat, (int)material[i]);
+        vox[i].x = density[i];
+        int m = material[i];
+        std::memcpy(&vox[i].y, &m, sizeof(float));
+        e->default_mass[i] = (double)density[i] * volume;
+    }
+    if (e->d_vox) cudaFree(e->d_vox);
+    e->d_vox = nullptr;
+    PMC_CUDA(e, cudaMalloc(&e->d_vox, sizeof(float2) * n));
+    PMC_CUDA(e, cudaMemcpy(e->d_vox, vox.data(), sizeof(float2) * n, cudaMemcpyHostToDevice));
+    e->h2d_bytes += (unsigned long long)(sizeof(float2) * n);
+    e->gi = make_grid(nx, ny, nz, origin, spacing);
+    e->has_grid = true;
+    e->max_material = max_mat;
+    if (!e->custom_scoring) {
+        e->si = e->gi;
+        if (e->d_mass) cudaFree(e->d_mass);
+        e->d_mass = nullptr;
+        PMC_CUDA(e, cudaMalloc(&e->d_mass, sizeof(double) * n));
+        PMC_CUDA(e, cudaMemcpy(e->d_mass, e->default_mass.data(), sizeof(double) * n, cudaMemcpyHostToDevice));
+    e->h2d_bytes += (unsigned long long)(sizeof(double) * n);
+        e->mass_len = n;
+    }
+    return PMC_OK;
+}
+
+int pmc_set_scoring(pmc_engine* e, const pmc_scoring_desc* s) {
+    if (!e) return PMC_ERR_INVALID;
+    if (!e->has_grid) return fail(e, PMC_ERR_STATE, "upload the transport grid first");
+    PMC_CUDA(e, cudaSetDevice(e->device));
+    if (!s) {
+        e->custom_scoring = false;
+        e->si = e->gi;
+        const long long n = e->gi.n_voxels;
+        if (e->d_mass) cudaFree(e->d_mass);
+        e->d_mass = nullptr;
+        PMC_CUDA(e, cudaMalloc(&e->d_mass, sizeof(double) * n));
+        PMC_CUDA(e, cudaMemcpy(e->d_mass, e->default_mass.data(), sizeof(double) * n, cudaMemcpyHostToDevice));
+    e->h2d_bytes += (unsigned long long)(sizeof(double) * n);
+        e->mass_len = n;
+        return PMC_OK;
+    }
+    if (s->nx < 1 || s->ny < 1 || s->nz < 1 || !s->voxel_mass)
+        return fail(e, PMC_ERR_INVALID, "invalid scoring grid");
+    const long long n = (long long)s->nx * s->ny * s->nz;
+    if (e->d_mass) cudaFree(e->d_mass);
+    e->d_mass = nullptr;
+    PMC_CUDA(e, cudaMalloc(&e->d_mass, sizeof(double) * n));
+    PMC_CUDA(e, cudaMemcpy(e->d_mass, s->voxel_mass, sizeof(double) * n, cudaMemcpyHostToDevice));
+    e->h2d_bytes += (unsigned long long)(sizeof(double) * n);
+    e->mass_len = n;
+    e->si = make_grid(s->nx, s->ny, s->nz, s->origin, s->spacing);
+    e->custom_scoring = true;
+    return PMC_OK;
+}
+
+int pmc_upload_tables(pmc_engine* e, const pmc_tables_desc* t) {
+    if (!e || !t) return PMC_ERR_INVALID;
+    const int M = t->n_materials, N = t->n_points;
+    if (M < 1 || M > 256) return fail(e, PMC_ERR_INVALID, "the B200 backend addresses 1..256 materials (uint8 voxel map); got %d", M);
+    if (N < 2) return fail(e, PMC_ERR_INVALID, "need at least two table nodes");
+    const double* req[] = {t->mu_compton, t->mu_photo, t->mu_pair, t->mu_rayleigh, t->majorant,
+                           t->stopping_restricted, t->stopping_radiative, t->moller,
+                           t->csda_range, t->scattering_power, t->log_eta, t->restricted_range,
+                           t->energy_of_restricted_range};
+    for (const double* a : req)
+        if (!a) return fail(e, PMC_ERR_INVALID, "null table array");
+    PMC_CUDA(e, cudaSetDevice(e->device));
+    free_tables(e);
+    const size_t MN = (size_t)M * N;
+    std::vector<float4> ch(MN), ea(MN);
+    std::vector<float2> eb(MN);
+    std::vector<float> maj(N), ec(MN), er(MN);
+    for (size_t i = 0; i < MN; ++i) {
+        ch[i] = make_float4((float)t->mu_compton[i], (float)t->mu_photo[i], (float)t->mu_pair[i],
+                            (float)t->mu_rayleigh[i]);
+        ea[i] = make_float4((float)t->csda_range[i], (float)t->moller[i],
+                            (float)t->restricted_range[i], (float)t->stopping_radiative[i]);
+        eb[i] = make_float2((float)t->scattering_power[i], (float)t->log_eta[i]);
+        ec[i] = (float)t->stopping_restricted[i];
+        er[i] = (float)t->energy_of_restricted_range[i];
+    }
+    for (int i = 0; i < N; ++i) maj[i] = (float)t->majorant[i];
+    auto put = [&](const void* src, size_t bytes, const void** dst) -> int {
+        void* p = nullptr;
+        PMC_CUDA(e, cudaMalloc(&p, std::max<size_t>(bytes, 16)));
+        PMC_CUDA(e, cudaMemcpy(p, src, bytes, cudaMemcpyHostToDevice));
+    e->h2d_bytes += (unsigned long long)(bytes);
+        e->table_allocs.push_back(p);
+        *dst = p;
+        return PMC_OK;
+    };
+    Tables T{};
+    int rc = put(ch.data(), sizeof(float4) * MN, (const void**)&T.ch);
+    if (!rc) rc = put(maj.data(), sizeof(float) * N, (const void**)&T.maj);
+    if (!rc) rc = put(ea.data(), sizeof(float4) * MN, (const void**)&T.ea);
+    if (!rc) rc = put(eb.data(), sizeof(float2) * MN, (const void**)&T.eb);
+    if (!rc) rc = put(ec.data(), sizeof(float) * MN, (const void**)&T.ec);
+    if (!rc) rc = put(er.data(), sizeof(float) * MN, (const void**)&T.er);
+    if (rc) return rc;
+    const int NC = t->n_coherent;
+    std::vector<float> cx(std::max(NC, 2), 0.0f), cc((size_t)M * std::max(NC, 2), 0.0f);
+    if (NC >= 2 && t->coherent_x && t->coherent_cumulative) {
+        for (int i = 0; i < NC; ++i) cx[i] = (float)t->coherent_x[i];
+        for (size_t i = 0; i < (size_t)M * NC; ++i) cc[i] = (float)t->coherent_cumulative[i];
+        T.n_coherent = NC;
+    } else {
+        cx[1] = 1.0f;
+        T.n_coherent = 2;
+    }
+    rc = put(cx.data(), sizeof(float) * cx.size(), (const void**)&T.coh_x);
+    if (!rc) rc = put(cc.data(), sizeof(float) * cc.size(), (const void**)&T.coh_cum);
+    if (rc) return rc;
+    T.n_points = N;
+    T.n_materials = M;
+    T.p_log_min = (float)t->photon_log_e_min;
+    T.p_inv_dlog = (float)t->photon_inv_dlog;
+    T.e_log_min = (float)t->electron_log_e_min;
+    T.e_inv_dlog = (float)t->electron_inv_dlog;
+    T.r_log_min = (float)t->range_log_r_min;
+    T.r_inv_dlog = (float)t->range_inv_dlog;
+    // keep the GS part of an earlier upload
+    T.gs4 = e->tab.gs4;
+    T.gs_ix0 = e->tab.gs_ix0;
+    T.gs_iy0 = e->tab.gs_iy0;
+    T.gs_n_eta = e->tab.gs_n_eta;
+    T.gs_n_theta2 = e->tab.gs_n_theta2;
+    T.gs_n_u = e->tab.gs_n_u;
+    T.gs_bins_per_log = e->tab.gs_bins_per_log;
+    e->tab = T;
+    e->has_tables = true;
+    return PMC_OK;
+}
+
+int pmc_upload_gs(pmc_engine* e, const float* values, int32_t ix0, int32_t iy0, int32_t n_eta,
+                  int32_t n_theta2, int32_t n_u, double bins_per_log) {
+    if (!e) return PMC_ERR_INVALID;
+    if (!values || n_eta < 2 || n_theta2 < 2 || n_u < 1 || !(bins_per_log > 0.0))
+        return fail(e, PMC_ERR_INVALID, "invalid Goudsmit-Saunderson grid");
+    PMC_CUDA(e, cudaSetDevice(e->device));
+    const size_t cells = (size_t)(n_eta - 1) * (n_theta2 - 1) * n_u;
+    std::vector<float4> g4(cells);
+    auto at = [&](int i, int j, int u) { return values[((size_t)i * n_theta2 + j) * n_u + u]; };
+    for (int i = 0; i < n_eta - 1; ++i)
+        for (int j = 0; j < n_theta2 - 1; ++j)
+            for (int u = 0; u < n_u; ++u)
+                g4[((size_t)i * (n_theta2 - 1) + j) * n_u + u] =
+                    make_float4(at(i, j, u), at(i + 1, j, u), at(i, j + 1, u), at(i + 1, j + 1, u));
+    if (e->d_gs4) cudaFree(e->d_gs4);
+    e->d_gs4 = nullptr;
+    PMC_CUDA(e, cudaMalloc(&e->d_gs4, sizeof(float4) * cells));
+    PMC_CUDA(e, cudaMemcpy(e->d_gs4, g4.data(), sizeof(float4) * cells, cudaMemcpyHostToDevice));
+    e->h2d_bytes += (unsigned long long)(sizeof(float4) * cells);
+    e->tab.gs4 = e->d_gs4;
+    e->tab.gs_ix0 = ix0;
+    e->tab.gs_iy0 = iy0;
+    e->tab.gs_n_eta = n_eta;
+    e->tab.gs_n_theta2 = n_theta2;
+    e->tab.gs_n_u = n_u;
+    e->tab.gs_bins_per_log = (float)bins_per_log;
+    e->has_gs = true;
+    return PMC_OK;
+}
+
+int pmc_run_forward(pmc_engine* e, const pmc_source_desc* src, const pmc_run_params* p,
+                    double* dose, double* dose_sigma, pmc_books* books) {
+    if (!e || !src || !p || !dose || !dose_sigma) return PMC_ERR_INVALID;
+    PMC_CUDA(e, cudaSetDevice(e->device));
+    if (p->n_histories < 1) return fail(e, PMC_ERR_INVALID, "need at least one history, got %lld", (long long)p->n_histories);
+    if (p->n_batches < 1 || p->n_histories % p->n_batches != 0)
+        return fail(e, PMC_ERR_INVALID, "n_histories=%lld not divisible by n_batches=%d", (long long)p->n_histories, p->n_batches);
+    RunPlan plan;
+    int rc = prepare_transport(e, p, &plan);
+    if (rc) return rc;
+    const long long n_vox = e->si.n_voxels;
+    rc = ensure_dense(e, n_vox);
+    if (rc) return rc;
+    rc = ensure(e, e->col_nhist, sizeof(double));
+    if (rc) return rc;
+    free_run_allocs(e);
+
+    const long long per_batch = p->n_histories / p->n_batches;
+    GenDesc G{};
+    G.forward = 1;
+    G.group = 1;
+    G.kind = src->kind;
+    G.per_batch_fwd = per_batch;
+    G.energy = (float)src->energy;
+    std::vector<float> z1(1, 0.0f);
+    switch (src->type) {
+        case PMC_SRC_PENCIL:
+            G.type = 0;
+            G.px = (float)src->position[0]; G.py = (float)src->position[1]; G.pz = (float)src->position[2];
+            G.dx = (float)src->direction[0]; G.dy = (float)src->direction[1]; G.dz = (float)src->direction[2];
+            break;
+        case PMC_SRC_PARALLEL: {
+            G.type = 1;
+            G.z0 = (float)src->z0;
+            std::vector<float> a(1, (float)src->x_lo), b(1, (float)src->x_extent),
+                c(1, (float)src->y_lo), d(1, (float)src->y_extent);
+            rc = upload_f32(e, a, &G.x_lo);
+            if (!rc) rc = upload_f32(e, b, &G.x_ext);
+            if (!rc) rc = upload_f32(e, c, &G.y_lo);
+            if (!rc) rc = upload_f32(e, d, &G.y_ext);
+            break;
+        }
+        case PMC_SRC_SPECTRAL: {
+            G.type = 2;
+            G.kind = PMC_PHOTON;
+            G.book_emitted = 1;
+            G.fx = (float)src->focal[0]; G.fy = (float)src->focal[1]; G.fz = (float)src->focal[2];
+            G.uax = (float)src->u_axis[0]; G.uay = (float)src->u_axis[1]; G.uaz = (float)src->u_axis[2];
+            G.vax = (float)src->v_axis[0]; G.vay = (float)src->v_axis[1]; G.vaz = (float)src->v_axis[2];
+            G.width_u = (float)src->width_u;
+            G.width_v = (float)src->width_v;
+            std::vector<float> cx(1, (float)src->center[0]), cy(1, (float)src->center[1]),
+                cz(1, (float)src->center[2]);
+            rc = upload_f32(e, cx, &G.cx);
+            if (!rc) rc = upload_f32(e, cy, &G.cy);
+            if (!rc) rc = upload_f32(e, cz, &G.cz);
+            if (!rc) rc = fill_gen_spectrum(e, G, src->n_bins, src->edges, src->cdf);
+            break;
+        }
+        case PMC_SRC_UPLOAD: {
+            G.type = 3;
+            G.book_emitted = 1;
+            if (!src->up_kind || !src->up_energy || !src->up_pos || !src->up_dir || !src->up_weight)
+                return fail(e, PMC_ERR_INVALID, "upload source without records");
+            const size_t n = (size_t)p->n_histories;
+            std::vector<int> k(src->up_kind, src->up_kind + n);
+            std::vector<float> en(src->up_energy, src->up_energy + n), ps(src->up_pos, src->up_pos + 3 * n),
+                dr(src->up_dir, src->up_dir + 3 * n), w(src->up_weight, src->up_weight + n);
+            for (size_t i = 0; i < n; ++i)
+                if (k[i] < 0 || k[i] > 2) return fail(e, PMC_ERR_INVALID, "bad particle kind in upload");
+            rc = upload_vec(e, k, &G.up_kind);
+            if (!rc) rc = upload_f32(e, en, &G.up_energy);
+            if (!rc) rc = upload_f32(e, ps, &G.up_pos);
+            if (!rc) rc = upload_f32(e, dr, &G.up_dir);
+            if (!rc) rc = upload_f32(e, w, &G.up_weight);
+            break;
+        }
+        default:
+            return fail(e, PMC_ERR_INVALID, "unknown source type %d", src->type);
+    }
+    if (rc) return rc;
+    if (G.kind != PMC_PHOTON && G.kind != PMC_ELECTRON && G.type != 3)
+        return fail(e, PMC_ERR_INVALID, "unknown primary kind %d", G.kind);
+    PMC_CUDA(e, cudaMemcpy(e->d_gen, &G, sizeof G, cudaMemcpyHostToDevice));
+    e->h2d_bytes += (unsigned long long)(sizeof G);
+    const double nh = (double)per_batch;
+    PMC_CUDA(e, cudaMemcpy(e->col_nhist.p, &nh, sizeof nh, cudaMemcpyHostToDevice));
+    e->h2d_bytes += (unsigned long long)(sizeof nh);
+
+    rc = reset_counters(e);
+    if (rc) return rc;
+    PMC_CUDA(e, cudaMemsetAsync(e->edep.p, 0, sizeof(double) * n_vox, e->stream));
+    PMC_CUDA(e, cudaMemsetAsync(e->s1.p, 0, sizeof(double) * n_vox, e->stream));
+    PMC_CUDA(e, cudaMemsetAsync(e->s2.p, 0, sizeof(double) * n_vox, e->stream));
+    PMC_CUDA(e, cudaMemsetAsync(e->d_total_q, 0, sizeof(unsigned long long), e->stream));
+    TransportParams P = make_params(e, p, plan);
+    float t_tr = 0.0f, t_red = 0.0f;
+    for (int b = 0; b < p->n_batches; ++b) {
+        PMC_CUDA(e, cudaEventRecord(e->ev[0], e->stream));
+        rc = run_batch(e, p, plan, P, b, (unsigned long long)per_batch);
+        if (rc) return rc;
+        PMC_CUDA(e, cudaEventRecord(e->ev[1], e->stream));
+        rc = launch_fold(e, n_vox, 1, (const double*)e->col_nhist.p);
+        if (rc) return rc;
+        PMC_CUDA(e, cudaEventRecord(e->ev[2], e->stream));
+        PMC_CUDA(e, cudaEventSynchronize(e->ev[2]));
+        float a = 0, c = 0;
+        cudaEventElapsedTime(&a, e->ev[0], e->ev[1]);
+        cudaEventElapsedTime(&c, e->ev[1], e->ev[2]);
+        t_tr += a;
+        t_red += c;
+        Sched s;
+        rc = read_sched(e, &s);
+        if (rc) return rc;
+        rc = check_flags(e, s);
+        if (rc) return rc;
+        if (e->progress) e->progress(e->progress_user, per_batch);
+    }
+    PMC_CUDA(e, cudaEventRecord(e->ev[0], e->stream));
+    rc = launch_finalize(e, n_vox, 1, p->n_batches);
+    if (rc) return rc;
+    PMC_CUDA(e, cudaEventRecord(e->ev[1], e->stream));
+    PMC_CUDA(e, cudaMemcpyAsync(dose, e->s1.p, sizeof(double) * n_vox, cudaMemcpyDeviceToHost, e->stream));
+        e->d2h_bytes += (unsigned long long)(sizeof(double) * n_vox);
+    PMC_CUDA(e, cudaMemcpyAsync(dose_sigma, e->s2.p, sizeof(double) * n_vox, cudaMemcpyDeviceToHost, e->stream));
+        e->d2h_bytes += (unsigned long long)(sizeof(double) * n_vox);
+    unsigned long long total_q = 0;
+    PMC_CUDA(e, cudaMemcpyAsync(&total_q, e->d_total_q, sizeof total_q, cudaMemcpyDeviceToHost, e->stream));
+        e->d2h_bytes += (unsigned long long)(sizeof total_q);
+    PMC_CUDA(e, cudaStreamSynchronize(e->stream));
+    float c = 0;
+    cudaEventElapsedTime(&c, e->ev[0], e->ev[1]);
+    e->counters.transport_ms = t_tr;
+    e->counters.reduce_ms = t_red + c;
+    if (books) {
+        std::memset(books, 0, sizeof *books);
+        books->deposited = (int64_t)total_q;
+    }
+    return finish_counters(e, books);
+}
+
+int pmc_run_dij(pmc_engine* e, const pmc_beamlet_desc* src, const int64_t* counts,
+                const pmc_run_params* p, int64_t* nnz_out, pmc_books* books) {
+    if (!e || !src || !counts || !p || !nnz_out) return PMC_ERR_INVALID;
+    PMC_CUDA(e, cudaSetDevice(e->device));
+    const int n_beam = src->n_beamlets;
+    if (n_beam < 1) return fail(e, PMC_ERR_INVALID, "need at least one beamlet");
+    if (p->n_batches < 1) return fail(e, PMC_ERR_INVALID, "need at least one batch");
+    for (int j = 0; j < n_beam; ++j) {
+        if (counts[j] < 1) return fail(e, PMC_ERR_INVALID, "need at least one history per beamlet, got %lld", (long long)counts[j]);
+        if (counts[j] % p->n_batches != 0)
+            return fail(e, PMC_ERR_INVALID, "n_histories_per_beamlet=%lld not divisible by n_batches=%d", (long long)counts[j], p->n_batches);
+    }
+    if (p->truncation < 0.0) return fail(e, PMC_ERR_INVALID, "negative truncation %g", p->truncation);
+    RunPlan plan;
+    int rc = prepare_transport(e, p, &plan);
+    if (rc) return rc;
+    const long long n_vox = e->si.n_voxels;
+    int group = p->beamlet_group_size > 0 ? p->beamlet_group_size : 0;
+    if (group == 0) {
+        // Auto: the largest group whose dense maps (int64 quanta + two float64
+        // sums = 24 bytes per entry) fit half of the free memory.
+        size_t free_b = 0, total_b = 0;
+        PMC_CUDA(e, cudaMemGetInfo(&free_b, &total_b));
+        const double budget = 0.5 * (double)free_b;
+        group = (int)std::max(1.0, std::floor(budget / (24.0 * (double)n_vox)));
+        group = std::min(group, std::min(n_beam, 4096));
+    }
+    group = std::min(group, n_beam);
+    rc = ensure_dense(e, n_vox * group);
+    if (!rc) rc = ensure(e, e->col_nhist, sizeof(double) * group);
+    if (rc) return rc;
+    if (src->type != PMC_BEAMLET_LATTICE && src->type != PMC_BEAMLET_SPECTRAL)
+        return fail(e, PMC_ERR_INVALID, "unknown beamlet source type %d", src->type);
+
+    std::vector<long long> offset(n_beam);
+    long long acc = 0;
+    for (int j = 0; j < n_beam; ++j) {
+        offset[j] = src->history_offsets ? src->history_offsets[j] : acc;
+        if (offset[j] < 0) return fail(e, PMC_ERR_INVALID, "negative history offset");
+        acc += counts[j];
+    }
+    rc = reset_counters(e);
+    if (rc) return rc;
+    PMC_CUDA(e, cudaMemsetAsync(e->d_total_q, 0, sizeof(unsigned long long), e->stream));
+    e->dij_indptr.assign(1, 0);
+    e->dij_indices.clear();
+    e->dij_dose.clear();
+    e->dij_sigma.clear();
+    float t_tr = 0.0f, t_red = 0.0f;
+
+    for (int g0 = 0; g0 < n_beam; g0 += group) {
+        const int gs = std::min(group, n_beam - g0);
+        free_run_allocs(e);
+        GenDesc G{};
+        G.forward = 0;
+        G.group = gs;
+        G.correlated = p->correlated ? 1 : 0;
+        G.kind = PMC_PHOTON;
+        std::vector<long long> pb(gs), pre(gs + 1, 0), off(gs);
+        std::vector<double> nh(gs);
+        for (int k = 0; k < gs; ++k) {
+            pb[k] = counts[g0 + k] / p->n_batches;
+            pre[k + 1] = pre[k] + pb[k];
+            off[k] = offset[g0 + k];
+            nh[k] = (double)pb[k];
+        }
+        rc = upload_vec(e, pb, &G.per_batch);
+        if (!rc) rc = upload_vec(e, pre, &G.pb_prefix);
+        if (!rc) rc = upload_vec(e, off, &G.hist_offset);
+        if (rc) return rc;
+        if (src->type == PMC_BEAMLET_LATTICE) {
+            if (!src->x_lo || !src->x_extent || !src->y_lo || !src->y_extent)
+                return fail(e, PMC_ERR_INVALID, "lattice source without bounds");
+            G.type = 1;
+            G.energy = (float)src->energy;
+            G.z0 = (float)src->z0;
+            std::vector<float> a(gs), b(gs), c(gs), d(gs);
+            for (int k = 0; k < gs; ++k) {
+                a[k] = (float)src->x_lo[g0 + k];
+                b[k] = (float)src->x_extent[g0 + k];
+                c[k] = (float)src->y_lo[g0 + k];
+                d[k] = (float)src->y_extent[g0 + k];
+            }
+            rc = upload_f32(e, a, &G.x_lo);
+            if (!rc) rc = upload_f32(e, b, &G.x_ext);
+            if (!rc) rc = upload_f32(e, c, &G.y_lo);
+            if (!rc) rc = upload_f32(e, d, &G.y_ext);
+        } else {
+            if (!src->centers) return fail(e, PMC_ERR_INVALID, "spectral beamlets without centres");
+            G.type = 2;
+            G.book_emitted = 1;
+            G.fx = (float)src->focal[0]; G.fy = (float)src->focal[1]; G.fz = (float)src->focal[2];
+            G.uax = (float)src->u_axis[0]; G.uay = (float)src->u_axis[1]; G.uaz = (float)src->u_axis[2];
+            G.vax = (float)src->v_axis[0]; G.vay = (float)src->v_axis[1]; G.vaz = (float)src->v_axis[2];
+            G.width_u = (float)src->width_u;
+            G.width_v = (float)src->width_v;
+            std::vector<float> cx(gs), cy(gs), cz(gs);
+            for (int k = 0; k < gs; ++k) {
+                cx[k] = (float)src->centers[3 * (g0 + k)];
+                cy[k] = (float)src->centers[3 * (g0 + k) + 1];
+                cz[k] = (float)src->centers[3 * (g0 + k) + 2];
+            }
+            rc = upload_f32(e, cx, &G.cx);
+            if (!rc) rc = upload_f32(e, cy, &G.cy);
+            if (!rc) rc = upload_f32(e, cz, &G.cz);
+            if (!rc) rc = fill_gen_spectrum(e, G, src->n_bins, src->edges, src->cdf);
+        }
+        if (rc) return rc;
+        PMC_CUDA(e, cudaMemcpy(e->d_gen, &G, sizeof G, cudaMemcpyHostToDevice));
+    e->h2d_bytes += (unsigned long long)(sizeof G);
+        PMC_CUDA(e, cudaMemcpy(e->col_nhist.p, nh.data(), sizeof(double) * gs, cudaMemcpyHostToDevice));
+    e->h2d_bytes += (unsigned long long)(sizeof(double) * gs);
+        const long long span = n_vox * gs;
+        PMC_CUDA(e, cudaMemsetAsync(e->edep.p, 0, sizeof(double) * span, e->stream));
+        PMC_CUDA(e, cudaMemsetAsync(e->s1.p, 0, sizeof(double) * span, e->stream));
+        PMC_CUDA(e, cudaMemsetAsync(e->s2.p, 0, sizeof(double) * span, e->stream));
+        TransportParams P = make_params(e, p, plan);
+        for (int b = 0; b < p->n_batches; ++b) {
+            PMC_CUDA(e, cudaEventRecord(e->ev[0], e->stream));
+            rc = run_batch(e, p, plan, P, b, (unsigned long long)pre[gs]);
+            if (rc) return rc;
+            PMC_CUDA(e, cudaEventRecord(e->ev[1], e->stream));
+            rc = launch_fold(e, n_vox, gs, (const double*)e->col_nhist.p);
+            if (rc) return rc;
+            PMC_CUDA(e, cudaEventRecord(e->ev[2], e->stream));
+            PMC_CUDA(e, cudaEventSynchronize(e->ev[2]));
+            float a = 0, c = 0;
+            cudaEventElapsedTime(&a, e->ev[0], e->ev[1]);
+            cudaEventElapsedTime(&c, e->ev[1], e->ev[2]);
+            t_tr += a;
+            t_red += c;
+        }
+        Sched s;
+        rc = read_sched(e, &s);
+        if (rc) return rc;
+        rc = check_flags(e, s);
+        if (rc) return rc;
+        PMC_CUDA(e, cudaEventRecord(e->ev[0], e->stream));
+        rc = launch_finalize(e, n_vox, gs, p->n_batches);
+        if (!rc) rc = truncate_group(e, n_vox, gs, p->truncation);
+        if (rc) return rc;
+        PMC_CUDA(e, cudaEventRecord(e->ev[1], e->stream));
+        PMC_CUDA(e, cudaEventSynchronize(e->ev[1]));
+        float c = 0;
+        cudaEventElapsedTime(&c, e->ev[0], e->ev[1]);
+        t_red += c;
+        if (e->progress) {
+            long long done = 0;
+            for (int k = 0; k < gs; ++k) done += counts[g0 + k];
+            e->progress(e->progress_user, done);
+        }
+    }
+    free_run_allocs(e);
+    unsigned long long total_q = 0;
+    PMC_CUDA(e, cudaMemcpyAsync(&total_q, e->d_total_q, sizeof total_q, cudaMemcpyDeviceToHost, e->stream));
+        e->d2h_bytes += (unsigned long long)(sizeof total_q);
+    PMC_CUDA(e, cudaStreamSynchronize(e->stream));
+    e->counters.transport_ms = t_tr;
+    e->counters.reduce_ms = t_red;
+    *nnz_out = (int64_t)e->dij_indices.size();
+    if (books) {
+        std::memset(books, 0, sizeof *books);
+        books->deposited = (int64_t)total_q;
+    }
+    return finish_counters(e, books);
+}
+
+int pmc_dij_fetch(pmc_engine* e, int64_t* indptr, int64_t* indices, double* dose, double* sigma) {
+    if (!e || !indptr) return PMC_ERR_INVALID;
+    const size_t nnz = e->dij_indices.size();
+    std::memcpy(indptr, e->dij_indptr.data(), sizeof(int64_t) * e->dij_indptr.size());
+    if (nnz) {
+        if (!indices || !dose || !sigma) return fail(e, PMC_ERR_INVALID, "null CSC buffer");
+        std::memcpy(indices, e->dij_indices.data(), sizeof(int64_t) * nnz);
+        std::memcpy(dose, e->dij_dose.data(), sizeof(double) * nnz);
+        std::memcpy(sigma, e->dij_sigma.data(), sizeof(double) * nnz);
+    }
+    return PMC_OK;
+}
+
+int pmc_set_stream(pmc_engine* e, void* stream) {
+    if (!e) return PMC_ERR_INVALID;
+    PMC_CUDA(e, cudaStreamSynchronize(e->stream));
+    e->stream = stream ? (cudaStream_t)stream : e->own_stream;
+    return PMC_OK;
+}
+
+int pmc_set_progress(pmc_engine* e, pmc_progress_fn fn, void* user) {
+    if (!e) return PMC_ERR_INVALID;
+    e->progress = fn;
+    e->progress_user = user;
+    return PMC_OK;
+}
+
+int pmc_get_counters(const pmc_engine* e, pmc_counters* c) {
+    if (!e || !c) return PMC_ERR_INVALID;
+    *c = e->counters;
+    c->h2d_bytes_total = (int64_t)e->h2d_bytes;
+    c->d2h_bytes_total = (int64_t)e->d2h_bytes;
+    return PMC_OK;
+}
+
+int pmc_reduce_dense(pmc_engine* e, const int64_t* quanta, int32_t n_batches, int32_t n_cols,
+                     int64_t n_vox, const double* voxel_mass, const double* histories_per_batch,
+                     double* mean, double* sigma, int64_t* total_quanta) {
+    if (!e || !quanta || !voxel_mass || !histories_per_batch || !mean || !sigma) return PMC_ERR_INVALID;
+    if (n_batches < 1 || n_cols < 1 || n_vox < 1) return fail(e, PMC_ERR_INVALID, "empty reduction");
+    PMC_CUDA(e, cudaSetDevice(e->device));
+    const long long span = (long long)n_cols * n_vox;
+    int rc = ensure_dense(e, span);
+    if (!rc) rc = ensure(e, e->col_nhist, sizeof(double) * n_cols);
+    if (rc) return rc;
+    // The reduction runs against the given masses, not the engine's scoring grid.
+    double* saved_mass = e->d_mass;
+    double* mass = nullptr;
+    PMC_CUDA(e, cudaMalloc(&mass, sizeof(double) * n_vox));
+    PMC_CUDA(e, cudaMemcpy(mass, voxel_mass, sizeof(double) * n_vox, cudaMemcpyHostToDevice));
+    e->h2d_bytes += (unsigned long long)(sizeof(double) * n_vox);
+    PMC_CUDA(e, cudaMemcpy(e->col_nhist.p, histories_per_batch, sizeof(double) * n_cols, cudaMemcpyHostToDevice));
+    e->h2d_bytes += (unsigned long long)(sizeof(double) * n_cols);
+    e->d_mass = mass;
+    PMC_CUDA(e, cudaMemsetAsync(e->s1.p, 0, sizeof(double) * span, e->stream));
+    PMC_CUDA(e, cudaMemsetAsync(e->s2.p, 0, sizeof(double) * span, e->stream));
+    PMC_CUDA(e, cudaMemsetAsync(e->d_total_q, 0, sizeof(unsigned long long), e->stream));
+    for (int b = 0; b < n_batches && !rc; ++b) {
+        PMC_CUDA(e, cudaMemcpyAsync(e->edep.p, quanta + (size_t)b * span, sizeof(int64_t) * span,
+                                    cudaMemcpyHostToDevice, e->stream));
+        rc = launch_fold(e, n_vox, n_cols, (const double*)e->col_nhist.p);
+    }
+    if (!rc) rc = launch_finalize(e, n_vox, n_cols, n_batches);
+    unsigned long long tq = 0;
+    if (!rc) {
+        cudaMemcpyAsync(mean, e->s1.p, sizeof(double) * span, cudaMemcpyDeviceToHost, e->stream);
+        cudaMemcpyAsync(sigma, e->s2.p, sizeof(double) * span, cudaMemcpyDeviceToHost, e->stream);
+        cudaMemcpyAsync(&tq, e->d_total_q, sizeof tq, cudaMemcpyDeviceToHost, e->stream);
+        cudaStreamSynchronize(e->stream);
+    }
+    e->d_mass = saved_mass;
+    cudaFree(mass);
+    if (total_quanta) *total_quanta = (int64_t)tq;
+    if (rc) return rc;
+    PMC_CUDA(e, cudaGetLastError());
+    return PMC_OK;
+}
+
+int pmc_truncate_dense(pmc_engine* e, const double* mean, const double* sigma, int32_t n_cols,
+                       int64_t n_vox, double truncation, int64_t* counts, int64_t* nnz) {
+    if (!e || !mean || !sigma || !nnz) return PMC_ERR_INVALID;
+    if (n_cols < 1 || n_vox < 1) return fail(e, PMC_ERR_INVALID, "empty truncation");
+    if (truncation < 0.0) return fail(e, PMC_ERR_INVALID, "negative truncation %g", truncation);
+    PMC_CUDA(e, cudaSetDevice(e->device));
+    const long long span = (long long)n_cols * n_vox;
+    int rc = ensure_dense(e, span);
+    if (rc) return rc;
+    PMC_CUDA(e, cudaMemcpy(e->s1.p, mean, sizeof(double) * span, cudaMemcpyHostToDevice));
+    e->h2d_bytes += (unsigned long long)(sizeof(double) * span);
+    PMC_CUDA(e, cudaMemcpy(e->s2.p, sigma, sizeof(double) * span, cudaMemcpyHostToDevice));
+    e->h2d_bytes += (unsigned long long)(sizeof(double) * span);
+    rc = ensure_colmax(e, n_cols);
+    if (rc) return rc;
+    PMC_CUDA(e, cudaMemsetAsync(e->d_colmax, 0, sizeof(unsigned long long) * n_cols, e->stream));
+    {
+        const int n_tiles = (int)((n_vox + kTileVoxels - 1) / kTileVoxels);
+        colmax_kernel<<<dim3(n_tiles, n_cols), kReduceThreads, 0, e->stream>>>(
+            (const double*)e->s1.p, n_vox, e->d_colmax);
+        PMC_CUDA(e, cudaGetLastError());
+    }
+    e->dij_indptr.assign(1, 0);
+    e->dij_indices.clear();
+    e->dij_dose.clear();
+    e->dij_sigma.clear();
+    rc = truncate_group(e, n_vox, n_cols, truncation);
+    if (rc) return rc;
+    if (counts)
+        for (int c = 0; c < n_cols; ++c) counts[c] = e->dij_indptr[c + 1] - e->dij_indptr[c];
+    *nnz = (int64_t)e->dij_indices.size();
+    return PMC_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,707 @@
+"""``B200Engine``: the B200 backend of pyRadMC, a drop-in for ``WarpEngine``.
+
+Same constructor fields and the same ``run`` / ``run_dij`` signatures, argument
+meanings, validation messages and result types as
+``pyradmc/backends/warp/engine.py`` (``WarpEngine``: :369, ``run``: :454,
+``run_dij``: :948).  The work runs in ``libpmc_b200.so`` (hand-written sm_100a
+CUDA behind the C-ABI of ``include/pyradmc_b200.h``); this module validates,
+flattens the host data through the caller's ``CrossSectionSource``, packs the
+call descriptors and wraps the results.  There is no CPU path: without the
+library and a CUDA device every run raises.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import math
+import threading
+from collections import deque
+from concurrent.futures import ThreadPoolExecutor
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from pyradmc_b200 import _lib, model
+
+__all__ = ["B200Engine", "DIJ_TRUNCATION_RELATIVE", "ECUT_MEV", "PCUT_MEV"]
+
+ECUT_MEV = 0.200  # pyradmc/__init__.py:22
+PCUT_MEV = 0.050  # pyradmc/__init__.py:25
+DIJ_TRUNCATION_RELATIVE = 1.0e-3  # pyradmc/__init__.py:28
+ENERGY_QUANTUM_MEV = 1.0e-9  # kernels.py:96
+_E_MAX_MARGIN = 1.0 + 1.0e-6  # engine.py:80
+GS_STEP_ENERGY_FRACTION = 0.20  # transport/electron.py:85
+STEP_ENERGY_FRACTION = 0.05  # transport/electron.py:73
+VERSION = "0.2.1"  # the pyRadMC release whose API this backend mirrors
+
+
+def default_step_energy_fraction(msc_model: str) -> float:
+    """transport/electron.py:97 — the per-model validated substep fraction."""
+    return GS_STEP_ENERGY_FRACTION if msc_model == "gs" else STEP_ENERGY_FRACTION
+
+
+def _validate_msc_model(msc_model: str) -> int:
+    if msc_model not in ("gaussian", "gs"):
+        raise ValueError(f"unknown msc_model {msc_model!r}; expected 'gaussian' or 'gs'")
+    return 1 if msc_model == "gs" else 0
+
+
+def validate_scoring_mode(scoring_mode: str, transport_electrons: bool) -> bool:
+    """scoring/dose_to_water.py:48 — True selects dose-to-water."""
+    if scoring_mode not in ("dose_to_medium", "dose_to_water"):
+        raise ValueError(
+            f"unknown scoring_mode {scoring_mode!r}; expected 'dose_to_medium' or 'dose_to_water'"
+        )
+    if scoring_mode == "dose_to_water" and not transport_electrons:
+        raise ValueError(
+            "dose_to_water requires electron transport: KERMA mode deposits carry no "
+            "electron to evaluate the stopping-power ratio on (it would need "
+            "mass-energy-absorption ratios instead)"
+        )
+    return scoring_mode == "dose_to_water"
+
+
+def _result_types():
+    """pyRadMC's own result classes when importable (a true drop-in), else the mirror."""
+    try:
+        from pyradmc.backends.results import RunProvenance, TransportResult
+        from pyradmc.scoring.dij import DijResult
+
+        return RunProvenance, TransportResult, DijResult
+    except ImportError:
+        return model.RunProvenance, model.TransportResult, model.DijResult
+
+
+def _progress_emitter(progress, total):
+    try:
+        from pyradmc.progress import ProgressEmitter
+
+        return ProgressEmitter(progress, total)
+    except ImportError:
+        return model.ProgressEmitter(progress, total)
+
+
+def _type_name(obj) -> str:
+    return type(obj).__name__
+
+
+class NativeError(RuntimeError):
+    """A failure reported by the C-ABI that has no reference exception type."""
+
+
+def _raise_for(code: int, message: str) -> None:
+    if code == _lib.PMC_OK:
+        return
+    if code == _lib.PMC_ERR_INVALID:
+        raise ValueError(message)
+    if code in (_lib.PMC_ERR_MAJORANT, _lib.PMC_ERR_QUEUE_OVERFLOW, _lib.PMC_ERR_STEP_CAP):
+        raise RuntimeError(message)
+    if code == _lib.PMC_ERR_OOM:
+        raise MemoryError(message)
+    raise NativeError(f"B200 backend error {code}: {message}")
+
+
+class _Native:
+    """One native engine (one CUDA device); calls are serialized by a lock."""
+
+    def __init__(self, device: str) -> None:
+        if not device.startswith("cuda"):
+            raise ValueError(
+                f"the B200 backend runs on CUDA devices only, got device={device!r} "
+                "(there is no CPU path)"
+            )
+        ordinal = int(device.split(":")[1]) if ":" in device else 0
+        self.lib = _lib.load()
+        if self.lib.pmc_device_count() <= ordinal:
+            raise RuntimeError(f"no CUDA device {device!r} visible to the B200 backend")
+        handle = C.c_void_p()
+        code = self.lib.pmc_create(C.byref(handle), ordinal)
+        if code != _lib.PMC_OK:
+            raise NativeError(f"pmc_create failed with code {code} on {device}")
+        self.handle = handle
+        self.device = device
+        self.lock = threading.Lock()
+        self.grid_key = None
+        self.table_key = None
+        self.gs_key = None
+        self.scoring_key = None
+        self._keep: list = []
+
+    def check(self, code: int) -> None:
+        if code != _lib.PMC_OK:
+            msg = self.lib.pmc_last_error(self.handle)
+            _raise_for(code, msg.decode() if msg else "")
+
+    def __del__(self) -> None:
+        handle = getattr(self, "handle", None)
+        if handle is not None and handle.value:
+            try:
+                self.lib.pmc_destroy(handle)
+            except Exception:
+                pass
+            self.handle = None
+
+
+@dataclass(frozen=True)
+class B200Engine:
+    """The B200 Monte Carlo dose engine over a voxel grid.
+
+    Parameters
+    ----------
+    grid, cross_sections
+        As in ``WarpEngine``: a ``VoxelGrid`` and a ``CrossSectionSource``
+        (pyRadMC's own, or this package's :class:`~pyradmc_b200.model.VoxelGrid`
+        and :class:`~pyradmc_b200.model.AnalyticWaterTables` mirrors).
+    device
+        ``"cuda:N"``.
+    chunk_size
+        Fresh primaries admitted per transport round (``None``: four per resident
+        transport thread).  Bit-inert: streams are pure functions of
+        ``(seed, history)`` and scoring is integer, so it only trades memory
+        for occupancy.
+    queue_factor
+        Queue slots per admitted primary; overflow raises, never drops.
+    block_size, blocks_per_sm, use_graph
+        Launch shape of the persistent transport kernels and whether each batch
+        drains inside one CUDA graph (a conditional WHILE node) or under a host
+        loop.  All bit-inert.
+    """
+
+    grid: object
+    cross_sections: object
+    device: str = "cuda:0"
+    chunk_size: int | None = None
+    queue_factor: int = 16
+    block_size: int | None = None
+    blocks_per_sm: int | None = None
+    use_graph: bool = True
+    max_steps: int | None = None
+    _natives: dict = field(default_factory=dict, init=False, repr=False, compare=False)
+    _table_cache: dict = field(default_factory=dict, init=False, repr=False, compare=False)
+    _table_cache_lock: threading.Lock = field(
+        default_factory=threading.Lock, init=False, repr=False, compare=False
+    )
+
+    # ---- host data ------------------------------------------------------------
+    def _native(self, device: str | None = None) -> _Native:
+        key = device or self.device
+        with self._table_cache_lock:
+            native = self._natives.get(key)
+            if native is None:
+                native = _Native(key)
+                self._natives[key] = native
+        return native
+
+    def _host_tables(self, e_max: float, pcut: float, ecut: float):
+        key = (ecut, pcut, e_max)
+        with self._table_cache_lock:
+            host = self._table_cache.get(key)
+            if host is None:
+                host = self.cross_sections.build_tables(
+                    ecut=ecut, pcut=pcut, e_max=e_max * _E_MAX_MARGIN
+                )
+                self._table_cache[key] = host
+        return host
+
+    def _gs_host(self, host, ecut: float, e_max: float):
+        """The GS node grid, built once per (ecut, e_max) before any launch."""
+        key = ("gs", ecut, e_max)
+        with self._table_cache_lock:
+            gs = self._table_cache.get(key)
+            if gs is None:
+                present = np.unique(np.asarray(self.grid.material)).astype(int).tolist()
+                if hasattr(self.cross_sections, "gs_grid_for"):
+                    gs = self.cross_sections.gs_grid_for(host, present)
+                else:
+                    from pyradmc.data.goudsmit_saunderson import (
+                        build_gs_grid,
+                        gs_window_from_tables,
+                    )
+
+                    gs = build_gs_grid(*gs_window_from_tables(host, present))
+                self._table_cache[key] = gs
+        return gs
+
+    def _upload(self, native: _Native, e_max: float, pcut: float, ecut: float, with_gs: bool,
+                scoring) -> None:
+        lib = native.lib
+        grid = self.grid
+        gkey = id(grid)
+        if native.grid_key != gkey:
+            if getattr(self.cross_sections, "n_materials", 1) > 256:
+                raise ValueError(
+                    "the B200 backend addresses at most 256 materials (uint8 voxel map); "
+                    f"this source declares {self.cross_sections.n_materials}"
+                )
+            shape = tuple(int(n) for n in grid.shape)
+            density = np.ascontiguousarray(np.asarray(grid.density), dtype=np.float32)
+            material = np.ascontiguousarray(np.asarray(grid.material).astype(np.uint8))
+            origin = np.asarray(grid.origin, dtype=np.float64)
+            spacing = np.asarray(grid.spacing, dtype=np.float64)
+            native.check(lib.pmc_upload_grid(
+                native.handle, shape[0], shape[1], shape[2], _lib.ptr(origin, C.c_double),
+                _lib.ptr(spacing, C.c_double), _lib.ptr(density, C.c_float),
+                _lib.ptr(material, C.c_uint8)))
+            native.grid_key = gkey
+            native.scoring_key = None
+        host = self._host_tables(e_max, pcut, ecut)
+        tkey = (id(host), ecut, pcut, e_max)
+        if native.table_key != tkey:
+            arrays = {}
+            for name in ("mu_compton", "mu_photo", "mu_pair", "mu_rayleigh", "majorant",
+                         "stopping_restricted", "stopping_radiative", "moller", "csda_range",
+                         "scattering_power", "log_eta", "restricted_range",
+                         "energy_of_restricted_range", "coherent_x", "coherent_cumulative"):
+                arrays[name] = np.ascontiguousarray(np.asarray(getattr(host, name)), dtype=np.float64)
+            n_mat = arrays["mu_compton"].shape[0]
+            desc = _lib.TablesDesc(
+                n_materials=n_mat,
+                n_points=int(host.n_points),
+                photon_log_e_min=float(host.photon_log_e_min),
+                photon_inv_dlog=float(host.photon_inv_dlog),
+                electron_log_e_min=float(host.electron_log_e_min),
+                electron_inv_dlog=float(host.electron_inv_dlog),
+                range_log_r_min=float(host.range_log_r_min),
+                range_inv_dlog=float(host.range_inv_dlog),
+                n_coherent=int(host.n_coherent),
+            )
+            for name, arr in arrays.items():
+                setattr(desc, name, _lib.ptr(arr, C.c_double))
+            native.check(lib.pmc_upload_tables(native.handle, C.byref(desc)))
+            native.table_key = tkey
+        if with_gs:
+            gs = self._gs_host(host, ecut, e_max)
+            gkey2 = id(gs)
+            if native.gs_key != gkey2:
+                values = np.ascontiguousarray(np.asarray(gs.values), dtype=np.float32)
+                n_eta, n_t2, n_u = values.shape
+                native.check(lib.pmc_upload_gs(native.handle, _lib.ptr(values, C.c_float),
+                                               int(gs.ix0), int(gs.iy0), n_eta, n_t2, n_u,
+                                               float(gs.bins_per_log)))
+                native.gs_key = gkey2
+        skey = id(scoring) if scoring is not None else ("default", gkey)
+        if native.scoring_key != skey:
+            if scoring is None:
+                scoring = model.ScoringGrid.for_grid(grid)
+            if _type_name(scoring) == "CylindricalScoringGrid":
+                raise ValueError("cylindrical scoring grids are not supported by the B200 backend")
+            mass = np.ascontiguousarray(np.asarray(scoring.voxel_mass).reshape(-1), dtype=np.float64)
+            sdesc = _lib.ScoringDesc(nx=int(scoring.shape[0]), ny=int(scoring.shape[1]),
+                                     nz=int(scoring.shape[2]))
+            sdesc.origin[:] = [float(v) for v in scoring.origin]
+            sdesc.spacing[:] = [float(v) for v in scoring.spacing]
+            sdesc.voxel_mass = _lib.ptr(mass, C.c_double)
+            native.check(lib.pmc_set_scoring(native.handle, C.byref(sdesc)))
+            native.scoring_key = skey
+
+    def _params(self, *, n_histories=0, n_batches, seed, pcut, ecut, transport_electrons,
+                msc_gs, step_energy_fraction, deposit_resolution, dose_to_water,
+                truncation=0.0, correlated=True, beamlet_group_size=None) -> _lib.RunParams:
+        return _lib.RunParams(
+            n_histories=int(n_histories),
+            n_batches=int(n_batches),
+            seed=int(seed) & 0xFFFFFFFFFFFFFFFF,
+            pcut=float(pcut),
+            ecut=float(ecut),
+            transport_electrons=1 if transport_electrons else 0,
+            msc_gs=msc_gs,
+            step_energy_fraction=float(step_energy_fraction),
+            deposit_resolution=float(deposit_resolution),
+            dose_to_water=dose_to_water,
+            photon_split_n=1,
+            truncation=float(truncation),
+            correlated=1 if correlated else 0,
+            beamlet_group_size=int(beamlet_group_size or 0),
+            chunk_size=int(self.chunk_size or 0),
+            queue_factor=int(self.queue_factor),
+            block_size=int(self.block_size or 0),
+            blocks_per_sm=int(self.blocks_per_sm or 0),
+            use_graph=1 if self.use_graph else 0,
+            max_steps=int(self.max_steps or 0),
+        )
+
+    def _provenance(self, seed, pcut, ecut, msc_model, step_energy_fraction,
+                    deposit_resolution_cm, devices=None):
+        RunProvenance, _, _ = _result_types()
+        return RunProvenance(
+            version=VERSION,
+            backend="b200",
+            device="+".join(devices) if devices else self.device,
+            seed=seed,
+            pcut_mev=pcut,
+            ecut_mev=ecut,
+            msc_model=msc_model,
+            step_energy_fraction=step_energy_fraction,
+            cross_sections=getattr(self.cross_sections, "provenance", type(self.cross_sections).__name__),
+            deposit_resolution_cm=deposit_resolution_cm,
+        )
+
+    def use_stream(self, stream: int | None, device: str | None = None) -> None:
+        """Run this engine's work on the caller's CUDA stream (a ``cudaStream_t``
+        as an int, e.g. ``torch.cuda.current_stream().cuda_stream``); None
+        restores the engine's own stream."""
+        native = self._native(device)
+        with native.lock:
+            native.check(native.lib.pmc_set_stream(native.handle, C.c_void_p(stream or 0)))
+
+    def drop_uploads(self, device: str | None = None) -> None:
+        """Forget what is resident, so the next call uploads grid, tables, GS
+        grid and scoring geometry again (an end-to-end timing from host data)."""
+        native = self._native(device)
+        with native.lock:
+            native.grid_key = native.table_key = native.gs_key = native.scoring_key = None
+
+    def last_counters(self, device: str | None = None) -> dict:
+        """Device event counters and device times of the last call on ``device``."""
+        native = self._native(device)
+        c = _lib.Counters()
+        native.check(native.lib.pmc_get_counters(native.handle, C.byref(c)))
+        return c.as_dict()
+
+    # ---- run ----------------------------------------------------------------------
+    def run(
+        self,
+        source,
+        n_histories: int,
+        n_batches: int,
+        seed: int,
+        pcut: float = PCUT_MEV,
+        ecut: float = ECUT_MEV,
+        transport_electrons: bool = True,
+        primary_kind: str = "photon",
+        scoring_grid=None,
+        scoring_mode: str = "dose_to_medium",
+        step_energy_fraction: float | None = None,
+        deposit_resolution_cm: float | None = None,
+        msc_model: str = "gs",
+        progress=None,
+        concurrent_batches: int = 1,
+    ):
+        """Transport ``n_histories`` primaries; the contract of ``WarpEngine.run``.
+
+        ``concurrent_batches`` is accepted for API compatibility and is inert:
+        a batch already drains inside one device-side graph with no host gaps
+        to hide, and the float64 fold stays in batch order either way.
+        """
+        if n_histories < 1:
+            raise ValueError(f"need at least one history, got {n_histories}")
+        if concurrent_batches < 1:
+            raise ValueError(f"need at least one lane, got concurrent_batches={concurrent_batches}")
+        if n_batches < 1:
+            raise ValueError(f"need at least one batch, got {n_batches}")
+        if n_histories % n_batches != 0:
+            raise ValueError(
+                f"n_histories={n_histories} not divisible by n_batches={n_batches}; "
+                "unequal batches would weight batch means inconsistently"
+            )
+        name = _type_name(source)
+        in_kernel = name in ("PencilBeamSource", "ParallelBeamSource")
+        if in_kernel and primary_kind not in ("photon", "electron"):
+            raise ValueError(f"unknown primary_kind {primary_kind!r}")
+        dose_to_water = 1 if validate_scoring_mode(scoring_mode, transport_electrons) else 0
+        msc_gs = _validate_msc_model(msc_model)
+        if step_energy_fraction is None:
+            step_energy_fraction = default_step_energy_fraction(msc_model)
+        if deposit_resolution_cm is not None and deposit_resolution_cm <= 0.0:
+            raise ValueError(f"deposit resolution must be positive, got {deposit_resolution_cm}")
+        deposit_resolution = 0.0 if deposit_resolution_cm is None else deposit_resolution_cm
+
+        src = _lib.SourceDesc()
+        keep = []
+        energy_emitted = None
+        if name == "PencilBeamSource":
+            src.type = _lib.PMC_SRC_PENCIL
+            src.kind = _lib.PMC_PHOTON if primary_kind == "photon" else _lib.PMC_ELECTRON
+            src.energy = float(source.energy)
+            src.position[:] = [float(v) for v in source.position]
+            src.direction[:] = [float(v) for v in source.direction]
+            energy_emitted = n_histories * source.max_energy
+        elif name == "ParallelBeamSource":
+            src.type = _lib.PMC_SRC_PARALLEL
+            src.kind = _lib.PMC_PHOTON if primary_kind == "photon" else _lib.PMC_ELECTRON
+            src.energy = float(source.energy)
+            src.z0 = float(source.z)
+            src.x_lo = float(source.x_range[0])
+            src.x_extent = float(source.x_range[1] - source.x_range[0])
+            src.y_lo = float(source.y_range[0])
+            src.y_extent = float(source.y_range[1] - source.y_range[0])
+            energy_emitted = n_histories * source.max_energy
+        elif name == "SpectralBeamSource":
+            spectrum = source.spectrum
+            edges = np.ascontiguousarray(spectrum.edges, dtype=np.float64)
+            cdf = np.ascontiguousarray(spectrum.cdf, dtype=np.float64)
+            keep += [edges, cdf]
+            src.type = _lib.PMC_SRC_SPECTRAL
+            src.kind = _lib.PMC_PHOTON
+            src.n_bins = int(cdf.size)
+            src.edges = _lib.ptr(edges, C.c_double)
+            src.cdf = _lib.ptr(cdf, C.c_double)
+            src.focal[:] = [float(v) for v in source.focal_point]
+            src.center[:] = [float(v) for v in source.center]
+            src.u_axis[:] = [float(v) for v in source.u_axis]
+            src.v_axis[:] = [float(v) for v in source.v_axis]
+            src.width_u = float(source.width_u)
+            src.width_v = float(source.width_v)
+        elif hasattr(source, "sample_batch"):
+            # Host pre-sampling route (Source.sample_batch): records in history order.
+            cols = source.sample_batch(seed, 0, n_histories)
+            codes = np.asarray(cols["particle_type"], dtype=np.int32)
+            iaea_to_kind = np.array([-1, 0, 1, 2], dtype=np.int32)
+            kind = np.ascontiguousarray(iaea_to_kind[codes])
+            energy = np.ascontiguousarray(cols["energy"], dtype=np.float32)
+            pos = np.ascontiguousarray(np.stack([cols["x"], cols["y"], cols["z"]], axis=1), dtype=np.float32)
+            dirs = np.ascontiguousarray(np.stack([cols["ux"], cols["uy"], cols["uz"]], axis=1), dtype=np.float32)
+            weight = np.ascontiguousarray(cols["weight"], dtype=np.float32)
+            keep += [kind, energy, pos, dirs, weight]
+            src.type = _lib.PMC_SRC_UPLOAD
+            src.up_kind = _lib.ptr(kind, C.c_int32)
+            src.up_energy = _lib.ptr(energy, C.c_float)
+            src.up_pos = _lib.ptr(pos, C.c_float)
+            src.up_dir = _lib.ptr(dirs, C.c_float)
+            src.up_weight = _lib.ptr(weight, C.c_float)
+        else:
+            raise ValueError(f"unsupported source type {name}")
+
+        params = self._params(
+            n_histories=n_histories, n_batches=n_batches, seed=seed, pcut=pcut, ecut=ecut,
+            transport_electrons=transport_electrons, msc_gs=msc_gs,
+            step_energy_fraction=step_energy_fraction, deposit_resolution=deposit_resolution,
+            dose_to_water=dose_to_water,
+        )
+        emitter = _progress_emitter(progress, n_histories)
+        scoring = scoring_grid
+        n_vox = (int(np.prod(scoring.shape)) if scoring is not None
+                 else int(np.prod(self.grid.shape)))
+        shape = tuple(scoring.shape) if scoring is not None else tuple(self.grid.shape)
+        dose = np.zeros(n_vox, dtype=np.float64)
+        sigma = np.zeros(n_vox, dtype=np.float64)
+        books = _lib.Books()
+        tick = _lib.PROGRESS_FN(lambda _u, n: emitter.tick(int(n)))
+        native = self._native()
+        lib = native.lib
+        with native.lock:
+            self._upload(native, source.max_energy, pcut, ecut, msc_gs == 1, scoring)
+            native.check(lib.pmc_set_progress(native.handle, C.cast(tick, C.c_void_p), None))
+            try:
+                code = lib.pmc_run_forward(native.handle, C.byref(src), C.byref(params),
+                                           _lib.ptr(dose, C.c_double), _lib.ptr(sigma, C.c_double),
+                                           C.byref(books))
+            finally:
+                lib.pmc_set_progress(native.handle, None, None)
+            native.check(code)
+        if energy_emitted is None:
+            energy_emitted = float(books.emitted) * ENERGY_QUANTUM_MEV
+        _, TransportResult, _ = _result_types()
+        return TransportResult(
+            dose=dose.reshape(shape),
+            dose_sigma=sigma.reshape(shape),
+            energy_emitted=energy_emitted,
+            energy_deposited=float(books.deposited) * ENERGY_QUANTUM_MEV,
+            energy_escaped=float(books.escaped) * ENERGY_QUANTUM_MEV,
+            energy_unscored=float(books.unscored) * ENERGY_QUANTUM_MEV,
+            n_histories=n_histories,
+            n_batches=n_batches,
+            scoring_mode=scoring_mode,
+            provenance=self._provenance(seed, pcut, ecut, msc_model, step_energy_fraction,
+                                        deposit_resolution_cm),
+        )
+
+    # ---- run_dij ------------------------------------------------------------------
+    def run_dij(
+        self,
+        source,
+        n_histories_per_beamlet,
+        n_batches: int,
+        seed: int,
+        pcut: float = PCUT_MEV,
+        ecut: float = ECUT_MEV,
+        transport_electrons: bool = True,
+        truncation: float = DIJ_TRUNCATION_RELATIVE,
+        correlated: bool = True,
+        beamlet_group_size: int | None = None,
+        scoring_grid=None,
+        scoring_mode: str = "dose_to_medium",
+        step_energy_fraction: float | None = None,
+        deposit_resolution_cm: float | None = None,
+        msc_model: str = "gs",
+        devices=None,
+        concurrent_batches: int = 1,
+        progress=None,
+    ):
+        """The Dij over the beamlets; the contract of ``WarpEngine.run_dij``.
+
+        Extension: ``n_histories_per_beamlet`` may be a sequence of per-beamlet
+        counts (each divisible by ``n_batches``).  Beamlet ``j`` then owns the
+        histories ``offset_j + r`` with ``offset_j`` the exclusive prefix sum of
+        the counts, so equal counts reproduce the reference mapping
+        ``h = j * n_per + r`` exactly.  ``DijResult.n_histories_per_beamlet``
+        carries the integer when the counts are equal and the maximum otherwise.
+        """
+        n_beamlets = int(source.n_beamlets)
+        if np.ndim(n_histories_per_beamlet) == 0:
+            counts = np.full(n_beamlets, int(n_histories_per_beamlet), dtype=np.int64)
+        else:
+            counts = np.asarray(n_histories_per_beamlet, dtype=np.int64).copy()
+            if counts.shape != (n_beamlets,):
+                raise ValueError(f"need {n_beamlets} per-beamlet history counts, got {counts.shape}")
+        for c in counts:
+            if c < 1:
+                raise ValueError(f"need at least one history per beamlet, got {int(c)}")
+            if c % n_batches != 0:
+                raise ValueError(
+                    f"n_histories_per_beamlet={int(c)} not divisible by "
+                    f"n_batches={n_batches}; unequal batches would weight batch means inconsistently"
+                )
+        if beamlet_group_size is not None and beamlet_group_size < 1:
+            raise ValueError(f"need a positive beamlet group size, got {beamlet_group_size}")
+        if concurrent_batches < 1:
+            raise ValueError(f"need at least one lane, got concurrent_batches={concurrent_batches}")
+        if truncation < 0.0:
+            raise ValueError(f"negative truncation {truncation}")
+        dose_to_water = 1 if validate_scoring_mode(scoring_mode, transport_electrons) else 0
+        msc_gs = _validate_msc_model(msc_model)
+        if step_energy_fraction is None:
+            step_energy_fraction = default_step_energy_fraction(msc_model)
+        if deposit_resolution_cm is not None and deposit_resolution_cm <= 0.0:
+            raise ValueError(f"deposit resolution must be positive, got {deposit_resolution_cm}")
+        deposit_resolution = 0.0 if deposit_resolution_cm is None else deposit_resolution_cm
+        device_list = [self.device] if devices is None else list(dict.fromkeys(devices))
+        if not device_list:
+            raise ValueError("devices must name at least one device")
+
+        name = _type_name(source)
+        offsets = np.zeros(n_beamlets, dtype=np.int64)
+        np.cumsum(counts[:-1], out=offsets[1:])
+        if name == "BeamletGridSource":
+            bounds = np.array([source.beamlet_bounds(j) for j in range(n_beamlets)], dtype=np.float64)
+            per = dict(x_lo=bounds[:, 0], x_extent=bounds[:, 1] - bounds[:, 0],
+                       y_lo=bounds[:, 2], y_extent=bounds[:, 3] - bounds[:, 2])
+            energy_emitted = float(np.sum(counts)) * source.max_energy
+        elif name == "SpectralBeamletSource":
+            per = dict(centers=np.asarray(source.centers, dtype=np.float64).reshape(n_beamlets, 3))
+            energy_emitted = None
+        else:
+            raise ValueError(f"unsupported beamlet source type {name}")
+
+        params = self._params(
+            n_batches=n_batches, seed=seed, pcut=pcut, ecut=ecut,
+            transport_electrons=transport_electrons, msc_gs=msc_gs,
+            step_energy_fraction=step_energy_fraction, deposit_resolution=deposit_resolution,
+            dose_to_water=dose_to_water, truncation=truncation, correlated=correlated,
+            beamlet_group_size=beamlet_group_size,
+        )
+        emitter = _progress_emitter(progress, int(np.sum(counts)))
+        group = beamlet_group_size or n_beamlets
+        group_starts = list(range(0, n_beamlets, group)) if len(device_list) > 1 else [0]
+        span = group if len(device_list) > 1 else n_beamlets
+        pending = deque(group_starts)
+        pending_lock = threading.Lock()
+
+        def next_group():
+            with pending_lock:
+                return pending.popleft() if pending else None
+
+        def shard(device: str):
+            native = self._native(device)
+            lib = native.lib
+            blocks = {}
+            totals = np.zeros(4, dtype=np.int64)
+            tick = _lib.PROGRESS_FN(lambda _u, n: emitter.tick(int(n)))
+            while (g0 := next_group()) is not None:
+                g1 = min(g0 + span, n_beamlets)
+                sl = slice(g0, g1)
+                desc = _lib.BeamletDesc(n_beamlets=g1 - g0)
+                keep = []
+                if name == "BeamletGridSource":
+                    desc.type = _lib.PMC_BEAMLET_LATTICE
+                    desc.energy = float(source.energy)
+                    desc.z0 = float(source.z)
+                    for key in ("x_lo", "x_extent", "y_lo", "y_extent"):
+                        arr = np.ascontiguousarray(per[key][sl])
+                        keep.append(arr)
+                        setattr(desc, key, _lib.ptr(arr, C.c_double))
+                else:
+                    spectrum = source.spectrum
+                    edges = np.ascontiguousarray(spectrum.edges, dtype=np.float64)
+                    cdf = np.ascontiguousarray(spectrum.cdf, dtype=np.float64)
+                    centers = np.ascontiguousarray(per["centers"][sl])
+                    keep += [edges, cdf, centers]
+                    desc.type = _lib.PMC_BEAMLET_SPECTRAL
+                    desc.n_bins = int(cdf.size)
+                    desc.edges = _lib.ptr(edges, C.c_double)
+                    desc.cdf = _lib.ptr(cdf, C.c_double)
+                    desc.focal[:] = [float(v) for v in source.focal_point]
+                    desc.u_axis[:] = [float(v) for v in source.u_axis]
+                    desc.v_axis[:] = [float(v) for v in source.v_axis]
+                    desc.width_u = float(source.width_u)
+                    desc.width_v = float(source.width_v)
+                    desc.centers = _lib.ptr(centers, C.c_double)
+                sub_counts = np.ascontiguousarray(counts[sl])
+                sub_offsets = np.ascontiguousarray(offsets[sl])
+                keep += [sub_counts, sub_offsets]
+                desc.history_offsets = _lib.ptr(sub_offsets, C.c_int64)
+                nnz = C.c_int64()
+                books = _lib.Books()
+                with native.lock:
+                    self._upload(native, source.max_energy, pcut, ecut, msc_gs == 1, scoring_grid)
+                    native.check(lib.pmc_set_progress(native.handle, C.cast(tick, C.c_void_p), None))
+                    try:
+                        code = lib.pmc_run_dij(native.handle, C.byref(desc),
+                                               _lib.ptr(sub_counts, C.c_int64), C.byref(params),
+                                               C.byref(nnz), C.byref(books))
+                    finally:
+                        lib.pmc_set_progress(native.handle, None, None)
+                    native.check(code)
+                    indptr = np.zeros(g1 - g0 + 1, dtype=np.int64)
+                    indices = np.zeros(nnz.value, dtype=np.int64)
+                    dose = np.zeros(nnz.value, dtype=np.float64)
+                    sigma = np.zeros(nnz.value, dtype=np.float64)
+                    native.check(lib.pmc_dij_fetch(native.handle, _lib.ptr(indptr, C.c_int64),
+                                                   _lib.ptr(indices, C.c_int64),
+                                                   _lib.ptr(dose, C.c_double),
+                                                   _lib.ptr(sigma, C.c_double)))
+                blocks[g0] = (np.diff(indptr), indices, dose, sigma)
+                totals += np.array([books.deposited, books.escaped, books.unscored, books.emitted])
+            return blocks, totals
+
+        if len(device_list) == 1:
+            results = [shard(device_list[0])]
+        else:
+            with ThreadPoolExecutor(max_workers=len(device_list)) as pool:
+                results = [f.result() for f in [pool.submit(shard, d) for d in device_list]]
+        blocks = {g: b for r, _ in results for g, b in r.items()}
+        totals = sum((t for _, t in results), np.zeros(4, dtype=np.int64))
+        counts_all, idx_all, dose_all, sig_all = [], [], [], []
+        for g0 in group_starts:
+            c, i, d, s = blocks[g0]
+            counts_all.append(c)
+            idx_all.append(i)
+            dose_all.append(d)
+            sig_all.append(s)
+        col_counts = np.concatenate(counts_all)
+        indptr = np.zeros(n_beamlets + 1, dtype=np.int64)
+        np.cumsum(col_counts, out=indptr[1:])
+        if energy_emitted is None:
+            energy_emitted = float(totals[3]) * ENERGY_QUANTUM_MEV
+        shape = tuple(scoring_grid.shape) if scoring_grid is not None else tuple(self.grid.shape)
+        _, _, DijResult = _result_types()
+        equal = bool(np.all(counts == counts[0]))
+        return DijResult(
+            grid_shape=shape,
+            n_beamlets=n_beamlets,
+            n_histories_per_beamlet=int(counts[0]) if equal else int(counts.max()),
+            n_batches=n_batches,
+            truncation=truncation,
+            indptr=indptr,
+            indices=np.concatenate(idx_all),
+            dose=np.concatenate(dose_all),
+            sigma=np.concatenate(sig_all),
+            energy_emitted=energy_emitted,
+            energy_deposited=float(totals[0]) * ENERGY_QUANTUM_MEV,
+            energy_escaped=float(totals[1]) * ENERGY_QUANTUM_MEV,
+            energy_unscored=float(totals[2]) * ENERGY_QUANTUM_MEV,
+            correlated=correlated,
+            scoring_mode=scoring_mode,
+            provenance=self._provenance(seed, pcut, ecut, msc_model, step_energy_fraction,
+                                        deposit_resolution_cm, devices=device_list),
+        )

@@ -1,0 +1,586 @@
+"""Host-side mirror of the pyRadMC objects the B200 engine consumes and returns.
+
+The engine is a drop-in for ``WarpEngine``: it accepts pyRadMC's own
+``VoxelGrid``, sources and ``CrossSectionSource`` objects unchanged, and returns
+pyRadMC's ``TransportResult``/``DijResult`` when pyRadMC is importable.  Where it
+is not (a GPU host with only this package), the classes below stand in with the
+same names, fields and semantics, so the same calls work:
+
+* :class:`VoxelGrid`            geometry/grid.py:227
+* :class:`PencilBeamSource`     geometry/source.py:279
+* :class:`ParallelBeamSource`   geometry/source.py:318
+* :class:`BeamletGridSource`    geometry/source.py:350
+* :class:`Spectrum`             geometry/spectrum.py:34
+* :class:`SpectralBeamSource`   geometry/source.py:560
+* :class:`SpectralBeamletSource` geometry/source.py:637
+* :class:`ScoringGrid`          scoring/grid.py:67 (``for_grid`` only)
+* :class:`RunProvenance`, :class:`TransportResult`  backends/results.py:19, :77
+* :class:`DijResult`            scoring/dij.py:195
+* :class:`ProgressEvent`, :class:`ProgressEmitter`  progress.py:30, :50
+* :class:`AnalyticWaterTables`  the analytic water source's flattened tables
+  (data/analytic.py:117 + data/tables.py:222), served from the packs that
+  ``pyradmc_b200/data/make_packs.py`` generated with pyRadMC's own builders.
+"""
+
+from __future__ import annotations
+
+import logging
+import math
+import threading
+import time
+from collections.abc import Callable, Sequence
+from dataclasses import dataclass, field
+from pathlib import Path
+from types import SimpleNamespace
+
+import numpy as np
+
+__all__ = [
+    "AnalyticWaterTables",
+    "BeamletGridSource",
+    "DijResult",
+    "ParallelBeamSource",
+    "PencilBeamSource",
+    "ProgressEmitter",
+    "ProgressEvent",
+    "RunProvenance",
+    "ScoringGrid",
+    "SpectralBeamSource",
+    "SpectralBeamletSource",
+    "Spectrum",
+    "TransportResult",
+    "VoxelGrid",
+    "ali_rogers_varian_6mv",
+]
+
+logger = logging.getLogger("pyradmc_b200.progress")
+
+DATA = Path(__file__).resolve().parent / "data"
+ELECTRON_MASS_MEV = 0.51099895069
+GY_PER_MEV_PER_G = 1.602176634e-10
+WATER = 0
+
+
+# ---- geometry ---------------------------------------------------------------------
+@dataclass(frozen=True)
+class VoxelGrid:
+    """Axis-aligned voxel grid with per-voxel density (g/cm^3) and material (cm)."""
+
+    shape: tuple[int, int, int]
+    spacing: tuple[float, float, float]
+    density: np.ndarray
+    material: np.ndarray
+    origin: tuple[float, float, float] = (0.0, 0.0, 0.0)
+
+    def __post_init__(self) -> None:
+        if any(n < 1 for n in self.shape):
+            raise ValueError(f"empty grid shape {self.shape}")
+        if any(s <= 0.0 for s in self.spacing):
+            raise ValueError(f"non-positive spacing {self.spacing}")
+        if self.density.shape != tuple(self.shape):
+            raise ValueError(f"density shape {self.density.shape} != grid shape {self.shape}")
+        if self.material.shape != tuple(self.shape):
+            raise ValueError(f"material shape {self.material.shape} != grid shape {self.shape}")
+        if np.any(self.density <= 0.0):
+            raise ValueError("non-positive voxel density; vacuum is not supported")
+        if np.any(self.material < 0):
+            raise ValueError("material index outside the registry")
+
+    @classmethod
+    def uniform_water(cls, shape, spacing, origin=(0.0, 0.0, 0.0)) -> VoxelGrid:
+        return cls(
+            shape=tuple(shape),
+            spacing=tuple(spacing),
+            origin=tuple(origin),
+            density=np.ones(shape, dtype=np.float64),
+            material=np.full(shape, WATER, dtype=np.int32),
+        )
+
+    @property
+    def voxel_volume(self) -> float:
+        return self.spacing[0] * self.spacing[1] * self.spacing[2]
+
+    @property
+    def upper_corner(self) -> tuple[float, float, float]:
+        return tuple(self.origin[i] + self.shape[i] * self.spacing[i] for i in range(3))
+
+    def max_density_by_material(self) -> tuple[tuple[int, float], ...]:
+        pairs = []
+        for material in np.unique(self.material):
+            pairs.append((int(material), float(self.density[self.material == material].max())))
+        return tuple(pairs)
+
+
+@dataclass(frozen=True)
+class ScoringGrid:
+    """Rectilinear scoring grid; ``for_grid`` is the engines' default."""
+
+    shape: tuple[int, int, int]
+    spacing: tuple[float, float, float]
+    origin: tuple[float, float, float]
+    voxel_mass: np.ndarray
+
+    @classmethod
+    def for_grid(cls, grid) -> ScoringGrid:
+        return cls(
+            shape=tuple(grid.shape),
+            spacing=tuple(grid.spacing),
+            origin=tuple(grid.origin),
+            voxel_mass=np.asarray(grid.density) * grid.voxel_volume,
+        )
+
+    @property
+    def n_voxels(self) -> int:
+        return int(self.shape[0] * self.shape[1] * self.shape[2])
+
+
+# ---- sources ----------------------------------------------------------------------
+def _normalized(v, name: str) -> tuple[float, float, float]:
+    n = math.sqrt(sum(c * c for c in v))
+    if n == 0.0:
+        raise ValueError(f"zero {name} vector")
+    return (v[0] / n, v[1] / n, v[2] / n)
+
+
+@dataclass(frozen=True)
+class PencilBeamSource:
+    energy: float
+    position: tuple[float, float, float]
+    direction: tuple[float, float, float]
+
+    def __post_init__(self) -> None:
+        if self.energy <= 0.0:
+            raise ValueError(f"non-positive energy {self.energy} MeV")
+        object.__setattr__(self, "direction", _normalized(self.direction, "direction"))
+
+    @property
+    def max_energy(self) -> float:
+        return self.energy
+
+
+@dataclass(frozen=True)
+class ParallelBeamSource:
+    energy: float
+    z: float
+    x_range: tuple[float, float]
+    y_range: tuple[float, float]
+
+    def __post_init__(self) -> None:
+        if self.energy <= 0.0:
+            raise ValueError(f"non-positive energy {self.energy} MeV")
+        if self.x_range[1] <= self.x_range[0] or self.y_range[1] <= self.y_range[0]:
+            raise ValueError("empty field")
+
+    @property
+    def max_energy(self) -> float:
+        return self.energy
+
+
+@dataclass(frozen=True)
+class BeamletGridSource:
+    energy: float
+    z: float
+    x_range: tuple[float, float]
+    y_range: tuple[float, float]
+    n_x: int
+    n_y: int
+
+    def __post_init__(self) -> None:
+        if self.energy <= 0.0:
+            raise ValueError(f"non-positive energy {self.energy} MeV")
+        if self.x_range[1] <= self.x_range[0] or self.y_range[1] <= self.y_range[0]:
+            raise ValueError("empty field")
+        if self.n_x < 1 or self.n_y < 1:
+            raise ValueError(f"lattice must be at least 1x1, got {self.n_x}x{self.n_y}")
+
+    @property
+    def max_energy(self) -> float:
+        return self.energy
+
+    @property
+    def n_beamlets(self) -> int:
+        return self.n_x * self.n_y
+
+    @staticmethod
+    def _edge(bounds, i: int, n: int) -> float:
+        lo, hi = bounds
+        if i == 0:
+            return lo
+        if i == n:
+            return hi
+        return lo + (hi - lo) * (i / n)
+
+    def beamlet_bounds(self, beamlet: int) -> tuple[float, float, float, float]:
+        """``(x_lo, x_hi, y_lo, y_hi)``: edges interpolated, never accumulated."""
+        if not 0 <= beamlet < self.n_beamlets:
+            raise IndexError(f"beamlet {beamlet} outside lattice of {self.n_beamlets}")
+        jx, jy = divmod(beamlet, self.n_y)
+        return (
+            self._edge(self.x_range, jx, self.n_x),
+            self._edge(self.x_range, jx + 1, self.n_x),
+            self._edge(self.y_range, jy, self.n_y),
+            self._edge(self.y_range, jy + 1, self.n_y),
+        )
+
+
+class Spectrum:
+    """Histogram photon spectrum sampled by CDF inversion (number convention)."""
+
+    def __init__(self, edges, weights, convention: str = "number") -> None:
+        e = np.asarray(edges, dtype=np.float64)
+        w = np.asarray(weights, dtype=np.float64)
+        if e.ndim != 1 or e.size < 2:
+            raise ValueError(f"a spectrum needs at least two edges, got shape {e.shape}")
+        if e[0] <= 0.0 or not np.all(np.diff(e) > 0.0):
+            raise ValueError("spectrum edges must be positive and strictly increasing")
+        if w.shape != (e.size - 1,) or np.any(w < 0.0):
+            raise ValueError("need one non-negative weight per bin")
+        if convention not in ("number", "energy_fluence"):
+            raise ValueError(f"unknown convention {convention!r}")
+        if convention == "energy_fluence":
+            w = w / (0.5 * (e[:-1] + e[1:]))
+        total = float(w.sum())
+        if total <= 0.0:
+            raise ValueError("spectrum weights must include at least one positive value")
+        self._edges = e
+        self._p = w / total
+        self._cdf = np.cumsum(self._p)
+
+    @property
+    def max_energy(self) -> float:
+        return float(self._edges[-1])
+
+    @property
+    def edges(self) -> np.ndarray:
+        return self._edges
+
+    @property
+    def cdf(self) -> np.ndarray:
+        return self._cdf
+
+    @property
+    def bin_probabilities(self) -> np.ndarray:
+        return self._p
+
+    @property
+    def mean_energy(self) -> float:
+        return float(np.sum(self._p * 0.5 * (self._edges[:-1] + self._edges[1:])))
+
+
+def ali_rogers_varian_6mv() -> Spectrum:
+    """The reference's ``ali_rogers_mv("varian-6mv", e_min=0.1)`` (from the pack)."""
+    with np.load(DATA / "spectrum_varian_6mv.npz") as z:
+        return Spectrum(z["edges"], z["weights"])
+
+
+@dataclass(frozen=True)
+class _Fan:
+    focal_point: tuple[float, float, float]
+    centers: tuple[tuple[float, float, float], ...]
+    width_u: float
+    width_v: float
+    u_axis: tuple[float, float, float]
+    v_axis: tuple[float, float, float]
+
+    def __post_init__(self) -> None:
+        if len(self.centers) == 0:
+            raise ValueError("a spectral source needs at least one aperture centre")
+        if self.width_u < 0.0 or self.width_v < 0.0:
+            raise ValueError("aperture widths must be non-negative")
+        u = _normalized(self.u_axis, "u_axis")
+        v = _normalized(self.v_axis, "v_axis")
+        cross = (u[1] * v[2] - u[2] * v[1], u[2] * v[0] - u[0] * v[2], u[0] * v[1] - u[1] * v[0])
+        if math.sqrt(sum(c * c for c in cross)) < 1.0e-12:
+            raise ValueError("aperture axes are parallel; they must span a plane")
+        object.__setattr__(self, "u_axis", u)
+        object.__setattr__(self, "v_axis", v)
+        object.__setattr__(self, "centers", tuple(tuple(c) for c in self.centers))
+
+
+class SpectralBeamSource:
+    def __init__(self, spectrum, focal_point, center, width_u, width_v,
+                 u_axis=(1.0, 0.0, 0.0), v_axis=(0.0, 1.0, 0.0)) -> None:
+        self._spectrum = spectrum
+        self._fan = _Fan(tuple(focal_point), (tuple(center),), width_u, width_v, u_axis, v_axis)
+
+    max_energy = property(lambda self: self._spectrum.max_energy)
+    spectrum = property(lambda self: self._spectrum)
+    focal_point = property(lambda self: self._fan.focal_point)
+    center = property(lambda self: self._fan.centers[0])
+    width_u = property(lambda self: self._fan.width_u)
+    width_v = property(lambda self: self._fan.width_v)
+    u_axis = property(lambda self: self._fan.u_axis)
+    v_axis = property(lambda self: self._fan.v_axis)
+
+
+class SpectralBeamletSource:
+    def __init__(self, spectrum, focal_point, centers, width_u, width_v,
+                 u_axis=(1.0, 0.0, 0.0), v_axis=(0.0, 1.0, 0.0)) -> None:
+        self._spectrum = spectrum
+        self._fan = _Fan(tuple(focal_point), tuple(centers), width_u, width_v, u_axis, v_axis)
+
+    max_energy = property(lambda self: self._spectrum.max_energy)
+    n_beamlets = property(lambda self: len(self._fan.centers))
+    spectrum = property(lambda self: self._spectrum)
+    focal_point = property(lambda self: self._fan.focal_point)
+    centers = property(lambda self: self._fan.centers)
+    width_u = property(lambda self: self._fan.width_u)
+    width_v = property(lambda self: self._fan.width_v)
+    u_axis = property(lambda self: self._fan.u_axis)
+    v_axis = property(lambda self: self._fan.v_axis)
+
+
+# ---- results ----------------------------------------------------------------------
+@dataclass(frozen=True)
+class RunProvenance:
+    version: str
+    backend: str
+    device: str
+    seed: int
+    pcut_mev: float
+    ecut_mev: float
+    msc_model: str
+    step_energy_fraction: float
+    cross_sections: str
+    deposit_resolution_cm: float | None = None
+
+    def summary(self) -> str:
+        return (
+            f"pyradmc {self.version} {self.backend}/{self.device} seed={self.seed} "
+            f"pcut={self.pcut_mev} ecut={self.ecut_mev} msc={self.msc_model} "
+            f"step={self.step_energy_fraction} deposit_res={self.deposit_resolution_cm} "
+            f"xs=[{self.cross_sections}]"
+        )
+
+
+@dataclass(frozen=True)
+class TransportResult:
+    dose: np.ndarray
+    dose_sigma: np.ndarray
+    energy_emitted: float
+    energy_deposited: float
+    energy_escaped: float
+    n_histories: int
+    n_batches: int
+    energy_unscored: float = 0.0
+    scoring_mode: str = "dose_to_medium"
+    provenance: RunProvenance | None = None
+
+
+@dataclass(frozen=True)
+class DijResult:
+    grid_shape: tuple[int, int, int]
+    n_beamlets: int
+    n_histories_per_beamlet: int
+    n_batches: int
+    truncation: float
+    indptr: np.ndarray
+    indices: np.ndarray
+    dose: np.ndarray
+    sigma: np.ndarray
+    energy_emitted: float
+    energy_deposited: float
+    energy_escaped: float
+    energy_unscored: float = 0.0
+    correlated: bool = False
+    scoring_mode: str = "dose_to_medium"
+    provenance: RunProvenance | None = None
+
+    @property
+    def n_voxels(self) -> int:
+        return int(np.prod(self.grid_shape))
+
+    def _scatter(self, values: np.ndarray, beamlet: int) -> np.ndarray:
+        if not 0 <= beamlet < self.n_beamlets:
+            raise IndexError(f"beamlet {beamlet} outside 0..{self.n_beamlets - 1}")
+        lo, hi = int(self.indptr[beamlet]), int(self.indptr[beamlet + 1])
+        out = np.zeros(self.n_voxels, dtype=np.float64)
+        out[self.indices[lo:hi]] = values[lo:hi]
+        return out.reshape(self.grid_shape)
+
+    def column_dense(self, beamlet: int) -> np.ndarray:
+        return self._scatter(self.dose, beamlet)
+
+    def sigma_dense(self, beamlet: int) -> np.ndarray:
+        return self._scatter(self.sigma, beamlet)
+
+    def dose_for_weights(self, weights: np.ndarray) -> np.ndarray:
+        w = np.asarray(weights, dtype=np.float64)
+        if w.shape != (self.n_beamlets,):
+            raise ValueError(f"weights shape {w.shape} != ({self.n_beamlets},)")
+        out = np.zeros(self.n_voxels, dtype=np.float64)
+        for j in range(self.n_beamlets):
+            lo, hi = int(self.indptr[j]), int(self.indptr[j + 1])
+            np.add.at(out, self.indices[lo:hi], w[j] * self.dose[lo:hi])
+        return out.reshape(self.grid_shape)
+
+    def dose_csc(self, unit: str = "mev_per_g"):
+        from scipy.sparse import csc_array
+
+        if unit not in ("mev_per_g", "gy"):
+            raise ValueError(f"unknown unit {unit!r}; expected 'mev_per_g' or 'gy'")
+        factor = 1.0 if unit == "mev_per_g" else GY_PER_MEV_PER_G
+        data = self.dose if factor == 1.0 else self.dose * factor
+        return csc_array((data, self.indices, self.indptr), shape=(self.n_voxels, self.n_beamlets))
+
+
+# ---- progress -----------------------------------------------------------------------
+@dataclass(frozen=True)
+class ProgressEvent:
+    histories_done: int
+    histories_total: int
+    elapsed_s: float
+    rate_hz: float
+
+
+class ProgressEmitter:
+    """Thread-safe progress ticks; a raising callback is logged and ignored."""
+
+    def __init__(self, callback: Callable | None, histories_total: int) -> None:
+        self._callback = callback
+        self._total = histories_total
+        self._done = 0
+        self._lock = threading.Lock()
+        self._start = time.monotonic()
+        self._last_t = self._start
+
+    def tick(self, histories: int) -> None:
+        with self._lock:
+            self._done += histories
+            now = time.monotonic()
+            dt = now - self._last_t
+            rate = histories / dt if dt > 0 else 0.0
+            self._last_t = now
+            event = ProgressEvent(self._done, self._total, now - self._start, rate)
+            logger.debug("progress: %d/%d histories (%.1f Hz)", event.histories_done,
+                         event.histories_total, event.rate_hz)
+            if self._callback is None:
+                return
+            try:
+                self._callback(event)
+            except Exception:
+                logger.exception("Progress callback raised; ignoring.")
+
+
+# ---- cross sections from the packs ----------------------------------------------------
+def _energy_label(energy: float) -> str:
+    return f"{energy:.4f}".rstrip("0").rstrip(".")
+
+
+class AnalyticWaterTables:
+    """The analytic water ``CrossSectionSource`` as flattened tables, from the packs.
+
+    Same constructor as ``AnalyticCrossSections(geometry_densities=...)``
+    (data/analytic.py:131): the Woodcock majorant is taken over the declared
+    ``(material, max density)`` pairs.  For water the majorant is the declared
+    maximum density times the unit-density majorant row of the pack (data/
+    analytic.py:196-206: ``max(density * mu_total)``), which is what scaling the
+    stored row does.  ``build_tables`` serves the pack whose ``e_max`` matches
+    the request exactly; other energies need pyRadMC's own builder.
+    """
+
+    _cache: dict = {}
+    _lock = threading.Lock()
+
+    def __init__(self, geometry_densities=((WATER, 1.0),)) -> None:
+        for material, density in geometry_densities:
+            if material != WATER:
+                raise ValueError(f"material index {material} beyond the analytic source (water only)")
+            if density <= 0.0:
+                raise ValueError(f"non-positive density {density} for material {material}")
+        self._geometry_densities = tuple(geometry_densities)
+        self._rho_max = max(d for _, d in geometry_densities)
+
+    n_materials = 1
+    provenance = (
+        "analytic closed-form water (Klein-Nishina without binding, power-law "
+        "photoelectric, fitted pair, Berger-Seltzer ICRU-37 stopping)"
+    )
+
+    @classmethod
+    def available_energies(cls) -> list[float]:
+        out = []
+        for path in sorted(DATA.glob("water_tables_*.npz")):
+            out.append(float(path.stem.split("_")[-1]))
+        return out
+
+    def _pack(self, e_max: float, ecut: float, pcut: float) -> dict:
+        e_primary = e_max / (1.0 + 1.0e-6)
+        path = DATA / f"water_tables_{_energy_label(e_primary)}.npz"
+        with self._lock:
+            cached = self._cache.get(path)
+            if cached is None:
+                if not path.exists():
+                    raise ValueError(
+                        f"no water table pack for e_max={e_max} MeV (packs: "
+                        f"{self.available_energies()}); pass pyRadMC's AnalyticCrossSections "
+                        "to build tables for other energies"
+                    )
+                with np.load(path) as z:
+                    cached = {k: z[k] for k in z.files}
+                self._cache[path] = cached
+        if not (
+            math.isclose(float(cached["e_max"]), e_max, rel_tol=0, abs_tol=1e-12)
+            and float(cached["ecut"]) == ecut
+            and float(cached["pcut"]) == pcut
+        ):
+            raise ValueError(
+                f"the water table packs are built at ecut={float(cached['ecut'])}, "
+                f"pcut={float(cached['pcut'])}, e_max={float(cached['e_max'])}; "
+                f"requested ecut={ecut}, pcut={pcut}, e_max={e_max}"
+            )
+        return cached
+
+    def build_tables(self, ecut: float, pcut: float, e_max: float, n_points=None):
+        z = self._pack(e_max, ecut, pcut)
+        fields = {k: v for k, v in z.items() if k != "provenance"}
+        for k in ("n_points", "n_coherent"):
+            fields[k] = int(fields[k])
+        for k in ("ecut", "pcut", "e_max", "photon_log_e_min", "photon_inv_dlog",
+                  "electron_log_e_min", "electron_inv_dlog", "range_log_r_min", "range_inv_dlog"):
+            fields[k] = float(fields[k])
+        fields["majorant"] = np.asarray(z["majorant"]) * self._rho_max
+        return SimpleNamespace(**fields)
+
+    def gs_grid_for(self, tables, materials: Sequence[int]):
+        """The GS node grid covering the window the kernels can reach.
+
+        The window is ``gs_window_from_tables`` (data/goudsmit_saunderson.py:
+        1222) restated; the packed grid is uploaded whole when it covers it, as
+        pyRadMC's own cached grid is (build_gs_grid returns a covering stored
+        grid as is, :1181-1196).
+        """
+        return gs_grid_from_pack(tables, materials)
+
+
+_gs_pack = None
+
+
+def gs_window(tables, materials) -> tuple[float, float, float]:
+    rows = np.asarray(sorted({int(m) for m in materials}), dtype=int)
+    if rows.size == 0:
+        raise ValueError("no materials given; the window would be empty")
+    log_eta = np.asarray(tables.log_eta)[rows]
+    ceiling = float(np.max(np.asarray(tables.scattering_power)[rows].max(axis=1)
+                           * np.asarray(tables.restricted_range)[rows].max(axis=1)))
+    return float(log_eta.min()), float(log_eta.max()), ceiling
+
+
+def gs_grid_from_pack(tables, materials):
+    global _gs_pack
+    if _gs_pack is None:
+        with np.load(DATA / "water_gs_grid.npz") as z:
+            _gs_pack = SimpleNamespace(values=np.ascontiguousarray(z["values"], dtype=np.float32),
+                                       ix0=int(z["ix0"]), iy0=int(z["iy0"]), n_u=int(z["n_u"]),
+                                       bins_per_log=float(z["bins_per_log"]))
+    lo, hi, t2 = gs_window(tables, materials)
+    bins = _gs_pack.bins_per_log
+    ix0, ix_top = math.floor(lo * bins), math.floor(hi * bins) + 1
+    iy0, iy_top = math.floor(math.log(1.0e-12) * bins), math.floor(math.log(t2) * bins) + 1
+    g = _gs_pack
+    covered = (g.ix0 <= ix0 and ix_top < g.ix0 + g.values.shape[0]
+               and g.iy0 <= iy0 and iy_top < g.iy0 + g.values.shape[1])
+    if not covered:
+        raise ValueError("the packed Goudsmit-Saunderson grid does not cover this run's window; "
+                         "use pyRadMC's build_gs_grid")
+    return g
