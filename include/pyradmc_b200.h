@@ -272,6 +272,30 @@ int pmc_truncate_dense(pmc_engine* engine, const double* mean, const double* sig
                        int32_t n_cols, int64_t n_vox, double truncation, int64_t* counts,
                        int64_t* nnz);
 
+/* Allocation-free truncation + CSC compaction.  No counterpart in the
+ * reference: it exists for callers that cannot call cudaMalloc (an application
+ * whose device memory all comes from its own pool, a process that fixes its
+ * footprint at start-up, work recorded into a CUDA graph).  It is the
+ * truncation and compaction of pmc_truncate_dense over caller-owned DEVICE
+ * buffers, with no allocation of any kind: its scratch is a static device
+ * array of about 3.2 MB that every GPU loading the library holds until exit.
+ *   mean, sigma  [n_cols][n_vox] float64 dose means and sigmas (device)
+ *   col_counts   [n_cols] int64 kept entries per column (device)
+ *   out_*        [out_capacity] CSC rows, doses, sigmas (device)
+ *   *nnz         the entry total (host); when it exceeds out_capacity the
+ *                call returns PMC_ERR_INVALID without writing out_*
+ * Limits: n_cols <= 4096 and n_cols * ceil(n_vox / 4096) <= 262144 (and at
+ * most 65535 tiles per column); larger sizes return PMC_ERR_INVALID.
+ * Work runs on `stream` (a cudaStream_t, NULL = the default stream) of the
+ * current device, and the call returns after it finished.  The first call on a
+ * device looks up the scratch array's device address, so make that first call
+ * before any stream capture.  All calls share the one array: calls that
+ * overlap on the GPU (other threads or streams) race. */
+int pmc_dij_compact_static(const double* mean, const double* sigma, int32_t n_cols,
+                           int64_t n_vox, double truncation, int64_t out_capacity,
+                           int64_t* col_counts, int64_t* out_indices, double* out_dose,
+                           double* out_sigma, int64_t* nnz, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

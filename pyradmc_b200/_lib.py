@@ -220,6 +220,11 @@ SIGNATURES: dict[str, tuple[object, list]] = {
         C.c_int,
         [C.c_void_p, _dp, _dp, C.c_int32, C.c_int64, C.c_double, _lp, _lp],
     ),
+    "pmc_dij_compact_static": (
+        C.c_int,
+        [C.c_void_p, C.c_void_p, C.c_int32, C.c_int64, C.c_double, C.c_int64, C.c_void_p,
+         C.c_void_p, C.c_void_p, C.c_void_p, _lp, C.c_void_p],
+    ),
 }
 
 PROGRESS_FN = C.CFUNCTYPE(None, C.c_void_p, C.c_int64)

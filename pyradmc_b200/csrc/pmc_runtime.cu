@@ -16,6 +16,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -1182,6 +1183,106 @@ int pmc_truncate_dense(pmc_engine* e, const double* mean, const double* sigma, i
     if (counts)
         for (int c = 0; c < n_cols; ++c) counts[c] = e->dij_indptr[c + 1] - e->dij_indptr[c];
     *nnz = (int64_t)e->dij_indices.size();
+    return PMC_OK;
+}
+
+}  // extern "C"
+
+// ============================================================================
+// Allocation-free truncation + CSC compaction (pmc_dij_compact_static)
+// ============================================================================
+// Some callers cannot call cudaMalloc: an application that owns all device
+// memory through its own pool or allocator, a process that forbids allocation
+// after start-up so its footprint stays fixed, or a caller recording work into
+// a CUDA graph, where an allocation would break the capture.  For them the
+// truncation + compaction scratch (column maxima, per-tile counts and offsets,
+// per-column counts, the entry total) lives in this file-scope device array
+// instead of engine-owned buffers.  Every GPU that loads the library holds it
+// until the process exits.
+namespace {
+
+constexpr int kStaticMaxCols = 4096;
+constexpr long long kStaticMaxTiles = 262144;  // columns x ceil(voxels / 4096)
+
+struct StaticScratch {
+    unsigned long long col_max[kStaticMaxCols];
+    long long col_counts[kStaticMaxCols];
+    unsigned long long total;
+    unsigned long long pad[31];
+    unsigned int tile_counts[kStaticMaxTiles];
+    unsigned long long tile_offsets[kStaticMaxTiles];
+};
+
+static __device__ __align__(256) StaticScratch g_static_scratch;
+
+constexpr int kStaticMaxDevices = 64;
+StaticScratch* g_scratch_ptr[kStaticMaxDevices] = {};
+std::mutex g_scratch_mutex;
+
+// Host code cannot use g_static_scratch's address directly (on the host the
+// name is only a stand-in for the device symbol), so the device address is
+// looked up once per device, with that device current.
+cudaError_t static_scratch(int device, StaticScratch** out) {
+    std::lock_guard<std::mutex> lock(g_scratch_mutex);
+    if (device < 0 || device >= kStaticMaxDevices) return cudaErrorInvalidDevice;
+    if (!g_scratch_ptr[device]) {
+        void* ptr = nullptr;
+        const cudaError_t st = cudaGetSymbolAddress(&ptr, g_static_scratch);
+        if (st != cudaSuccess) return st;
+        g_scratch_ptr[device] = (StaticScratch*)ptr;
+    }
+    *out = g_scratch_ptr[device];
+    return cudaSuccess;
+}
+
+}  // namespace
+
+extern "C" {
+
+int pmc_dij_compact_static(const double* mean, const double* sigma, int32_t n_cols, int64_t n_vox,
+                           double truncation, int64_t out_capacity, int64_t* col_counts,
+                           int64_t* out_indices, double* out_dose, double* out_sigma,
+                           int64_t* nnz, void* stream) {
+    if (!mean || !sigma || !col_counts || !nnz || n_cols < 1 || n_vox < 1 || out_capacity < 0)
+        return PMC_ERR_INVALID;
+    if (!(truncation >= 0.0)) return PMC_ERR_INVALID;
+    const long long n_tiles = (n_vox + kTileVoxels - 1) / kTileVoxels;
+    if (n_cols > kStaticMaxCols || n_tiles * n_cols > kStaticMaxTiles || n_tiles > 65535)
+        return PMC_ERR_INVALID;  // beyond the static scratch: at most 4096 columns and
+                                 // 262144 tiles of 4096 voxels, 65535 tiles per column
+    int device = 0;
+    if (cudaGetDevice(&device) != cudaSuccess) return PMC_ERR_CUDA;
+    StaticScratch* scratch = nullptr;
+    if (static_scratch(device, &scratch) != cudaSuccess) return PMC_ERR_CUDA;
+    cudaStream_t st = (cudaStream_t)stream;
+    // The array keeps the previous call's contents: the maxima must restart at 0.
+    if (cudaMemsetAsync(scratch->col_max, 0, sizeof(unsigned long long) * n_cols, st) != cudaSuccess)
+        return PMC_ERR_CUDA;
+    const dim3 grid((unsigned)n_tiles, (unsigned)n_cols);
+    colmax_kernel<<<grid, kReduceThreads, 0, st>>>(mean, n_vox, scratch->col_max);
+    count_kept_kernel<<<grid, kReduceThreads, 0, st>>>(mean, n_vox, (int)n_tiles, truncation,
+                                                        scratch->col_max, scratch->tile_counts);
+    scan_tiles_kernel<<<1, 1024, 0, st>>>(scratch->tile_counts, n_tiles * n_cols,
+                                          scratch->tile_offsets, n_cols, (int)n_tiles,
+                                          scratch->col_counts, &scratch->total);
+    if (cudaGetLastError() != cudaSuccess) return PMC_ERR_CUDA;
+    unsigned long long total = 0;
+    if (cudaMemcpyAsync(&total, &scratch->total, sizeof total, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess)
+        return PMC_ERR_CUDA;
+    *nnz = (int64_t)total;
+    if ((long long)total > out_capacity) return PMC_ERR_INVALID;  // *nnz tells the size needed
+    if (total > 0) {
+        if (!out_indices || !out_dose || !out_sigma) return PMC_ERR_INVALID;
+        compact_kernel<<<grid, kReduceThreads, 0, st>>>(
+            mean, sigma, n_vox, (int)n_tiles, truncation, scratch->col_max, scratch->tile_offsets,
+            (long long*)out_indices, out_dose, out_sigma);
+    }
+    if (cudaMemcpyAsync(col_counts, scratch->col_counts, sizeof(long long) * n_cols,
+                        cudaMemcpyDeviceToDevice, st) != cudaSuccess)
+        return PMC_ERR_CUDA;
+    if (cudaGetLastError() != cudaSuccess || cudaStreamSynchronize(st) != cudaSuccess)
+        return PMC_ERR_CUDA;
     return PMC_OK;
 }
 
