@@ -42,22 +42,32 @@ N_BATCHES = 10
 SEED = 20260726
 
 
+WORKLOAD = "dij100"
+
+
 def workload(rank: int = 0):
+    """The benchmark Dij; ``--workload dij10`` is the reduced case the ncu
+    captures use (the same phantom, one row of 10 beamlets, 1e5 histories each)."""
     from pyradmc_b200 import phantoms
     from pyradmc_b200.model import AnalyticWaterTables
 
     grid = phantoms.ellipsoid_phantom(seed=SEED)
-    source = phantoms.beamlet_fan(grid)
-    counts = phantoms.log_uniform_counts(source.n_beamlets, n_batches=N_BATCHES, seed=SEED)
+    if WORKLOAD == "dij10":
+        source = phantoms.beamlet_fan(grid, n_x=10, n_y=1)
+        counts = np.full(source.n_beamlets, 100_000, dtype=np.int64)
+    else:
+        source = phantoms.beamlet_fan(grid)
+        counts = phantoms.log_uniform_counts(source.n_beamlets, n_batches=N_BATCHES, seed=SEED)
     xs = AnalyticWaterTables(geometry_densities=grid.max_density_by_material())
     return grid, xs, source, counts
 
 
 def config_dict(counts, l2_note):
     return {
-        "workload": "dij_128cube_100beamlets_6MV",
+        "workload": ("dij_128cube_100beamlets_6MV" if WORKLOAD == "dij100"
+                     else "dij_128cube_10beamlets_6MV_profile"),
         "phantom": "128^3 at 2.5 mm, water + seeded ellipsoids rho U(0.2,1.9)",
-        "beamlets": 100,
+        "beamlets": int(len(counts)),
         "beamlet_mm": 5,
         "spectrum": "Ali-Rogers varian-6mv, e_min 0.1 MeV",
         "histories_per_dij": int(np.sum(counts)),
@@ -256,7 +266,7 @@ def b200_arm(args, world, rank, local):
     device = f"cuda:{local}"
     torch.cuda.set_device(local)
     grid, xs, source, counts = workload(rank)
-    engine = B200Engine(grid, xs, device=device)
+    engine = B200Engine(grid, xs, device=device, use_graph=not args.no_graph)
     stream = torch.cuda.Stream(device=device)  # an explicit stream: the legacy default is 0
     torch.cuda.set_stream(stream)
     engine.use_stream(stream.cuda_stream)
@@ -320,7 +330,7 @@ def b200_arm(args, world, rank, local):
     if rank != 0:
         return 0
     clock = clocks.summary()
-    base = cpu_baseline(grid, xs, source, counts) if world == 1 else None
+    base = cpu_baseline(grid, xs, source, counts) if world == 1 and not args.no_cpu_baseline else None
     traffic_path = ROOT / "profiles" / "transport_traffic.json"
     traffic = None
     if traffic_path.exists():
@@ -376,7 +386,16 @@ def main() -> int:
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("b200", "reference"), default="b200")
+    ap.add_argument("--workload", choices=("dij100", "dij10"), default="dij100",
+                    help="dij10: the reduced case used for ncu captures")
+    ap.add_argument("--no-graph", action="store_true",
+                    help="drain batches with the host loop instead of the CUDA graph (bit-identical; "
+                         "ncu cannot profile kernels inside graphs with conditional nodes)")
+    ap.add_argument("--no-cpu-baseline", action="store_true",
+                    help="skip the CPU baseline leg (profiling runs)")
     args = ap.parse_args()
+    global WORKLOAD
+    WORKLOAD = args.workload
     world, rank, local = dist_setup(args.gpus)
     try:
         if args.impl == "reference":

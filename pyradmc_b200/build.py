@@ -21,6 +21,10 @@ INCLUDE = PACKAGE.parent / "include"
 ARCH_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = [
     "-O3",
+    # Approximate float32 transcendentals and division for the float32
+    # transport (as the Warp kernels compile with fast_math); the float64
+    # reductions use explicit round-to-nearest intrinsics and are unaffected.
+    "--use_fast_math",
     "-lineinfo",
     "-std=c++17",
     "--expt-relaxed-constexpr",

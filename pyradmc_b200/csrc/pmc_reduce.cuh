@@ -25,32 +25,44 @@ __device__ __forceinline__ unsigned long long warp_sum_u64(unsigned long long v)
     return v;
 }
 
+constexpr int kFoldPerThread = 8;
+constexpr int kFoldChunk = kReduceThreads * kFoldPerThread;  // voxels per fold block
+
 // Fold one batch's quanta map into the running sums and consume it (reset the
-// folded entries).  Empty entries are skipped: adding +0.0 leaves the sums
-// bit-unchanged, so the skip is exact (kernels.py:804-852).
+// folded entries).  Grid: x = chunks of kFoldChunk voxels, y = column, so the
+// column (and its history count) is known per block.  Each thread first issues
+// all of its quanta loads, then folds the non-empty ones: empty entries are
+// skipped, since adding +0.0 leaves the sums bit-unchanged (kernels.py:804-852).
 __global__ void __launch_bounds__(kReduceThreads)
 fold_kernel(unsigned long long* __restrict__ edep, const double* __restrict__ mass,
-            const double* __restrict__ col_nhist, long long n_vox, long long n_total,
-            double* __restrict__ s1, double* __restrict__ s2,
-            unsigned long long* __restrict__ total_q) {
+            const double* __restrict__ col_nhist, long long n_vox, double* __restrict__ s1,
+            double* __restrict__ s2, unsigned long long* __restrict__ total_q) {
+    const long long col = blockIdx.y;
+    const long long base = col * n_vox;
+    const long long start = (long long)blockIdx.x * kFoldChunk + threadIdx.x;
+    unsigned long long q[kFoldPerThread];
+#pragma unroll
+    for (int k = 0; k < kFoldPerThread; ++k) {
+        const long long v = start + (long long)k * kReduceThreads;
+        q[k] = v < n_vox ? __ldcs(edep + base + v) : 0ull;
+    }
     unsigned long long local = 0;
-    const long long stride = (long long)gridDim.x * blockDim.x;
-    for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < n_total;
-         idx += stride) {
-        const unsigned long long q = edep[idx];
-        if (q == 0ull) continue;
+    const double nh = col_nhist[col];
+#pragma unroll
+    for (int k = 0; k < kFoldPerThread; ++k) {
+        if (q[k] == 0ull) continue;
+        const long long v = start + (long long)k * kReduceThreads;
+        const long long idx = base + v;
         edep[idx] = 0ull;
-        const long long col = idx / n_vox;
-        const long long vox = idx - col * n_vox;
-        const double m = mass[vox];
+        const double m = mass[v];
         double d = 0.0;
         if (m > 0.0) {
-            const double energy = __dmul_rn((double)(long long)q, kQuantum);
-            d = __ddiv_rn(energy, __dmul_rn(m, col_nhist[col]));
+            const double energy = __dmul_rn((double)(long long)q[k], kQuantum);
+            d = __ddiv_rn(energy, __dmul_rn(m, nh));
         }
         s1[idx] = __dadd_rn(s1[idx], d);
         s2[idx] = __dadd_rn(s2[idx], __dmul_rn(d, d));
-        local += q;
+        local += q[k];
     }
     local = warp_sum_u64(local);
     if ((threadIdx.x & 31) == 0 && local) atomicAdd(total_q, local);

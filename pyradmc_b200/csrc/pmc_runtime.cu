@@ -88,11 +88,9 @@ struct pmc_engine {
     int graph_block = 0;
     TransportParams graph_params{};
 
-    // results of the last Dij
+    // the CSC of the last Dij: indptr on the host, entries in out_* on the device
     std::vector<long long> dij_indptr;
-    std::vector<long long> dij_indices;
-    std::vector<double> dij_dose;
-    std::vector<double> dij_sigma;
+    long long csc_nnz = 0;
 
     pmc_counters counters{};
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
@@ -288,7 +286,10 @@ struct RunPlan {
     long long max_steps = 0;
 };
 
-int prepare_transport(pmc_engine* e, const pmc_run_params* p, RunPlan* plan) {
+// max_block: the most primaries one batch block of this call holds; admission
+// never needs more than that per round.
+int prepare_transport(pmc_engine* e, const pmc_run_params* p, unsigned long long max_block,
+                      RunPlan* plan) {
     if (!e->has_grid) return fail(e, PMC_ERR_STATE, "no transport grid uploaded");
     if (!e->has_tables) return fail(e, PMC_ERR_STATE, "no cross-section tables uploaded");
     if (p->msc_gs && !e->has_gs)
@@ -301,7 +302,8 @@ int prepare_transport(pmc_engine* e, const pmc_run_params* p, RunPlan* plan) {
     if (rc) return rc;
     const unsigned long long resident =
         (unsigned long long)std::max(plan->grid_ph, plan->grid_el) * plan->block;
-    plan->budget = p->chunk_size > 0 ? (unsigned long long)p->chunk_size : 4ull * resident;
+    plan->budget = p->chunk_size > 0 ? (unsigned long long)p->chunk_size : 16ull * resident;
+    plan->budget = std::max(1ull, std::min(plan->budget, max_block));
     const int qf = p->queue_factor > 0 ? p->queue_factor : 16;
     const unsigned long long cap64 = plan->budget * (unsigned long long)qf;
     if (cap64 > 0x7fffffffull)
@@ -381,12 +383,10 @@ int run_batch(pmc_engine* e, const pmc_run_params* p, const RunPlan& plan, Trans
 }
 
 int launch_fold(pmc_engine* e, long long n_vox, int group, const double* d_col_nhist) {
-    const long long n_total = n_vox * group;
-    const int blocks = (int)std::min<long long>((n_total + kReduceThreads - 1) / kReduceThreads,
-                                                (long long)e->sm_count * 16);
-    fold_kernel<<<std::max(blocks, 1), kReduceThreads, 0, e->stream>>>(
-        (unsigned long long*)e->edep.p, e->d_mass, d_col_nhist, n_vox, n_total, (double*)e->s1.p,
-        (double*)e->s2.p, e->d_total_q);
+    const dim3 grid((unsigned)((n_vox + kFoldChunk - 1) / kFoldChunk), (unsigned)group);
+    fold_kernel<<<grid, kReduceThreads, 0, e->stream>>>((unsigned long long*)e->edep.p, e->d_mass,
+                                                        d_col_nhist, n_vox, (double*)e->s1.p,
+                                                        (double*)e->s2.p, e->d_total_q);
     PMC_CUDA(e, cudaGetLastError());
     e->counters.reduce_launches += 1;
     return PMC_OK;
@@ -413,9 +413,25 @@ int launch_finalize(pmc_engine* e, long long n_vox, int group, int n_batches) {
     return PMC_OK;
 }
 
-// Truncate + compact the finalized group held in s1 (mean) / s2 (sigma) and
-// append its columns to the host CSC.
-int truncate_group(pmc_engine* e, long long n_vox, int group, double truncation) {
+// Grow a device buffer to at least `bytes`, keeping its first `keep` bytes.
+int grow_keep(pmc_engine* e, DevBuf& b, size_t bytes, size_t keep) {
+    if (b.p && b.bytes >= bytes) return PMC_OK;
+    const size_t cap = std::max(bytes, b.bytes + b.bytes / 2);
+    void* p = nullptr;
+    PMC_CUDA(e, cudaMalloc(&p, cap));
+    if (keep) PMC_CUDA(e, cudaMemcpyAsync(p, b.p, keep, cudaMemcpyDeviceToDevice, e->stream));
+    PMC_CUDA(e, cudaStreamSynchronize(e->stream));
+    if (b.p) cudaFree(b.p);
+    b.p = p;
+    b.bytes = cap;
+    return PMC_OK;
+}
+
+// First half of the truncation of the finalized group held in s1 (mean):
+// count the kept entries per (column, tile) and scan them on the device.
+// Returns the group's entry total and per-column counts on the host.
+int truncate_count(pmc_engine* e, long long n_vox, int group, double truncation,
+                   unsigned long long* nnz, std::vector<long long>* counts) {
     const int n_tiles = (int)((n_vox + kTileVoxels - 1) / kTileVoxels);
     const long long n_tc = (long long)n_tiles * group;
     int rc = ensure(e, e->tile_counts, sizeof(unsigned int) * n_tc);
@@ -429,38 +445,37 @@ int truncate_group(pmc_engine* e, long long n_vox, int group, double truncation)
         (const unsigned int*)e->tile_counts.p, n_tc, (unsigned long long*)e->tile_offsets.p, group,
         n_tiles, (long long*)e->col_counts.p, e->d_nnz);
     PMC_CUDA(e, cudaGetLastError());
-    unsigned long long nnz = 0;
-    std::vector<long long> counts(group);
-    PMC_CUDA(e, cudaMemcpyAsync(&nnz, e->d_nnz, sizeof nnz, cudaMemcpyDeviceToHost, e->stream));
-        e->d2h_bytes += (unsigned long long)(sizeof nnz);
-    PMC_CUDA(e, cudaMemcpyAsync(counts.data(), e->col_counts.p, sizeof(long long) * group, cudaMemcpyDeviceToHost, e->stream));
-        e->d2h_bytes += (unsigned long long)(sizeof(long long) * group);
+    e->counters.reduce_launches += 2;
+    counts->resize(group);
+    PMC_CUDA(e, cudaMemcpyAsync(nnz, e->d_nnz, sizeof *nnz, cudaMemcpyDeviceToHost, e->stream));
+    PMC_CUDA(e, cudaMemcpyAsync(counts->data(), e->col_counts.p, sizeof(long long) * group,
+                                cudaMemcpyDeviceToHost, e->stream));
+    e->d2h_bytes += sizeof *nnz + sizeof(long long) * group;
     PMC_CUDA(e, cudaStreamSynchronize(e->stream));
-    rc = ensure(e, e->out_idx, sizeof(long long) * nnz);
-    if (!rc) rc = ensure(e, e->out_dose, sizeof(double) * nnz);
-    if (!rc) rc = ensure(e, e->out_sigma, sizeof(double) * nnz);
+    return PMC_OK;
+}
+
+// Second half: write the kept entries behind the CSC already accumulated on
+// the device (earlier groups), in ascending voxel order per column.
+int truncate_compact(pmc_engine* e, long long n_vox, int group, double truncation,
+                     unsigned long long nnz, const std::vector<long long>& counts) {
+    const int n_tiles = (int)((n_vox + kTileVoxels - 1) / kTileVoxels);
+    const size_t base = (size_t)e->csc_nnz;
+    const size_t total = base + (size_t)nnz;
+    int rc = grow_keep(e, e->out_idx, sizeof(long long) * total, sizeof(long long) * base);
+    if (!rc) rc = grow_keep(e, e->out_dose, sizeof(double) * total, sizeof(double) * base);
+    if (!rc) rc = grow_keep(e, e->out_sigma, sizeof(double) * total, sizeof(double) * base);
     if (rc) return rc;
     if (nnz > 0) {
         compact_kernel<<<dim3(n_tiles, group), kReduceThreads, 0, e->stream>>>(
             (const double*)e->s1.p, (const double*)e->s2.p, n_vox, n_tiles, truncation,
-            e->d_colmax, (const unsigned long long*)e->tile_offsets.p, (long long*)e->out_idx.p,
-            (double*)e->out_dose.p, (double*)e->out_sigma.p);
+            e->d_colmax, (const unsigned long long*)e->tile_offsets.p,
+            (long long*)e->out_idx.p + base, (double*)e->out_dose.p + base,
+            (double*)e->out_sigma.p + base);
         PMC_CUDA(e, cudaGetLastError());
+        e->counters.reduce_launches += 1;
     }
-    e->counters.reduce_launches += nnz > 0 ? 3 : 2;
-    const size_t old = e->dij_indices.size();
-    e->dij_indices.resize(old + nnz);
-    e->dij_dose.resize(old + nnz);
-    e->dij_sigma.resize(old + nnz);
-    if (nnz > 0) {
-        PMC_CUDA(e, cudaMemcpyAsync(e->dij_indices.data() + old, e->out_idx.p, sizeof(long long) * nnz, cudaMemcpyDeviceToHost, e->stream));
-        e->d2h_bytes += (unsigned long long)(sizeof(long long) * nnz);
-        PMC_CUDA(e, cudaMemcpyAsync(e->dij_dose.data() + old, e->out_dose.p, sizeof(double) * nnz, cudaMemcpyDeviceToHost, e->stream));
-        e->d2h_bytes += (unsigned long long)(sizeof(double) * nnz);
-        PMC_CUDA(e, cudaMemcpyAsync(e->dij_sigma.data() + old, e->out_sigma.p, sizeof(double) * nnz, cudaMemcpyDeviceToHost, e->stream));
-        e->d2h_bytes += (unsigned long long)(sizeof(double) * nnz);
-        PMC_CUDA(e, cudaStreamSynchronize(e->stream));
-    }
+    e->csc_nnz = (long long)total;
     for (int c = 0; c < group; ++c) e->dij_indptr.push_back(e->dij_indptr.back() + counts[c]);
     return PMC_OK;
 }
@@ -774,7 +789,7 @@ int pmc_run_forward(pmc_engine* e, const pmc_source_desc* src, const pmc_run_par
     if (p->n_batches < 1 || p->n_histories % p->n_batches != 0)
         return fail(e, PMC_ERR_INVALID, "n_histories=%lld not divisible by n_batches=%d", (long long)p->n_histories, p->n_batches);
     RunPlan plan;
-    int rc = prepare_transport(e, p, &plan);
+    int rc = prepare_transport(e, p, (unsigned long long)(p->n_histories / p->n_batches), &plan);
     if (rc) return rc;
     const long long n_vox = e->si.n_voxels;
     rc = ensure_dense(e, n_vox);
@@ -920,8 +935,10 @@ int pmc_run_dij(pmc_engine* e, const pmc_beamlet_desc* src, const int64_t* count
             return fail(e, PMC_ERR_INVALID, "n_histories_per_beamlet=%lld not divisible by n_batches=%d", (long long)counts[j], p->n_batches);
     }
     if (p->truncation < 0.0) return fail(e, PMC_ERR_INVALID, "negative truncation %g", p->truncation);
+    unsigned long long all_block = 0;
+    for (int j = 0; j < n_beam; ++j) all_block += (unsigned long long)(counts[j] / p->n_batches);
     RunPlan plan;
-    int rc = prepare_transport(e, p, &plan);
+    int rc = prepare_transport(e, p, all_block, &plan);
     if (rc) return rc;
     const long long n_vox = e->si.n_voxels;
     int group = p->beamlet_group_size > 0 ? p->beamlet_group_size : 0;
@@ -952,9 +969,7 @@ int pmc_run_dij(pmc_engine* e, const pmc_beamlet_desc* src, const int64_t* count
     if (rc) return rc;
     PMC_CUDA(e, cudaMemsetAsync(e->d_total_q, 0, sizeof(unsigned long long), e->stream));
     e->dij_indptr.assign(1, 0);
-    e->dij_indices.clear();
-    e->dij_dose.clear();
-    e->dij_sigma.clear();
+    e->csc_nnz = 0;
     float t_tr = 0.0f, t_red = 0.0f;
 
     for (int g0 = 0; g0 < n_beam; g0 += group) {
@@ -1044,15 +1059,29 @@ int pmc_run_dij(pmc_engine* e, const pmc_beamlet_desc* src, const int64_t* count
         if (rc) return rc;
         rc = check_flags(e, s);
         if (rc) return rc;
+        // finalize + count + scan, then (after the entry total is known) compact;
+        // device time only, the host read of the total in between excluded.
+        unsigned long long g_nnz = 0;
+        std::vector<long long> g_counts;
         PMC_CUDA(e, cudaEventRecord(e->ev[0], e->stream));
         rc = launch_finalize(e, n_vox, gs, p->n_batches);
-        if (!rc) rc = truncate_group(e, n_vox, gs, p->truncation);
         if (rc) return rc;
         PMC_CUDA(e, cudaEventRecord(e->ev[1], e->stream));
-        PMC_CUDA(e, cudaEventSynchronize(e->ev[1]));
-        float c = 0;
-        cudaEventElapsedTime(&c, e->ev[0], e->ev[1]);
-        t_red += c;
+        rc = truncate_count(e, n_vox, gs, p->truncation, &g_nnz, &g_counts);
+        if (rc) return rc;
+        rc = grow_keep(e, e->out_idx, sizeof(long long) * (e->csc_nnz + g_nnz), sizeof(long long) * e->csc_nnz);
+        if (!rc) rc = grow_keep(e, e->out_dose, sizeof(double) * (e->csc_nnz + g_nnz), sizeof(double) * e->csc_nnz);
+        if (!rc) rc = grow_keep(e, e->out_sigma, sizeof(double) * (e->csc_nnz + g_nnz), sizeof(double) * e->csc_nnz);
+        if (rc) return rc;
+        PMC_CUDA(e, cudaEventRecord(e->ev[2], e->stream));
+        rc = truncate_compact(e, n_vox, gs, p->truncation, g_nnz, g_counts);
+        if (rc) return rc;
+        PMC_CUDA(e, cudaEventRecord(e->ev[3], e->stream));
+        PMC_CUDA(e, cudaEventSynchronize(e->ev[3]));
+        float c0 = 0, c1 = 0;
+        cudaEventElapsedTime(&c0, e->ev[0], e->ev[1]);  // finalize (count+scan ride in the
+        cudaEventElapsedTime(&c1, e->ev[2], e->ev[3]);  // synchronizing read; tiny kernels)
+        t_red += c0 + c1;
         if (e->progress) {
             long long done = 0;
             for (int k = 0; k < gs; ++k) done += counts[g0 + k];
@@ -1066,7 +1095,7 @@ int pmc_run_dij(pmc_engine* e, const pmc_beamlet_desc* src, const int64_t* count
     PMC_CUDA(e, cudaStreamSynchronize(e->stream));
     e->counters.transport_ms = t_tr;
     e->counters.reduce_ms = t_red;
-    *nnz_out = (int64_t)e->dij_indices.size();
+    *nnz_out = (int64_t)e->csc_nnz;
     if (books) {
         std::memset(books, 0, sizeof *books);
         books->deposited = (int64_t)total_q;
@@ -1076,13 +1105,16 @@ int pmc_run_dij(pmc_engine* e, const pmc_beamlet_desc* src, const int64_t* count
 
 int pmc_dij_fetch(pmc_engine* e, int64_t* indptr, int64_t* indices, double* dose, double* sigma) {
     if (!e || !indptr) return PMC_ERR_INVALID;
-    const size_t nnz = e->dij_indices.size();
+    PMC_CUDA(e, cudaSetDevice(e->device));
+    const size_t nnz = (size_t)e->csc_nnz;
     std::memcpy(indptr, e->dij_indptr.data(), sizeof(int64_t) * e->dij_indptr.size());
     if (nnz) {
         if (!indices || !dose || !sigma) return fail(e, PMC_ERR_INVALID, "null CSC buffer");
-        std::memcpy(indices, e->dij_indices.data(), sizeof(int64_t) * nnz);
-        std::memcpy(dose, e->dij_dose.data(), sizeof(double) * nnz);
-        std::memcpy(sigma, e->dij_sigma.data(), sizeof(double) * nnz);
+        PMC_CUDA(e, cudaMemcpyAsync(indices, e->out_idx.p, sizeof(int64_t) * nnz, cudaMemcpyDeviceToHost, e->stream));
+        PMC_CUDA(e, cudaMemcpyAsync(dose, e->out_dose.p, sizeof(double) * nnz, cudaMemcpyDeviceToHost, e->stream));
+        PMC_CUDA(e, cudaMemcpyAsync(sigma, e->out_sigma.p, sizeof(double) * nnz, cudaMemcpyDeviceToHost, e->stream));
+        PMC_CUDA(e, cudaStreamSynchronize(e->stream));
+        e->d2h_bytes += 3 * 8 * nnz;
     }
     return PMC_OK;
 }
@@ -1175,14 +1207,16 @@ int pmc_truncate_dense(pmc_engine* e, const double* mean, const double* sigma, i
         PMC_CUDA(e, cudaGetLastError());
     }
     e->dij_indptr.assign(1, 0);
-    e->dij_indices.clear();
-    e->dij_dose.clear();
-    e->dij_sigma.clear();
-    rc = truncate_group(e, n_vox, n_cols, truncation);
+    e->csc_nnz = 0;
+    unsigned long long t_nnz = 0;
+    std::vector<long long> t_counts;
+    rc = truncate_count(e, n_vox, n_cols, truncation, &t_nnz, &t_counts);
+    if (!rc) rc = truncate_compact(e, n_vox, n_cols, truncation, t_nnz, t_counts);
     if (rc) return rc;
+    PMC_CUDA(e, cudaStreamSynchronize(e->stream));
     if (counts)
         for (int c = 0; c < n_cols; ++c) counts[c] = e->dij_indptr[c + 1] - e->dij_indptr[c];
-    *nnz = (int64_t)e->dij_indices.size();
+    *nnz = (int64_t)e->csc_nnz;
     return PMC_OK;
 }
 

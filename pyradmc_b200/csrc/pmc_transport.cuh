@@ -136,19 +136,55 @@ __device__ __forceinline__ float spr_factor(const TransportParams& P, float e, i
     return sw / sm;
 }
 
+// Where a deposit's quanta go.  DirectSink issues one atomic per deposit;
+// HeldSink keeps one pending (entry, quanta) pair in registers and merges the
+// next deposit into it when it lands in the same entry — an electron's two
+// half-substep deposits and its next substep's usually do — so a run of
+// deposits into one voxel costs one atomic.  Integer sums: merging is exact.
+struct DirectSink {
+    unsigned long long n = 0;  // atomics issued
+    __device__ __forceinline__ void add(const TransportParams& P, long long flat,
+                                        unsigned long long q) {
+        atomicAdd(P.edep + flat, q);
+        ++n;
+    }
+};
+
+struct HeldSink {
+    long long idx = -1;
+    unsigned long long q = 0;
+    unsigned long long n = 0;
+    __device__ __forceinline__ void add(const TransportParams& P, long long flat,
+                                        unsigned long long quanta) {
+        if (flat == idx) {
+            q += quanta;
+            return;
+        }
+        release(P);
+        idx = flat;
+        q = quanta;
+    }
+    __device__ __forceinline__ void release(const TransportParams& P) {
+        if (q != 0ull) {
+            atomicAdd(P.edep + idx, q);
+            ++n;
+        }
+        idx = -1;
+        q = 0ull;
+    }
+};
+
 // kernels.py:536 _deposit: quantize once, route by position into the scoring
 // grid of this particle's column, or into the unscored book.
+template <class Sink>
 __device__ __forceinline__ void deposit(const TransportParams& P, BlockBooks& B, long long base,
                                        float x, float y, float z, float amount, float factor,
-                                       unsigned long long& n_dep) {
+                                       Sink& sink) {
     if (point_inside(x, y, z, P.si)) {
         const long long idx = flat_index(x, y, z, P.si);
         const long long q =
             (long long)((double)amount * (double)factor * kInvQuantum + 0.5);
-        if (q != 0) {
-            atomicAdd(P.edep + base + idx, (unsigned long long)q);
-            ++n_dep;
-        }
+        if (q != 0) sink.add(P, base + idx, (unsigned long long)q);
         if (P.dose_to_water) {
             book_add(&B.deposited, (long long)((double)amount * kInvQuantum + 0.5));
         }
@@ -162,26 +198,26 @@ __device__ __forceinline__ void escape(BlockBooks& B, float amount) {
 }
 
 // kernels.py:600 _deposit_or_escape: escape is decided on the transport grid.
+template <class Sink>
 __device__ __forceinline__ void deposit_or_escape(const TransportParams& P, BlockBooks& B,
                                                   long long base, float x, float y, float z,
-                                                  float amount, float factor,
-                                                  unsigned long long& n_dep) {
+                                                  float amount, float factor, Sink& sink) {
     if (amount <= 0.0f) return;
-    if (point_inside(x, y, z, P.gi)) deposit(P, B, base, x, y, z, amount, factor, n_dep);
+    if (point_inside(x, y, z, P.gi)) deposit(P, B, base, x, y, z, amount, factor, sink);
     else escape(B, amount);
 }
 
 // kernels.py:631 _deposit_spread: equal pieces at piece midpoints.
+template <class Sink>
 __device__ inline void deposit_spread(const TransportParams& P, BlockBooks& B, long long base,
                                       float x, float y, float z, float ux, float uy, float uz,
-                                      float length, float amount, float factor,
-                                      unsigned long long& n_dep) {
+                                      float length, float amount, float factor, Sink& sink) {
     const int n = substep_pieces(length, P.deposit_resolution);
     const float share = amount / (float)n;
     const float piece = length / (float)n;
     for (int k = 0; k < n; ++k) {
         const float t = ((float)k + 0.5f) * piece;
-        deposit_or_escape(P, B, base, x + ux * t, y + uy * t, z + uz * t, share, factor, n_dep);
+        deposit_or_escape(P, B, base, x + ux * t, y + uy * t, z + uz * t, share, factor, sink);
     }
 }
 
@@ -352,12 +388,12 @@ __device__ inline int generate_primary(const TransportParams& P, const GenDesc& 
 }
 
 // ---- annihilation at rest (transport/particles.py:75, kernels.py:675) ------------
+template <class Sink>
 __device__ inline void annihilate_at_rest(const TransportParams& P, BlockBooks& B, Particle& p,
-                                          long long base, int q_photon, float factor,
-                                          unsigned long long& n_dep,
+                                          long long base, int q_photon, float factor, Sink& sink,
                                           unsigned long long& n_push) {
     if (P.pcut >= kElectronMass) {
-        deposit(P, B, base, p.x, p.y, p.z, p.w * 2.0f * kElectronMass, factor, n_dep);
+        deposit(P, B, base, p.x, p.y, p.z, p.w * 2.0f * kElectronMass, factor, sink);
         return;
     }
     float ax, ay, az;
@@ -418,7 +454,7 @@ __device__ __forceinline__ void block_sum_add(unsigned long long* dst, unsigned 
 // ---- the photon kernel ---------------------------------------------------------------
 // One lane transports one photon to termination (Woodcock tracking), then takes
 // the next: queued photons first, then fresh primaries of the batch block.
-__global__ void __launch_bounds__(256) photon_kernel(TransportParams P) {
+__global__ void __launch_bounds__(256, 3) photon_kernel(TransportParams P) {
     __shared__ BlockBooks B;
     init_books(B);
     Sched* S = P.sched;
@@ -431,7 +467,8 @@ __global__ void __launch_bounds__(256) photon_kernel(TransportParams P) {
     const Tables& T = P.tab;
     const float pcut = P.pcut, ecut = P.ecut;
 
-    unsigned long long n_flight = 0, n_inter = 0, n_dep = 0, n_push = 0, n_prim = 0;
+    unsigned long long n_flight = 0, n_inter = 0, n_push = 0, n_prim = 0;
+    DirectSink dep;
     Particle p;
     bool active = false, exhausted = false;
     float e_tab = -1.0f, maj = 0.0f;
@@ -539,14 +576,14 @@ __global__ void __launch_bounds__(256) photon_kernel(TransportParams P) {
                                    ex, ey, ez, sid, n_push);
                     } else {
                         deposit(P, B, base, p.x, p.y, p.z, split_w * recoil,
-                                spr_factor(P, recoil, mat), n_dep);
+                                spr_factor(P, recoil, mat), dep);
                     }
                     float gx = p.ux, gy = p.uy, gz = p.uz;
                     rotate_direction(gx, gy, gz, compton_cos_theta(p.e, ratio), phi);
                     const float es = p.e * ratio;
                     if (es <= pcut) {
                         deposit(P, B, base, p.x, p.y, p.z, split_w * es, spr_factor(P, es, mat),
-                                n_dep);
+                                dep);
                         continue;
                     }
                     float cw = split_w;
@@ -576,12 +613,12 @@ __global__ void __launch_bounds__(256) photon_kernel(TransportParams P) {
                 queue_push(P, q_el, kElectron, p.beamlet, recoil, p.w, p.x, p.y, p.z, ex, ey, ez,
                            sid, n_push);
             } else {
-                deposit(P, B, base, p.x, p.y, p.z, p.w * recoil, spr_factor(P, recoil, mat), n_dep);
+                deposit(P, B, base, p.x, p.y, p.z, p.w * recoil, spr_factor(P, recoil, mat), dep);
             }
             rotate_direction(p.ux, p.uy, p.uz, compton_cos_theta(p.e, ratio), phi);
             p.e *= ratio;
             if (p.e <= pcut) {
-                deposit(P, B, base, p.x, p.y, p.z, p.w * p.e, spr_factor(P, p.e, mat), n_dep);
+                deposit(P, B, base, p.x, p.y, p.z, p.w * p.e, spr_factor(P, p.e, mat), dep);
                 active = false;
                 continue;
             }
@@ -600,7 +637,7 @@ __global__ void __launch_bounds__(256) photon_kernel(TransportParams P) {
                 queue_push(P, q_el, kElectron, p.beamlet, p.e, p.w, p.x, p.y, p.z, p.ux, p.uy,
                            p.uz, sid, n_push);
             } else {
-                deposit(P, B, base, p.x, p.y, p.z, p.w * p.e, spr_factor(P, p.e, mat), n_dep);
+                deposit(P, B, base, p.x, p.y, p.z, p.w * p.e, spr_factor(P, p.e, mat), dep);
             }
             active = false;
         } else {  // pair production
@@ -615,7 +652,7 @@ __global__ void __launch_bounds__(256) photon_kernel(TransportParams P) {
                                p.uy, p.uz, sid, n_push);
                 } else {
                     deposit(P, B, base, p.x, p.y, p.z, p.w * share_e, spr_factor(P, share_e, mat),
-                            n_dep);
+                            dep);
                 }
                 if (share_p > ecut) {
                     const StreamId sid = p.rng.spawn();
@@ -623,14 +660,14 @@ __global__ void __launch_bounds__(256) photon_kernel(TransportParams P) {
                                p.uy, p.uz, sid, n_push);
                 } else {
                     deposit(P, B, base, p.x, p.y, p.z, p.w * share_p, spr_factor(P, share_p, mat),
-                            n_dep);
+                            dep);
                     annihilate_at_rest(P, B, p, base, q_out, spr_factor(P, kElectronMass, mat),
-                                       n_dep, n_push);
+                                       dep, n_push);
                 }
             } else {
                 deposit(P, B, base, p.x, p.y, p.z, p.w * kinetic, spr_factor(P, kinetic, mat),
-                        n_dep);
-                annihilate_at_rest(P, B, p, base, q_out, spr_factor(P, kElectronMass, mat), n_dep,
+                        dep);
+                annihilate_at_rest(P, B, p, base, q_out, spr_factor(P, kElectronMass, mat), dep,
                                    n_push);
             }
             active = false;
@@ -639,7 +676,7 @@ __global__ void __launch_bounds__(256) photon_kernel(TransportParams P) {
 
     block_sum_add(&B.flights, n_flight);
     block_sum_add(&B.interactions, n_inter);
-    block_sum_add(&B.deposits, n_dep);
+    block_sum_add(&B.deposits, dep.n);
     block_sum_add(&B.pushes, n_push);
     block_sum_add(&B.primaries, n_prim);
     flush_books(P, B);
@@ -659,7 +696,7 @@ __global__ void __launch_bounds__(256) photon_kernel(TransportParams P) {
 // One lane runs one electron or positron to ECUT (Class II condensed history,
 // electron.py:345-481); delta rays go to the next round's electron queue,
 // bremsstrahlung and annihilation photons to the next photon round.
-__global__ void __launch_bounds__(256) electron_kernel(TransportParams P) {
+__global__ void __launch_bounds__(256, 4) electron_kernel(TransportParams P) {
     __shared__ BlockBooks B;
     init_books(B);
     Sched* S = P.sched;
@@ -669,7 +706,8 @@ __global__ void __launch_bounds__(256) electron_kernel(TransportParams P) {
     const Tables& T = P.tab;
     const float pcut = P.pcut, ecut = P.ecut;
 
-    unsigned long long n_sub = 0, n_dep = 0, n_push = 0;
+    unsigned long long n_sub = 0, n_push = 0;
+    HeldSink dep;
     Particle p;
     bool active = false, exhausted = false;
     float latent = 0.0f;
@@ -680,6 +718,7 @@ __global__ void __launch_bounds__(256) electron_kernel(TransportParams P) {
             if (__any_sync(0xffffffffu, (*(volatile int*)&S->flags) & (kFlagOverflow | kFlagStepCap)))
                 break;
         }
+        if (!active) dep.release(P);  // the finished particle's last held deposit
         if (!active && !exhausted) {
             const unsigned int i = fetch_one(&S->head[q_in]);
             if (i < n_in) {
@@ -702,9 +741,9 @@ __global__ void __launch_bounds__(256) electron_kernel(TransportParams P) {
         }
         if (p.e <= ecut) {  // terminal: local deposit (electron.py:347-365)
             const int tm = __float_as_int(__ldg(P.vox + flat_index(p.x, p.y, p.z, P.gi)).y);
-            deposit(P, B, base, p.x, p.y, p.z, p.w * p.e, spr_factor(P, p.e, tm), n_dep);
+            deposit(P, B, base, p.x, p.y, p.z, p.w * p.e, spr_factor(P, p.e, tm), dep);
             if (p.kind == kPositron)
-                annihilate_at_rest(P, B, p, base, q_ph, spr_factor(P, kElectronMass, tm), n_dep,
+                annihilate_at_rest(P, B, p, base, q_ph, spr_factor(P, kElectronMass, tm), dep,
                                    n_push);
             active = false;
             continue;
@@ -763,7 +802,7 @@ __global__ void __launch_bounds__(256) electron_kernel(TransportParams P) {
         if (s > 0.0f) d1 = continuous * (s1 / s);
         const float d2 = continuous - d1;
 
-        deposit_spread(P, B, base, p.x, p.y, p.z, p.ux, p.uy, p.uz, s1, p.w * d1, factor, n_dep);
+        deposit_spread(P, B, base, p.x, p.y, p.z, p.ux, p.uy, p.uz, s1, p.w * d1, factor, dep);
         p.e -= d1;
         p.x += p.ux * s1;
         p.y += p.uy * s1;
@@ -802,12 +841,12 @@ __global__ void __launch_bounds__(256) electron_kernel(TransportParams P) {
                                sid, n_push);
                 }
             } else {
-                deposit_or_escape(P, B, base, p.x, p.y, p.z, p.w * k, spr_factor(P, k, mat), n_dep);
+                deposit_or_escape(P, B, base, p.x, p.y, p.z, p.w * k, spr_factor(P, k, mat), dep);
             }
             p.e -= k;
         }
 
-        deposit_spread(P, B, base, p.x, p.y, p.z, p.ux, p.uy, p.uz, s2, p.w * d2, factor, n_dep);
+        deposit_spread(P, B, base, p.x, p.y, p.z, p.ux, p.uy, p.uz, s2, p.w * d2, factor, dep);
         p.e -= d2;
         p.x += p.ux * s2;
         p.y += p.uy * s2;
@@ -834,8 +873,9 @@ __global__ void __launch_bounds__(256) electron_kernel(TransportParams P) {
         }
     }
 
+    dep.release(P);
     block_sum_add(&B.substeps, n_sub);
-    block_sum_add(&B.deposits, n_dep);
+    block_sum_add(&B.deposits, dep.n);
     block_sum_add(&B.pushes, n_push);
     flush_books(P, B);
 

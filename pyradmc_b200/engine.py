@@ -653,9 +653,9 @@ class B200Engine:
                         lib.pmc_set_progress(native.handle, None, None)
                     native.check(code)
                     indptr = np.zeros(g1 - g0 + 1, dtype=np.int64)
-                    indices = np.zeros(nnz.value, dtype=np.int64)
-                    dose = np.zeros(nnz.value, dtype=np.float64)
-                    sigma = np.zeros(nnz.value, dtype=np.float64)
+                    indices = np.empty(nnz.value, dtype=np.int64)
+                    dose = np.empty(nnz.value, dtype=np.float64)
+                    sigma = np.empty(nnz.value, dtype=np.float64)
                     native.check(lib.pmc_dij_fetch(native.handle, _lib.ptr(indptr, C.c_int64),
                                                    _lib.ptr(indices, C.c_int64),
                                                    _lib.ptr(dose, C.c_double),
@@ -681,6 +681,10 @@ class B200Engine:
         col_counts = np.concatenate(counts_all)
         indptr = np.zeros(n_beamlets + 1, dtype=np.int64)
         np.cumsum(col_counts, out=indptr[1:])
+
+        def joined(parts):  # one block (one device) needs no copy
+            return parts[0] if len(parts) == 1 else np.concatenate(parts)
+
         if energy_emitted is None:
             energy_emitted = float(totals[3]) * ENERGY_QUANTUM_MEV
         shape = tuple(scoring_grid.shape) if scoring_grid is not None else tuple(self.grid.shape)
@@ -693,9 +697,9 @@ class B200Engine:
             n_batches=n_batches,
             truncation=truncation,
             indptr=indptr,
-            indices=np.concatenate(idx_all),
-            dose=np.concatenate(dose_all),
-            sigma=np.concatenate(sig_all),
+            indices=joined(idx_all),
+            dose=joined(dose_all),
+            sigma=joined(sig_all),
             energy_emitted=energy_emitted,
             energy_deposited=float(totals[0]) * ENERGY_QUANTUM_MEV,
             energy_escaped=float(totals[1]) * ENERGY_QUANTUM_MEV,
