@@ -185,32 +185,40 @@ def all_sum(world, values):
 
 
 # ---- the CPU baseline -----------------------------------------------------------------
-def cpu_baseline(grid, xs, source, counts, target_seconds=15.0):
-    """The C oracle on all host cores, on a bounded sample of the same Dij."""
+def _oracle_sample(grid, xs, source, counts, per_col, seed):
+    """Time the C oracle on `per_col` histories of every beamlet (one batch)."""
     import oracle
 
     tab = xs.build_tables(0.2, 0.05, source.max_energy * (1 + 1e-6))
     gs = xs.gs_grid_for(tab, [0])
-    threads = oracle.max_threads()
-    sample = 20
+    t0 = time.perf_counter()
+    oracle.run(grid, tab, gs, source, counts=list(counts), n_batches=1, seed=seed, forward=False,
+               n_threads=oracle.max_threads(), max_histories=per_col)
+    return time.perf_counter() - t0, int(np.sum(np.minimum(counts, per_col)))
 
-    def run(per_col):
-        t0 = time.perf_counter()
-        oracle.run(grid, tab, gs, source, counts=list(counts), n_batches=1, seed=SEED,
-                   forward=False, n_threads=threads, max_histories=per_col)
-        return time.perf_counter() - t0
 
-    elapsed = run(sample)
-    if elapsed < target_seconds:
-        sample = int(sample * min(200.0, target_seconds / max(elapsed, 1e-3)))
-        elapsed = run(sample)
-    done = int(np.sum(np.minimum(counts, sample)))
+def calibrate_sample(grid, xs, source, counts, target_seconds):
+    """Grow the per-beamlet sample until one run takes ~target_seconds (or covers
+    the whole workload), so the oracle's fixed costs do not dominate the rate."""
+    per_col = 100
+    elapsed, done = _oracle_sample(grid, xs, source, counts, per_col, SEED)
+    while elapsed < 0.7 * target_seconds and per_col < int(np.max(counts)):
+        per_col = int(per_col * min(8.0, max(1.5, target_seconds / max(elapsed, 1e-3))))
+        elapsed, done = _oracle_sample(grid, xs, source, counts, per_col, SEED)
+    return per_col, elapsed, done
+
+
+def cpu_baseline(grid, xs, source, counts, target_seconds=15.0):
+    """The C oracle on all host cores, on a bounded sample of the same Dij."""
+    import oracle
+
+    per_col, elapsed, done = calibrate_sample(grid, xs, source, counts, target_seconds)
     return {
         "value": done / elapsed,
         "unit": "histories/s",
-        "cores": threads,
+        "cores": oracle.max_threads(),
         "kind": "port",
-        "sample": f"{sample} histories of each of the 100 beamlets ({done} histories, "
+        "sample": f"{per_col} histories of each of the {len(counts)} beamlets ({done} histories, "
                   f"{elapsed:.1f} s), same phantom/spectrum/physics, one batch",
     }
 
@@ -221,17 +229,14 @@ def reference_arm(args, world, rank):
     grid, xs, source, counts = workload()
     import oracle
 
-    tab = xs.build_tables(0.2, 0.05, source.max_energy * (1 + 1e-6))
-    gs = xs.gs_grid_for(tab, [0])
     threads = oracle.max_threads()
-    per_col = 200  # bounded sample per beamlet per step
-    times, done = [], int(np.sum(np.minimum(counts, per_col)))
-    for step in range(args.warmup + args.steps):
-        t0 = time.perf_counter()
-        oracle.run(grid, tab, gs, source, counts=list(counts), n_batches=1, seed=SEED + step,
-                   forward=False, n_threads=threads, max_histories=per_col)
-        if step >= args.warmup:
-            times.append(time.perf_counter() - t0)
+    # the first warm-up step sizes the per-step sample (~10 s of CPU work)
+    per_col, _, _ = calibrate_sample(grid, xs, source, counts, 10.0)
+    times, done = [], 0
+    for step in range(max(0, args.warmup - 1) + args.steps):
+        elapsed, done = _oracle_sample(grid, xs, source, counts, per_col, SEED + step)
+        if step >= max(0, args.warmup - 1):
+            times.append(elapsed)
     total = sum(times)
     value = done * len(times) / total
     line = {
