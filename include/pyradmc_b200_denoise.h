@@ -1,0 +1,108 @@
+/*
+ * pyradmc_b200_denoise.h — C-ABI of the Dij-column denoiser (libpmc_b200.so).
+ *
+ * No counterpart in pyRadMC: the reference has no learned component.  A small
+ * 3D U-Net maps a low-history dose column (plus the density) to an estimate of
+ * the high-history column.  These entry points are its building blocks; the
+ * network, its training loop and its use on a Dij live in the host module
+ * pyradmc_b200/denoiser.py.
+ *
+ * Conventions
+ *   - All pointers are DEVICE pointers of the current device; `stream` is a
+ *     cudaStream_t (NULL = the default stream).  Calls enqueue work and return
+ *     without waiting.
+ *   - Activations are bf16 (raw 16-bit storage, passed as void*) in NDHWC
+ *     order: channels innermost, then x, y, z, batch.  Every channel count is
+ *     a multiple of 8 (16-byte rows).
+ *   - A 3x3x3 convolution's weights are bf16 [cout][kpad] with column
+ *     k = tap * cin + ci, tap = kz * 9 + ky * 3 + kx (the tap at offset
+ *     (kz-1, ky-1, kx-1)), and columns k >= 27 * cin zero.  kpad is 27 * cin
+ *     rounded up to a multiple of 64.  Convolutions have stride 1 and zero
+ *     padding 1; products accumulate in fp32.
+ *   - Return 0 on success, -1 for arguments outside what the kernels support
+ *     (nothing launched), -2 when a launch failed.
+ */
+#ifndef PYRADMC_B200_DENOISE_H
+#define PYRADMC_B200_DENOISE_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* y = act(conv3d(x, w) + bias) in bf16; relu != 0 selects ReLU.  bias is fp32
+ * [cout] or NULL.  cout in {8, 16, 32, 48, 64, 96, 128, 192}.  The data
+ * gradient of a convolution is this call on the output gradient with the
+ * weights from pmd_flip_weights (cin and cout swapped, relu = 0). */
+int pmd_conv3d(const void* x, const void* w, const float* bias, void* y, int n, int d, int h,
+               int w_, int cin, int cout, int kpad, int relu, void* stream);
+
+/* Weight gradient, ADDED into fp32 dw [cout][kpad] (and dbias [cout] when not
+ * NULL): dw[co][k] += sum over voxels of g[v][co] * im2col(x)[v][k].
+ * cout in {16, 32, 64, 128}.  The sum order is not fixed (fp32 atomics). */
+int pmd_conv3d_wgrad(const void* x, const void* g, float* dw, float* dbias, int n, int d, int h,
+                     int w_, int cin, int cout, int kpad, void* stream);
+
+/* Data-gradient weights: wd[ci][tap * cout + co] = w[co][(26 - tap) * cin + ci],
+ * bf16 [cin][kpad_d], columns past 27 * cout zero. */
+int pmd_flip_weights(const void* w, void* wd, int cin, int cout, int kpad, int kpad_d, void* stream);
+
+/* ReLU backward in place: g[i] = 0 where y[i] <= 0 (n elements). */
+int pmd_relu_mask(void* g, const void* y, int64_t n, void* stream);
+
+/* 2x2x2 average pooling of x [n, d, h, w, c] into y [n, d/2, h/2, w/2, c], and
+ * its gradient (written, or added onto gx when accumulate != 0). */
+int pmd_avgpool(const void* x, void* y, int n, int d, int h, int w, int c, void* stream);
+int pmd_avgpool_grad(const void* gy, void* gx, int n, int d, int h, int w, int c, int accumulate,
+                     void* stream);
+
+/* Decoder join: out [n, d, h, w, c_up + c_skip] = concat(nearest-upsample x2 of
+ * up [n, d/2, h/2, w/2, c_up], skip), and its gradient (the skip part written,
+ * or added onto gskip when accumulate != 0). */
+int pmd_upcat(const void* up, const void* skip, void* out, int n, int d, int h, int w, int c_up,
+              int c_skip, void* stream);
+int pmd_upcat_grad(const void* gout, void* gup, void* gskip, int n, int d, int h, int w, int c_up,
+                   int c_skip, int accumulate, void* stream);
+
+/* Output head: out[m] = base[m] + b[0] + sum_c w[c] * f[m][c] over m voxels
+ * (fp32; base may be NULL), and its gradient: df = g w^T (bf16), dw += f^T g,
+ * db += sum g (c <= 64). */
+int pmd_head(const void* f, const float* w, const float* b, const float* base, float* out,
+             int64_t m, int c, void* stream);
+int pmd_head_grad(const void* f, const float* w, const float* g, void* df, float* dw, float* db,
+                  int64_t m, int c, void* stream);
+
+/* Loss l = mean_m |pred - target| * (1 + lambda * weight[m]) ADDED into
+ * loss[0], and grad = dl/dpred (weight may be NULL). */
+int pmd_loss(const float* pred, const float* target, const float* weight, float lambda,
+             float* grad, float* loss, int64_t m, void* stream);
+
+/* Adam (Kingma & Ba) on n fp32 parameters at step >= 1; refreshes the bf16
+ * copy p16 (same indexing) when not NULL. */
+int pmd_adam(float* p, const float* g, float* m, float* v, void* p16, int64_t n, float lr,
+             float beta1, float beta2, float eps, int step, void* stream);
+
+/* Network input, 8 channels [m][8]: dose[m] / colmax[m / vox] (colmax NULL:
+ * no scaling; a zero maximum scales by 1), density[m % vox] when
+ * density_shared != 0 else density[m], and six zero channels.  base (fp32,
+ * may be NULL) receives the scaled dose. */
+int pmd_pack_input(const float* dose, const float* density, const float* colmax, int64_t vox,
+                   int density_shared, void* x, float* base, int64_t m, void* stream);
+
+/* Dense columns from a CSC matrix: dense[col * vox + indices[j]] = values[j]
+ * (float) for j in [indptr[col], indptr[col + 1]); the rest of dense must be
+ * zeroed by the caller.  Also colmax[col] = max of the column's values
+ * (colmax zeroed by the caller).  n_cols <= 65535. */
+int pmd_csc_to_dense(const int64_t* indptr, const int64_t* indices, const double* values,
+                     int n_cols, int64_t vox, float* dense, float* colmax, void* stream);
+
+/* Back to dose units: mean[m] = max(out[m], 0) * colmax[m / vox] (float64). */
+int pmd_unscale(const float* out, const float* colmax, int64_t vox, double* mean, int64_t m,
+                void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PYRADMC_B200_DENOISE_H */

@@ -227,6 +227,30 @@ SIGNATURES: dict[str, tuple[object, list]] = {
     ),
 }
 
+# The denoiser's entry points (include/pyradmc_b200_denoise.h); every pointer is
+# a device address.
+_v = C.c_void_p
+_i = C.c_int
+_l = C.c_int64
+_f = C.c_float
+SIGNATURES.update({
+    "pmd_conv3d": (_i, [_v, _v, _v, _v, _i, _i, _i, _i, _i, _i, _i, _i, _v]),
+    "pmd_conv3d_wgrad": (_i, [_v, _v, _v, _v, _i, _i, _i, _i, _i, _i, _i, _v]),
+    "pmd_flip_weights": (_i, [_v, _v, _i, _i, _i, _i, _v]),
+    "pmd_relu_mask": (_i, [_v, _v, _l, _v]),
+    "pmd_avgpool": (_i, [_v, _v, _i, _i, _i, _i, _i, _v]),
+    "pmd_avgpool_grad": (_i, [_v, _v, _i, _i, _i, _i, _i, _i, _v]),
+    "pmd_upcat": (_i, [_v, _v, _v, _i, _i, _i, _i, _i, _i, _v]),
+    "pmd_upcat_grad": (_i, [_v, _v, _v, _i, _i, _i, _i, _i, _i, _i, _v]),
+    "pmd_head": (_i, [_v, _v, _v, _v, _v, _l, _i, _v]),
+    "pmd_head_grad": (_i, [_v, _v, _v, _v, _v, _v, _l, _i, _v]),
+    "pmd_loss": (_i, [_v, _v, _v, _f, _v, _v, _l, _v]),
+    "pmd_adam": (_i, [_v, _v, _v, _v, _v, _l, _f, _f, _f, _f, _i, _v]),
+    "pmd_pack_input": (_i, [_v, _v, _v, _l, _i, _v, _v, _l, _v]),
+    "pmd_csc_to_dense": (_i, [_v, _v, _v, _i, _l, _v, _v, _v]),
+    "pmd_unscale": (_i, [_v, _v, _l, _v, _l, _v]),
+})
+
 PROGRESS_FN = C.CFUNCTYPE(None, C.c_void_p, C.c_int64)
 
 _lib: C.CDLL | None = None

@@ -1,8 +1,10 @@
 """Build the sm_100a shared library of the B200 backend, in-tree.
 
-``python -m pyradmc_b200.build`` compiles ``csrc/pmc_runtime.cu`` (which includes
-every kernel header) with nvcc for ``sm_100a`` into ``_lib/libpmc_b200.so``.  The
-library is rebuilt only when a source is newer than it, unless ``force`` is set.
+``python -m pyradmc_b200.build`` compiles each translation unit in ``csrc/``
+(``pmc_runtime.cu``, which includes every transport kernel header, and
+``denoise.cu``) with nvcc for ``sm_100a``, in parallel, and links them into
+``_lib/libpmc_b200.so``.  The library is rebuilt only when a source is newer than
+it, unless ``force`` is set.
 """
 
 from __future__ import annotations
@@ -30,9 +32,8 @@ NVCC_FLAGS = [
     "--expt-relaxed-constexpr",
     "-Xcompiler",
     "-fPIC",
-    "-shared",
-    "-lcudart",
 ]
+UNITS = ("pmc_runtime.cu", "denoise.cu")
 
 
 def nvcc() -> str:
@@ -60,19 +61,36 @@ def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) 
     if not force and not needs_build():
         return LIBRARY
     LIBDIR.mkdir(exist_ok=True)
-    tmp = LIBRARY.with_suffix(f".so.tmp{os.getpid()}")
-    cmd = [nvcc(), *ARCH_FLAGS, *NVCC_FLAGS, f"-I{INCLUDE}", str(CSRC / "pmc_runtime.cu"), "-o", str(tmp)]
-    if ptxas_info:
-        cmd.insert(1, "-Xptxas=-v")
-    if verbose:
-        print(" ".join(cmd), file=sys.stderr)
-    proc = subprocess.run(cmd, capture_output=True, text=True)
-    if proc.returncode != 0:
+    tag = f"tmp{os.getpid()}"
+    tmp = LIBRARY.with_suffix(f".so.{tag}")
+    objects = [LIBDIR / f"{Path(u).stem}.{tag}.o" for u in UNITS]
+    procs = []
+    for unit, obj in zip(UNITS, objects):
+        cmd = [nvcc(), *ARCH_FLAGS, *NVCC_FLAGS, f"-I{INCLUDE}", "-c", str(CSRC / unit), "-o", str(obj)]
+        if ptxas_info:
+            cmd.insert(1, "-Xptxas=-v")
+        if verbose:
+            print(" ".join(cmd), file=sys.stderr)
+        procs.append(subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True))
+    failures = []
+    for proc in procs:
+        out, err = proc.communicate()
+        if proc.returncode != 0:
+            failures.append(f"nvcc failed ({proc.returncode}):\n{out}\n{err}")
+        elif ptxas_info or verbose:
+            sys.stderr.write(err)
+    try:
+        if failures:
+            raise RuntimeError("\n".join(failures))
+        link = [nvcc(), *ARCH_FLAGS, "-shared", *(str(o) for o in objects), "-lcudart", "-o", str(tmp)]
+        proc = subprocess.run(link, capture_output=True, text=True)
+        if proc.returncode != 0:
+            raise RuntimeError(f"nvcc link failed ({proc.returncode}):\n{proc.stdout}\n{proc.stderr}")
+        tmp.replace(LIBRARY)
+    finally:
         tmp.unlink(missing_ok=True)
-        raise RuntimeError(f"nvcc failed ({proc.returncode}):\n{proc.stdout}\n{proc.stderr}")
-    if ptxas_info or verbose:
-        sys.stderr.write(proc.stderr)
-    tmp.replace(LIBRARY)
+        for obj in objects:
+            obj.unlink(missing_ok=True)
     return LIBRARY
 
 

@@ -1,0 +1,744 @@
+// denoise.cu — the 3D U-Net denoiser's kernels (no counterpart in pyRadMC).
+//
+// Activations are bf16 in NDHWC (channels innermost); weights bf16 as
+// [Cout][Kpad] with K = tap * Cin + ci over the 27 taps of a 3x3x3 kernel
+// (zero padded to a multiple of 64); every product accumulates in fp32.
+//
+// Convolution is an implicit GEMM on the tensor cores (mma.sync m16n8k16
+// bf16 -> fp32): M = voxels, N = output channels, K = 27 * Cin.  The A tile is
+// gathered straight from the activation with 16-byte cp.async copies whose
+// zero-fill form supplies the convolution's zero padding, double-buffered
+// against the MMAs.  The same kernel runs the data gradient (with flipped,
+// transposed weights); the weight gradient is a second implicit GEMM that
+// reduces over voxels and adds its fp32 partial into the gradient buffer.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "pyradmc_b200_denoise.h"
+
+namespace pmd {
+
+constexpr int kBM = 64;      // voxels per CTA tile
+constexpr int kBK = 32;      // K per pipeline stage
+constexpr int kPadK = 8;     // smem row padding (elements) against ldmatrix bank conflicts
+constexpr int kRowK = kBK + kPadK;
+constexpr int kThreads = 128;
+
+struct ConvShape {
+    int n, d, h, w;     // batch and spatial size (stride 1, padding 1)
+    int cin, cout;      // cin % 8 == 0, cout % 8 == 0
+    int kpad;           // 27 * cin rounded up to a multiple of 64
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void cp_async16(void* dst, const void* src, bool valid) {
+    const int n = valid ? 16 : 0;  // src-size 0: the 16 destination bytes are zero-filled
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(smem_u32(dst)), "l"(src),
+                 "r"(n));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
+}
+
+__device__ __forceinline__ void ldmatrix_x4(uint32_t& r0, uint32_t& r1, uint32_t& r2, uint32_t& r3,
+                                            const void* p) {
+    asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];\n"
+                 : "=r"(r0), "=r"(r1), "=r"(r2), "=r"(r3)
+                 : "r"(smem_u32(p)));
+}
+__device__ __forceinline__ void ldmatrix_x2(uint32_t& r0, uint32_t& r1, const void* p) {
+    asm volatile("ldmatrix.sync.aligned.m8n8.x2.shared.b16 {%0,%1}, [%2];\n"
+                 : "=r"(r0), "=r"(r1)
+                 : "r"(smem_u32(p)));
+}
+__device__ __forceinline__ void ldmatrix_x2_t(uint32_t& r0, uint32_t& r1, const void* p) {
+    asm volatile("ldmatrix.sync.aligned.m8n8.x2.trans.shared.b16 {%0,%1}, [%2];\n"
+                 : "=r"(r0), "=r"(r1)
+                 : "r"(smem_u32(p)));
+}
+__device__ __forceinline__ void ldmatrix_x4_t(uint32_t& r0, uint32_t& r1, uint32_t& r2, uint32_t& r3,
+                                              const void* p) {
+    asm volatile("ldmatrix.sync.aligned.m8n8.x4.trans.shared.b16 {%0,%1,%2,%3}, [%4];\n"
+                 : "=r"(r0), "=r"(r1), "=r"(r2), "=r"(r3)
+                 : "r"(smem_u32(p)));
+}
+
+__device__ __forceinline__ void mma_bf16(float* d, uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3,
+                                         uint32_t b0, uint32_t b1) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, "
+        "{%8,%9}, {%0,%1,%2,%3};\n"
+        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+        : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+}
+
+// Source of one 8-channel chunk of the implicit A matrix: voxel m's neighbour
+// at tap (k / cin) and channels (k % cin) .. +7; null when it lies in the
+// zero padding or past K.
+__device__ __forceinline__ const __nv_bfloat16* a_chunk(const __nv_bfloat16* x, const ConvShape& s,
+                                                        int nz, int zz, int yy, int xx, int k) {
+    if (k >= 27 * s.cin) return nullptr;
+    const int tap = k / s.cin;
+    const int ci = k - tap * s.cin;
+    const int z = zz + tap / 9 - 1;
+    const int y = yy + (tap / 3) % 3 - 1;
+    const int xq = xx + tap % 3 - 1;
+    if ((unsigned)z >= (unsigned)s.d || (unsigned)y >= (unsigned)s.h || (unsigned)xq >= (unsigned)s.w)
+        return nullptr;
+    return x + ((((long long)nz * s.d + z) * s.h + y) * s.w + xq) * s.cin + ci;
+}
+
+// ---- forward / data-gradient convolution ------------------------------------------
+// Y[m][co] = act(bias[co] + sum_k A[m][k] W[co][k]).  BN = cout (a multiple of 8).
+// Four warps; warp w owns tile rows 16w .. 16w+15 and every output channel.
+template <int BN>
+__global__ void __launch_bounds__(kThreads)
+conv3d_kernel(const __nv_bfloat16* __restrict__ x, const __nv_bfloat16* __restrict__ wt,
+              const float* __restrict__ bias, __nv_bfloat16* __restrict__ y, ConvShape s, int relu) {
+    __shared__ __align__(16) __nv_bfloat16 As[2][kBM][kRowK];
+    __shared__ __align__(16) __nv_bfloat16 Bs[2][BN][kRowK];
+    const int tid = threadIdx.x;
+    const int lane = tid & 31, warp = tid >> 5;
+    const long long m_total = (long long)s.n * s.d * s.h * s.w;
+    const long long m0 = (long long)blockIdx.x * kBM;
+
+    // each thread gathers rows tid / 4 and tid / 4 + 32, 8-element chunk tid % 4
+    const int chunk = tid & 3;
+    int rz[2], ry[2], rx[2], rn[2];
+    bool rvalid[2];
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+        const long long m = m0 + (tid >> 2) + 32 * i;
+        rvalid[i] = m < m_total;
+        long long t = rvalid[i] ? m : 0;
+        rx[i] = (int)(t % s.w);
+        t /= s.w;
+        ry[i] = (int)(t % s.h);
+        t /= s.h;
+        rz[i] = (int)(t % s.d);
+        rn[i] = (int)(t / s.d);
+    }
+
+    auto load_stage = [&](int stage, int kb) {
+        const int k = kb * kBK + chunk * 8;
+#pragma unroll
+        for (int i = 0; i < 2; ++i) {
+            const __nv_bfloat16* src = rvalid[i] ? a_chunk(x, s, rn[i], rz[i], ry[i], rx[i], k) : nullptr;
+            cp_async16(&As[stage][(tid >> 2) + 32 * i][chunk * 8], src ? src : x, src != nullptr);
+        }
+        for (int c = tid; c < BN * 4; c += kThreads) {
+            const int row = c >> 2, cc = c & 3;
+            cp_async16(&Bs[stage][row][cc * 8], wt + (long long)row * s.kpad + kb * kBK + cc * 8, true);
+        }
+        cp_async_commit();
+    };
+
+    float acc[BN / 8][4];
+#pragma unroll
+    for (int j = 0; j < BN / 8; ++j) acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.0f;
+
+    const int n_kb = s.kpad / kBK;
+    load_stage(0, 0);
+    for (int kb = 0; kb < n_kb; ++kb) {
+        const int cur = kb & 1;
+        if (kb + 1 < n_kb) {
+            load_stage(cur ^ 1, kb + 1);
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
+        }
+        __syncthreads();
+#pragma unroll
+        for (int ks = 0; ks < kBK / 16; ++ks) {
+            uint32_t a0, a1, a2, a3;
+            ldmatrix_x4(a0, a1, a2, a3, &As[cur][warp * 16 + (lane & 15)][ks * 16 + (lane >> 4) * 8]);
+#pragma unroll
+            for (int j = 0; j < BN / 8; ++j) {
+                uint32_t b0, b1;
+                ldmatrix_x2(b0, b1, &Bs[cur][j * 8 + (lane & 7)][ks * 16 + ((lane >> 3) & 1) * 8]);
+                mma_bf16(acc[j], a0, a1, a2, a3, b0, b1);
+            }
+        }
+        __syncthreads();
+    }
+
+    // epilogue: bias, ReLU, bf16, NDHWC store
+    const int r_lo = warp * 16 + (lane >> 2);
+#pragma unroll
+    for (int half = 0; half < 2; ++half) {
+        const long long m = m0 + r_lo + 8 * half;
+        if (m >= m_total) continue;
+        __nv_bfloat16* out = y + m * s.cout;
+#pragma unroll
+        for (int j = 0; j < BN / 8; ++j) {
+            const int co = j * 8 + (lane & 3) * 2;
+            float v0 = acc[j][2 * half], v1 = acc[j][2 * half + 1];
+            if (bias) {
+                v0 += bias[co];
+                v1 += bias[co + 1];
+            }
+            if (relu) {
+                v0 = fmaxf(v0, 0.0f);
+                v1 = fmaxf(v1, 0.0f);
+            }
+            *reinterpret_cast<__nv_bfloat162*>(out + co) = __floats2bfloat162_rn(v0, v1);
+        }
+    }
+}
+
+// ---- weight gradient ----------------------------------------------------------------
+// dW[co][k] += sum_m G[m][co] A[m][k] over this CTA's voxel range.  Grid: x =
+// 64-wide k tiles, y = voxel splits.  MMA rows = co (BC = cout), cols = k,
+// reduction = voxels; both operands come from voxel-major smem tiles through
+// transposing ldmatrix loads.
+constexpr int kWK = 64;   // k columns per CTA
+constexpr int kWM = 32;   // voxels per pipeline stage
+template <int BC>
+__global__ void __launch_bounds__(kThreads)
+conv3d_wgrad_kernel(const __nv_bfloat16* __restrict__ x, const __nv_bfloat16* __restrict__ g,
+                    float* __restrict__ dw, float* __restrict__ dbias, ConvShape s,
+                    long long voxels_per_split) {
+    __shared__ __align__(16) __nv_bfloat16 Gs[2][kWM][BC + 8];
+    __shared__ __align__(16) __nv_bfloat16 Xs[2][kWM][kWK + 8];
+    const int tid = threadIdx.x;
+    const int lane = tid & 31, warp = tid >> 5;
+    const long long m_total = (long long)s.n * s.d * s.h * s.w;
+    const long long v_begin = (long long)blockIdx.y * voxels_per_split;
+    const long long v_end = min(v_begin + voxels_per_split, m_total);
+    const int k0 = blockIdx.x * kWK;
+    // warp tiling of the (BC x 64) output: BC/16 row tiles x 8 col tiles over 4 warps
+    constexpr int kRowTiles = BC / 16;
+    constexpr int kTiles = kRowTiles * (kWK / 8);
+    constexpr int kPerWarp = (kTiles + 3) / 4;
+    float acc[kPerWarp][4];
+#pragma unroll
+    for (int t = 0; t < kPerWarp; ++t) acc[t][0] = acc[t][1] = acc[t][2] = acc[t][3] = 0.0f;
+    float bacc = 0.0f;  // bias gradient: thread tid < BC sums column tid of G
+
+    auto load_stage = [&](int stage, long long v0) {
+        // G tile: kWM voxels x BC channels
+        for (int c = tid; c < kWM * (BC / 8); c += kThreads) {
+            const int row = c / (BC / 8), cc = c % (BC / 8);
+            const long long v = v0 + row;
+            const bool ok = v < v_end;
+            cp_async16(&Gs[stage][row][cc * 8], ok ? g + v * s.cout + cc * 8 : g, ok);
+        }
+        // im2col tile: kWM voxels x kWK k
+        for (int c = tid; c < kWM * (kWK / 8); c += kThreads) {
+            const int row = c / (kWK / 8), cc = c % (kWK / 8);
+            const long long v = v0 + row;
+            const __nv_bfloat16* src = nullptr;
+            if (v < v_end) {
+                long long t = v;
+                const int xx = (int)(t % s.w);
+                t /= s.w;
+                const int yy = (int)(t % s.h);
+                t /= s.h;
+                const int zz = (int)(t % s.d);
+                const int nz = (int)(t / s.d);
+                src = a_chunk(x, s, nz, zz, yy, xx, k0 + cc * 8);
+            }
+            cp_async16(&Xs[stage][row][cc * 8], src ? src : x, src != nullptr);
+        }
+        cp_async_commit();
+    };
+
+    const long long n_steps = (v_end - v_begin + kWM - 1) / kWM;
+    if (n_steps <= 0) return;
+    load_stage(0, v_begin);
+    for (long long st = 0; st < n_steps; ++st) {
+        const int cur = (int)(st & 1);
+        if (st + 1 < n_steps) {
+            load_stage(cur ^ 1, v_begin + (st + 1) * kWM);
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
+        }
+        __syncthreads();
+        if (dbias != nullptr && blockIdx.x == 0 && tid < BC) {
+#pragma unroll 4
+            for (int r = 0; r < kWM; ++r) bacc += __bfloat162float(Gs[cur][r][tid]);
+        }
+#pragma unroll
+        for (int ks = 0; ks < kWM / 16; ++ks) {
+#pragma unroll
+            for (int t = 0; t < kPerWarp; ++t) {
+                const int tile = warp * kPerWarp + t;
+                if (tile >= kTiles) break;
+                const int rt = tile / (kWK / 8), ct = tile % (kWK / 8);
+                uint32_t a0, a1, a2, a3, b0, b1;
+                // A = G^T: rows co (16), cols voxels (16)
+                {
+                    const int q = lane >> 3, r = lane & 7;
+                    const int vrow = ks * 16 + (q >> 1) * 8 + r;
+                    const int col = rt * 16 + (q & 1) * 8;
+                    ldmatrix_x4_t(a0, a1, a2, a3, &Gs[cur][vrow][col]);
+                }
+                // B = im2col: K = voxels (16), N = k (8); lanes 0-15 address its two 8x8 halves
+                {
+                    const int vrow = ks * 16 + (lane & 15);
+                    ldmatrix_x2_t(b0, b1, &Xs[cur][vrow][ct * 8]);
+                }
+                mma_bf16(acc[t], a0, a1, a2, a3, b0, b1);
+            }
+        }
+        __syncthreads();
+    }
+    // add this split's partial into dW (fp32)
+#pragma unroll
+    for (int t = 0; t < kPerWarp; ++t) {
+        const int tile = warp * kPerWarp + t;
+        if (tile >= kTiles) break;
+        const int rt = tile / (kWK / 8), ct = tile % (kWK / 8);
+        const int co = rt * 16 + (lane >> 2);
+        const int k = k0 + ct * 8 + (lane & 3) * 2;
+        atomicAdd(dw + (long long)co * s.kpad + k, acc[t][0]);
+        atomicAdd(dw + (long long)co * s.kpad + k + 1, acc[t][1]);
+        atomicAdd(dw + (long long)(co + 8) * s.kpad + k, acc[t][2]);
+        atomicAdd(dw + (long long)(co + 8) * s.kpad + k + 1, acc[t][3]);
+    }
+    if (dbias != nullptr && blockIdx.x == 0 && tid < BC) atomicAdd(dbias + tid, bacc);
+}
+
+// ---- element-wise and data-movement kernels -------------------------------------------
+// ReLU backward in place: g <- g * (y > 0).
+__global__ void relu_mask_kernel(__nv_bfloat16* g, const __nv_bfloat16* y, long long n) {
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
+        if (!(__bfloat162float(y[i]) > 0.0f)) g[i] = __float2bfloat16(0.0f);
+}
+
+// Weights for the data gradient: Wd[ci][tap' * cout + co] = W[co][(26 - tap') * cin + ci].
+__global__ void flip_weights_kernel(const __nv_bfloat16* w, __nv_bfloat16* wd, int cin, int cout,
+                                    int kpad, int kpad_d) {
+    const long long n = (long long)cin * kpad_d;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const int ci = (int)(i / kpad_d), k = (int)(i % kpad_d);
+        __nv_bfloat16 v = __float2bfloat16(0.0f);
+        if (k < 27 * cout) {
+            const int tap = k / cout, co = k % cout;
+            v = w[(long long)co * kpad + (26 - tap) * cin + ci];
+        }
+        wd[i] = v;
+    }
+}
+
+// 2x2x2 average pooling, NDHWC; and its gradient (each input voxel gets 1/8).
+__global__ void avgpool_kernel(const __nv_bfloat16* x, __nv_bfloat16* y, int n, int d, int h, int w,
+                               int c) {
+    const int d2 = d / 2, h2 = h / 2, w2 = w / 2;
+    const long long total = (long long)n * d2 * h2 * w2 * c;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += stride) {
+        long long t = i;
+        const int ch = (int)(t % c); t /= c;
+        const int xx = (int)(t % w2); t /= w2;
+        const int yy = (int)(t % h2); t /= h2;
+        const int zz = (int)(t % d2);
+        const int nn = (int)(t / d2);
+        float s = 0.0f;
+        for (int dz = 0; dz < 2; ++dz)
+            for (int dy = 0; dy < 2; ++dy)
+                for (int dx = 0; dx < 2; ++dx)
+                    s += __bfloat162float(
+                        x[((((long long)nn * d + 2 * zz + dz) * h + 2 * yy + dy) * w + 2 * xx + dx) * c + ch]);
+        y[i] = __float2bfloat16(0.125f * s);
+    }
+}
+
+__global__ void avgpool_grad_kernel(const __nv_bfloat16* gy, __nv_bfloat16* gx, int n, int d, int h,
+                                    int w, int c, int accumulate) {
+    const long long total = (long long)n * d * h * w * c;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += stride) {
+        long long t = i;
+        const int ch = (int)(t % c); t /= c;
+        const int xx = (int)(t % w); t /= w;
+        const int yy = (int)(t % h); t /= h;
+        const int zz = (int)(t % d);
+        const int nn = (int)(t / d);
+        const float v = 0.125f * __bfloat162float(
+            gy[((((long long)nn * (d / 2) + zz / 2) * (h / 2) + yy / 2) * (w / 2) + xx / 2) * c + ch]);
+        gx[i] = __float2bfloat16(accumulate ? v + __bfloat162float(gx[i]) : v);
+    }
+}
+
+// Nearest 2x upsampling of `up` (c_up channels) into channels [0, c_up) of a
+// concatenated tensor whose channels [c_up, c_up + c_skip) copy the skip input.
+__global__ void upcat_kernel(const __nv_bfloat16* up, const __nv_bfloat16* skip, __nv_bfloat16* out,
+                             int n, int d, int h, int w, int c_up, int c_skip) {
+    const int c = c_up + c_skip;
+    const long long total = (long long)n * d * h * w * c;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += stride) {
+        long long t = i;
+        const int ch = (int)(t % c); t /= c;
+        const long long vox = t;
+        const int xx = (int)(t % w); t /= w;
+        const int yy = (int)(t % h); t /= h;
+        const int zz = (int)(t % d);
+        const int nn = (int)(t / d);
+        __nv_bfloat16 v;
+        if (ch < c_up)
+            v = up[((((long long)nn * (d / 2) + zz / 2) * (h / 2) + yy / 2) * (w / 2) + xx / 2) * c_up + ch];
+        else
+            v = skip[vox * c_skip + (ch - c_up)];
+        out[i] = v;
+    }
+}
+
+// Gradient of upcat: the up part sums its 8 children; the skip part is copied
+// (added onto an existing skip gradient when `accumulate`).
+__global__ void upcat_grad_kernel(const __nv_bfloat16* gout, __nv_bfloat16* gup, __nv_bfloat16* gskip,
+                                  int n, int d, int h, int w, int c_up, int c_skip, int accumulate) {
+    const int c = c_up + c_skip;
+    const int d2 = d / 2, h2 = h / 2, w2 = w / 2;
+    const long long n_up = (long long)n * d2 * h2 * w2 * c_up;
+    const long long n_skip = (long long)n * d * h * w * c_skip;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n_up + n_skip; i += stride) {
+        if (i < n_up) {
+            long long t = i;
+            const int ch = (int)(t % c_up); t /= c_up;
+            const int xx = (int)(t % w2); t /= w2;
+            const int yy = (int)(t % h2); t /= h2;
+            const int zz = (int)(t % d2);
+            const int nn = (int)(t / d2);
+            float s = 0.0f;
+            for (int dz = 0; dz < 2; ++dz)
+                for (int dy = 0; dy < 2; ++dy)
+                    for (int dx = 0; dx < 2; ++dx)
+                        s += __bfloat162float(
+                            gout[((((long long)nn * d + 2 * zz + dz) * h + 2 * yy + dy) * w + 2 * xx + dx) * c + ch]);
+            gup[i] = __float2bfloat16(s);
+        } else {
+            const long long j = i - n_up;
+            const long long vox = j / c_skip;
+            const int ch = (int)(j % c_skip);
+            const float v = __bfloat162float(gout[vox * c + c_up + ch]);
+            gskip[j] = __float2bfloat16(accumulate ? v + __bfloat162float(gskip[j]) : v);
+        }
+    }
+}
+
+// Head: out[m] = base[m] + b + sum_c w[c] f[m][c] (a 1x1x1 conv to one channel,
+// added to the noisy input dose: the network predicts a correction).
+__global__ void head_kernel(const __nv_bfloat16* f, const float* w, const float* b, const float* base,
+                            float* out, long long m_total, int c) {
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long m = (long long)blockIdx.x * blockDim.x + threadIdx.x; m < m_total; m += stride) {
+        float s = b[0] + (base ? base[m] : 0.0f);
+        for (int k = 0; k < c; ++k) s += w[k] * __bfloat162float(f[m * c + k]);
+        out[m] = s;
+    }
+}
+
+// Loss (L1 plus an L1 weighted by the target's precision) and its gradient with
+// respect to the prediction:
+//   l = |p - t| * (1 + lambda * weight),  dl/dp = sign(p - t) * (1 + lambda * weight),
+// both divided by the voxel count.  Partial sums accumulate into loss[0].
+__global__ void loss_kernel(const float* pred, const float* target, const float* weight,
+                            float lambda, float* grad, float* loss, long long m_total) {
+    float local = 0.0f;
+    const float inv_n = 1.0f / (float)m_total;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long m = (long long)blockIdx.x * blockDim.x + threadIdx.x; m < m_total; m += stride) {
+        const float diff = pred[m] - target[m];
+        const float wgt = 1.0f + lambda * (weight ? weight[m] : 0.0f);
+        local += fabsf(diff) * wgt;
+        grad[m] = (diff > 0.0f ? wgt : (diff < 0.0f ? -wgt : 0.0f)) * inv_n;
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) local += __shfl_xor_sync(0xffffffffu, local, off);
+    if ((threadIdx.x & 31) == 0) atomicAdd(loss, local * inv_n);
+}
+
+// Head backward: dF[m][c] = g[m] w[c] (bf16), dW[c] += sum_m g[m] f[m][c], db += sum_m g[m].
+__global__ void head_grad_kernel(const __nv_bfloat16* f, const float* w, const float* g,
+                                 __nv_bfloat16* df, float* dw, float* db, long long m_total, int c) {
+    float lw[64];
+    for (int k = 0; k < c; ++k) lw[k] = 0.0f;
+    float lb = 0.0f;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long m = (long long)blockIdx.x * blockDim.x + threadIdx.x; m < m_total; m += stride) {
+        const float gm = g[m];
+        lb += gm;
+        for (int k = 0; k < c; ++k) {
+            lw[k] += gm * __bfloat162float(f[m * c + k]);
+            df[m * c + k] = __float2bfloat16(gm * w[k]);
+        }
+    }
+    for (int k = 0; k < c; ++k) {
+        float v = lw[k];
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+        if ((threadIdx.x & 31) == 0) atomicAdd(dw + k, v);
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) lb += __shfl_xor_sync(0xffffffffu, lb, off);
+    if ((threadIdx.x & 31) == 0) atomicAdd(db, lb);
+}
+
+// Adam on fp32 master parameters; refreshes the bf16 working copy (when given)
+// at the same flat index.
+__global__ void adam_kernel(float* p, const float* g, float* m, float* v, __nv_bfloat16* p16,
+                            long long n, float lr, float beta1, float beta2, float eps, float bc1,
+                            float bc2) {
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const float gi = g[i];
+        const float mi = beta1 * m[i] + (1.0f - beta1) * gi;
+        const float vi = beta2 * v[i] + (1.0f - beta2) * gi * gi;
+        m[i] = mi;
+        v[i] = vi;
+        const float pi = p[i] - lr * (mi / bc1) / (sqrtf(vi / bc2) + eps);
+        p[i] = pi;
+        if (p16) p16[i] = __float2bfloat16(pi);
+    }
+}
+
+// Network input: channel 0 the column-normalized dose, channel 1 the density,
+// 2..7 zero; one 16-byte store per voxel.
+__global__ void pack_input_kernel(const float* dose, const float* density, const float* colmax,
+                                  long long vox, int density_shared, __nv_bfloat16* x, float* base,
+                                  long long m_total) {
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long m = (long long)blockIdx.x * blockDim.x + threadIdx.x; m < m_total; m += stride) {
+        float scale = 1.0f;
+        if (colmax) {
+            const float c = colmax[m / vox];
+            scale = c > 0.0f ? 1.0f / c : 1.0f;
+        }
+        const float v = dose[m] * scale;
+        const float rho = density[density_shared ? m % vox : m];
+        if (base) base[m] = v;
+        union {
+            uint4 u;
+            __nv_bfloat162 h[4];
+        } pk;
+        pk.h[0] = __floats2bfloat162_rn(v, rho);
+        pk.h[1] = pk.h[2] = pk.h[3] = __floats2bfloat162_rn(0.0f, 0.0f);
+        *reinterpret_cast<uint4*>(x + m * 8) = pk.u;
+    }
+}
+
+// CSC -> dense columns, with each column's maximum (values are non-negative, so
+// the float bit patterns order like the values).
+__global__ void csc_to_dense_kernel(const int64_t* indptr, const int64_t* indices,
+                                    const double* values, long long vox, float* dense,
+                                    float* colmax) {
+    const int col = blockIdx.y;
+    const long long begin = indptr[col], end = indptr[col + 1];
+    float local = 0.0f;
+    for (long long j = begin + (long long)blockIdx.x * blockDim.x + threadIdx.x; j < end;
+         j += (long long)gridDim.x * blockDim.x) {
+        const float v = (float)values[j];
+        dense[(long long)col * vox + indices[j]] = v;
+        local = fmaxf(local, v);
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) local = fmaxf(local, __shfl_xor_sync(0xffffffffu, local, off));
+    if ((threadIdx.x & 31) == 0 && local > 0.0f)
+        atomicMax(reinterpret_cast<int*>(colmax + col), __float_as_int(local));
+}
+
+__global__ void unscale_kernel(const float* out, const float* colmax, long long vox, double* mean,
+                               long long m_total) {
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long m = (long long)blockIdx.x * blockDim.x + threadIdx.x; m < m_total; m += stride) {
+        const float c = colmax[m / vox];
+        mean[m] = (double)fmaxf(out[m], 0.0f) * (double)(c > 0.0f ? c : 1.0f);
+    }
+}
+
+}  // namespace pmd
+
+using namespace pmd;
+
+namespace {
+
+int grid_for(long long n, int block = 256) {
+    long long b = (n + block - 1) / block;
+    if (b > 148LL * 32) b = 148LL * 32;
+    return (int)(b < 1 ? 1 : b);
+}
+
+template <int BN>
+void launch_conv(const __nv_bfloat16* x, const __nv_bfloat16* w, const float* bias, __nv_bfloat16* y,
+                 ConvShape s, int relu, cudaStream_t st) {
+    const long long m = (long long)s.n * s.d * s.h * s.w;
+    conv3d_kernel<BN><<<(unsigned)((m + kBM - 1) / kBM), kThreads, 0, st>>>(x, w, bias, y, s, relu);
+}
+
+template <int BC>
+void launch_wgrad(const __nv_bfloat16* x, const __nv_bfloat16* g, float* dw, float* db, ConvShape s,
+                  cudaStream_t st) {
+    const long long m = (long long)s.n * s.d * s.h * s.w;
+    const int kt = s.kpad / kWK;
+    // enough voxel splits for ~4 CTAs per SM over all k tiles
+    long long splits = (148LL * 4 + kt - 1) / kt;
+    long long per = (m + splits - 1) / splits;
+    per = ((per + kWM - 1) / kWM) * kWM;
+    splits = (m + per - 1) / per;
+    conv3d_wgrad_kernel<BC><<<dim3(kt, (unsigned)splits), kThreads, 0, st>>>(x, g, dw, db, s, per);
+}
+
+int launched() { return cudaGetLastError() == cudaSuccess ? 0 : -2; }
+
+}  // namespace
+
+extern "C" {
+
+int pmd_conv3d(const void* x, const void* w, const float* bias, void* y, int n, int d, int h, int wd,
+               int cin, int cout, int kpad, int relu, void* stream) {
+    ConvShape s{n, d, h, wd, cin, cout, kpad};
+    if (n < 1 || d < 1 || h < 1 || wd < 1 || cin < 8 || cin % 8 || kpad % 64 || kpad < 27 * cin)
+        return -1;
+    auto X = (const __nv_bfloat16*)x;
+    auto W = (const __nv_bfloat16*)w;
+    auto Y = (__nv_bfloat16*)y;
+    cudaStream_t st = (cudaStream_t)stream;
+    switch (cout) {
+        case 8: launch_conv<8>(X, W, bias, Y, s, relu, st); break;
+        case 16: launch_conv<16>(X, W, bias, Y, s, relu, st); break;
+        case 32: launch_conv<32>(X, W, bias, Y, s, relu, st); break;
+        case 48: launch_conv<48>(X, W, bias, Y, s, relu, st); break;
+        case 64: launch_conv<64>(X, W, bias, Y, s, relu, st); break;
+        case 96: launch_conv<96>(X, W, bias, Y, s, relu, st); break;
+        case 128: launch_conv<128>(X, W, bias, Y, s, relu, st); break;
+        case 192: launch_conv<192>(X, W, bias, Y, s, relu, st); break;
+        default: return -1;
+    }
+    return launched();
+}
+
+int pmd_conv3d_wgrad(const void* x, const void* g, float* dw, float* dbias, int n, int d, int h,
+                     int wd, int cin, int cout, int kpad, void* stream) {
+    ConvShape s{n, d, h, wd, cin, cout, kpad};
+    if (n < 1 || d < 1 || h < 1 || wd < 1 || cin < 8 || cin % 8 || kpad % kWK || kpad < 27 * cin)
+        return -1;
+    auto X = (const __nv_bfloat16*)x;
+    auto G = (const __nv_bfloat16*)g;
+    cudaStream_t st = (cudaStream_t)stream;
+    switch (cout) {
+        case 16: launch_wgrad<16>(X, G, dw, dbias, s, st); break;
+        case 32: launch_wgrad<32>(X, G, dw, dbias, s, st); break;
+        case 64: launch_wgrad<64>(X, G, dw, dbias, s, st); break;
+        case 128: launch_wgrad<128>(X, G, dw, dbias, s, st); break;
+        default: return -1;
+    }
+    return launched();
+}
+
+int pmd_flip_weights(const void* w, void* wd, int cin, int cout, int kpad, int kpad_d, void* stream) {
+    if (cin < 1 || cout < 1 || kpad < 27 * cin || kpad_d < 27 * cout) return -1;
+    flip_weights_kernel<<<grid_for((long long)cin * kpad_d), 256, 0, (cudaStream_t)stream>>>(
+        (const __nv_bfloat16*)w, (__nv_bfloat16*)wd, cin, cout, kpad, kpad_d);
+    return launched();
+}
+
+int pmd_relu_mask(void* g, const void* y, int64_t n, void* stream) {
+    relu_mask_kernel<<<grid_for(n), 256, 0, (cudaStream_t)stream>>>((__nv_bfloat16*)g,
+                                                                    (const __nv_bfloat16*)y, n);
+    return launched();
+}
+
+int pmd_avgpool(const void* x, void* y, int n, int d, int h, int w, int c, void* stream) {
+    if (d % 2 || h % 2 || w % 2) return -1;
+    avgpool_kernel<<<grid_for((long long)n * d * h * w * c / 8), 256, 0, (cudaStream_t)stream>>>(
+        (const __nv_bfloat16*)x, (__nv_bfloat16*)y, n, d, h, w, c);
+    return launched();
+}
+
+int pmd_avgpool_grad(const void* gy, void* gx, int n, int d, int h, int w, int c, int accumulate,
+                     void* stream) {
+    if (d % 2 || h % 2 || w % 2) return -1;
+    avgpool_grad_kernel<<<grid_for((long long)n * d * h * w * c), 256, 0, (cudaStream_t)stream>>>(
+        (const __nv_bfloat16*)gy, (__nv_bfloat16*)gx, n, d, h, w, c, accumulate);
+    return launched();
+}
+
+int pmd_upcat(const void* up, const void* skip, void* out, int n, int d, int h, int w, int c_up,
+              int c_skip, void* stream) {
+    if (d % 2 || h % 2 || w % 2 || c_skip < 1) return -1;
+    upcat_kernel<<<grid_for((long long)n * d * h * w * (c_up + c_skip)), 256, 0, (cudaStream_t)stream>>>(
+        (const __nv_bfloat16*)up, (const __nv_bfloat16*)skip, (__nv_bfloat16*)out, n, d, h, w, c_up,
+        c_skip);
+    return launched();
+}
+
+int pmd_upcat_grad(const void* gout, void* gup, void* gskip, int n, int d, int h, int w, int c_up,
+                   int c_skip, int accumulate, void* stream) {
+    if (d % 2 || h % 2 || w % 2 || c_skip < 1) return -1;
+    const long long total = (long long)n * d * h * w * c_skip + (long long)n * d * h * w * c_up / 8;
+    upcat_grad_kernel<<<grid_for(total), 256, 0, (cudaStream_t)stream>>>(
+        (const __nv_bfloat16*)gout, (__nv_bfloat16*)gup, (__nv_bfloat16*)gskip, n, d, h, w, c_up,
+        c_skip, accumulate);
+    return launched();
+}
+
+int pmd_head(const void* f, const float* w, const float* b, const float* base, float* out,
+             int64_t m, int c, void* stream) {
+    head_kernel<<<grid_for(m), 256, 0, (cudaStream_t)stream>>>((const __nv_bfloat16*)f, w, b, base,
+                                                                out, m, c);
+    return launched();
+}
+
+int pmd_head_grad(const void* f, const float* w, const float* g, void* df, float* dw, float* db,
+                  int64_t m, int c, void* stream) {
+    if (c > 64) return -1;
+    head_grad_kernel<<<grid_for(m), 256, 0, (cudaStream_t)stream>>>(
+        (const __nv_bfloat16*)f, w, g, (__nv_bfloat16*)df, dw, db, m, c);
+    return launched();
+}
+
+int pmd_loss(const float* pred, const float* target, const float* weight, float lambda,
+             float* grad, float* loss, int64_t m, void* stream) {
+    loss_kernel<<<grid_for(m), 256, 0, (cudaStream_t)stream>>>(pred, target, weight, lambda, grad,
+                                                                loss, m);
+    return launched();
+}
+
+int pmd_adam(float* p, const float* g, float* m, float* v, void* p16, int64_t n, float lr,
+             float beta1, float beta2, float eps, int step, void* stream) {
+    if (step < 1) return -1;
+    const float bc1 = 1.0f - powf(beta1, (float)step);
+    const float bc2 = 1.0f - powf(beta2, (float)step);
+    adam_kernel<<<grid_for(n), 256, 0, (cudaStream_t)stream>>>(p, g, m, v, (__nv_bfloat16*)p16, n, lr,
+                                                                beta1, beta2, eps, bc1, bc2);
+    return launched();
+}
+
+int pmd_pack_input(const float* dose, const float* density, const float* colmax, int64_t vox,
+                   int density_shared, void* x, float* base, int64_t m, void* stream) {
+    if (vox < 1) return -1;
+    pack_input_kernel<<<grid_for(m), 256, 0, (cudaStream_t)stream>>>(
+        dose, density, colmax, vox, density_shared, (__nv_bfloat16*)x, base, m);
+    return launched();
+}
+
+int pmd_csc_to_dense(const int64_t* indptr, const int64_t* indices, const double* values,
+                     int n_cols, int64_t vox, float* dense, float* colmax, void* stream) {
+    if (n_cols < 0 || n_cols > 65535 || vox < 1) return -1;
+    if (n_cols == 0) return 0;
+    csc_to_dense_kernel<<<dim3(64, n_cols), 256, 0, (cudaStream_t)stream>>>(indptr, indices, values,
+                                                                            vox, dense, colmax);
+    return launched();
+}
+
+int pmd_unscale(const float* out, const float* colmax, int64_t vox, double* mean, int64_t m,
+                void* stream) {
+    if (vox < 1) return -1;
+    unscale_kernel<<<grid_for(m), 256, 0, (cudaStream_t)stream>>>(out, colmax, vox, mean, m);
+    return launched();
+}
+
+}  // extern "C"

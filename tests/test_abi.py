@@ -16,11 +16,12 @@ from pyradmc_b200 import _lib
 from tests.conftest import ROOT, cuda_available
 
 HEADER = ROOT / "include" / "pyradmc_b200.h"
+DENOISE_HEADER = ROOT / "include" / "pyradmc_b200_denoise.h"
 
 
 def declared_symbols() -> set[str]:
-    text = HEADER.read_text()
-    return set(re.findall(r"\b(pmc_[a-z_]+)\s*\(", text)) - {"pmc_progress_fn"}
+    text = HEADER.read_text() + DENOISE_HEADER.read_text()
+    return set(re.findall(r"\b(pm[cd]_[a-z0-9_]+)\s*\(", text)) - {"pmc_progress_fn"}
 
 
 def test_library_exports_every_declared_symbol():
@@ -32,8 +33,9 @@ def test_library_exports_every_declared_symbol():
     assert declared <= set(_lib.SIGNATURES), "ctypes signatures missing for some symbols"
     out = subprocess.run(["nm", "-D", "--defined-only", str(_lib.library_path())],
                          capture_output=True, text=True, check=True).stdout
-    exported = set(re.findall(r"\bT (pmc_\w+)", out))
+    exported = set(re.findall(r"\bT (pm[cd]_\w+)", out))
     assert declared <= exported
+    assert any(name.startswith("pmd_") for name in declared)
 
 
 def test_abi_version():

@@ -1,0 +1,92 @@
+"""The denoiser's host side without a GPU: parameter layout, the oracle's
+weight-layout conversions (pinned against a direct loop over the taps), argument
+checks of the C-ABI that return before any launch, and the no-CPU-fallback rule."""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+import torch
+
+from oracle.unet import OracleUNet, conv3d_reference, conv_weight, weight_to_flat
+from pyradmc_b200 import _lib
+from pyradmc_b200.denoiser import (IN_CHANNELS, LEVELS, forward_flops_per_voxel, init_parameters,
+                                   kpad_for, layout)
+from tests.conftest import cuda_available
+
+
+def test_layout_is_aligned_and_padded():
+    layers, head_w, head_b, n = layout()
+    assert [l.cout for l in layers] == [16, 16, 32, 32, 64, 64, 128, 128, 64, 64, 32, 32, 16, 16]
+    assert layers[0].cin == IN_CHANNELS and layers[8].cin == LEVELS[3] + LEVELS[2]
+    ends = 0
+    for l in layers:
+        assert l.kpad % 64 == 0 and l.kpad >= 27 * l.cin and l.kpad - 27 * l.cin < 64
+        assert l.w_off % 64 == 0 and l.b_off % 64 == 0 and l.w_off >= ends
+        ends = l.b_off + l.cout
+    assert head_w % 64 == 0 and head_b > head_w and n > head_b
+    p = init_parameters(0)
+    assert p.shape == (n,) and p.dtype == np.float32
+    for l in layers:
+        w = p[l.w_off:l.w_off + l.cout * l.kpad].reshape(l.cout, l.kpad)
+        assert (w[:, 27 * l.cin:] == 0).all() and w[:, :27 * l.cin].std() > 0
+    assert (p[head_w:head_b + 1] == 0).all()
+    assert kpad_for(8) == 256 and kpad_for(128) == 3456 and kpad_for(48) == 1344
+    # 2*27*(8*16 + 16*16 + 48*16 + 16*16) at full resolution plus the coarser levels
+    assert 130_000 < forward_flops_per_voxel() < 140_000
+
+
+def test_oracle_convolution_follows_the_tap_order_of_the_kernels():
+    rng = np.random.default_rng(1)
+    n, d, h, w, cin, cout = 1, 3, 4, 5, 8, 2
+    kpad = kpad_for(cin)
+    x = rng.normal(size=(n, d, h, w, cin)).astype(np.float32)
+    wt = np.zeros((cout, kpad), dtype=np.float32)
+    wt[:, :27 * cin] = rng.normal(size=(cout, 27 * cin))
+    ref = np.zeros((n, d, h, w, cout))
+    for z in range(d):
+        for y in range(h):
+            for xx in range(w):
+                for tap in range(27):
+                    zz, yy, x3 = z + tap // 9 - 1, y + (tap // 3) % 3 - 1, xx + tap % 3 - 1
+                    if 0 <= zz < d and 0 <= yy < h and 0 <= x3 < w:
+                        ref[0, z, y, xx] += wt[:, tap * cin:(tap + 1) * cin] @ x[0, zz, yy, x3]
+    got = conv3d_reference(x, wt, None, cin, cout, kpad, relu=False)
+    np.testing.assert_allclose(got, ref, rtol=1e-5, atol=1e-5)
+
+
+def test_weight_conversions_round_trip():
+    layers, *_ = layout()
+    p = init_parameters(2)
+    for l in layers[:3]:
+        w = conv_weight(p, l)
+        assert tuple(w.shape) == (l.cout, l.cin, 3, 3, 3)
+        np.testing.assert_array_equal(weight_to_flat(w, l), p[l.w_off:l.w_off + l.cout * l.kpad])
+
+
+def test_oracle_network_with_a_zero_head_is_the_identity():
+    rng = np.random.default_rng(0)
+    dose = torch.from_numpy(rng.random((1, 8, 8, 8)).astype(np.float32))
+    rho = torch.ones_like(dose)
+    out = OracleUNet(init_parameters(0)).forward(dose, rho)
+    assert torch.equal(out, dose)
+
+
+def test_abi_rejects_unsupported_shapes_before_launching():
+    lib = _lib.load()
+    assert lib.pmd_conv3d(None, None, None, None, 1, 8, 8, 8, 8, 24, 256, 1, None) == -1  # cout
+    assert lib.pmd_conv3d(None, None, None, None, 1, 8, 8, 8, 12, 16, 384, 1, None) == -1  # cin
+    assert lib.pmd_conv3d(None, None, None, None, 1, 8, 8, 8, 8, 16, 200, 1, None) == -1  # kpad
+    assert lib.pmd_conv3d_wgrad(None, None, None, None, 1, 8, 8, 8, 8, 8, 256, None) == -1
+    assert lib.pmd_head_grad(None, None, None, None, None, None, 10, 65, None) == -1
+    assert lib.pmd_csc_to_dense(None, None, None, 70000, 1, None, None, None) == -1
+    assert lib.pmd_avgpool(None, None, 1, 3, 4, 4, 8, None) == -1
+    assert lib.pmd_adam(None, None, None, None, None, 10, 1e-3, 0.9, 0.999, 1e-8, 0, None) == -1
+
+
+@pytest.mark.skipif(cuda_available(), reason="checks the no-device behaviour")
+def test_network_refuses_to_run_without_a_cuda_device():
+    from pyradmc_b200.denoiser import UNet3D
+
+    with pytest.raises(RuntimeError, match="CUDA device only"):
+        UNet3D("cuda:0")

@@ -1,0 +1,233 @@
+"""The denoiser's kernels against the float32 CPU oracle (torch conv3d + autograd).
+
+Every convolution entry point (forward, data gradient through the flipped
+weights, weight gradient), the pooling and joining kernels with their
+gradients, and the whole U-Net's parameter gradient are compared with the
+oracle on the same bf16-rounded operands.  Tolerances: the kernels accumulate
+in fp32 like the oracle, so what separates them is the bf16 rounding of a
+kernel's OUTPUT (relative 2^-8) and of intermediate activations in the full
+network; the fp32 weight gradient differs only in summation order.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from oracle.unet import OracleUNet, bf16, conv3d_reference
+from pyradmc_b200 import _lib
+from pyradmc_b200.denoiser import LEVELS, UNet3D, init_parameters, kpad_for, layout
+
+pytestmark = pytest.mark.gpu
+
+BF16_REL = 2.0 ** -8
+
+
+def _dev(a, dtype):
+    import torch
+
+    return torch.from_numpy(np.ascontiguousarray(a)).to("cuda:0").to(dtype)
+
+
+def _weights(rng, cin, cout):
+    kpad = kpad_for(cin)
+    w = np.zeros((cout, kpad), dtype=np.float32)
+    w[:, :27 * cin] = bf16(rng.normal(0, np.sqrt(2.0 / (27 * cin)), (cout, 27 * cin)))
+    return w, kpad
+
+
+CONV_SHAPES = [
+    # (n, d, h, w, cin, cout): ragged voxel counts, non-cubic grids, every cout tile
+    (1, 8, 8, 8, 8, 16),
+    (2, 6, 5, 7, 16, 8),
+    (1, 4, 8, 6, 48, 16),
+    (1, 8, 8, 8, 96, 32),
+    (2, 4, 4, 4, 192, 64),
+    (1, 4, 6, 4, 64, 48),
+    (1, 4, 4, 4, 128, 96),
+    (1, 2, 4, 4, 64, 128),
+    (1, 2, 2, 4, 128, 192),
+]
+
+
+@pytest.mark.parametrize("shape", CONV_SHAPES)
+def test_conv3d_forward_matches_oracle(gpu, shape):
+    import torch
+
+    n, d, h, w, cin, cout = shape
+    rng = np.random.default_rng(sum(shape) * 31 + cin)
+    x = bf16(rng.normal(size=(n, d, h, w, cin)))
+    wt, kpad = _weights(rng, cin, cout)
+    bias = rng.normal(size=cout).astype(np.float32)
+    lib = _lib.load()
+    dx, dw, db = _dev(x, torch.bfloat16), _dev(wt, torch.bfloat16), _dev(bias, torch.float32)
+    for relu in (0, 1):
+        y = torch.full((n, d, h, w, cout), float("nan"), dtype=torch.bfloat16, device=gpu)
+        assert lib.pmd_conv3d(dx.data_ptr(), dw.data_ptr(), db.data_ptr(), y.data_ptr(), n, d, h, w,
+                              cin, cout, kpad, relu, None) == 0
+        got = y.float().cpu().numpy()
+        ref = conv3d_reference(x, wt, bias, cin, cout, kpad, bool(relu))
+        assert np.isfinite(got).all()
+        np.testing.assert_allclose(got, ref, rtol=BF16_REL, atol=1e-5 * np.abs(ref).max())
+
+
+@pytest.mark.parametrize("shape", [(1, 8, 8, 8, 8, 16), (2, 6, 5, 7, 16, 32), (1, 4, 6, 4, 64, 64),
+                                   (1, 4, 4, 4, 192, 64), (1, 4, 4, 8, 48, 16),
+                                   (1, 2, 4, 4, 128, 128)])
+def test_conv3d_weight_gradient_matches_oracle(gpu, shape):
+    import torch
+    from torch.nn.grad import conv3d_weight
+
+    n, d, h, w, cin, cout = shape
+    rng = np.random.default_rng(7 + cin + cout)
+    x = bf16(rng.normal(size=(n, d, h, w, cin)))
+    g = bf16(rng.normal(size=(n, d, h, w, cout)))
+    kpad = kpad_for(cin)
+    dw = torch.zeros((cout, kpad), dtype=torch.float32, device=gpu)
+    db = torch.zeros(cout, dtype=torch.float32, device=gpu)
+    dx, dg = _dev(x, torch.bfloat16), _dev(g, torch.bfloat16)
+    assert _lib.load().pmd_conv3d_wgrad(dx.data_ptr(), dg.data_ptr(), dw.data_ptr(), db.data_ptr(),
+                                        n, d, h, w, cin, cout, kpad, None) == 0
+    xt = torch.from_numpy(x.transpose(0, 4, 1, 2, 3).copy())
+    gt = torch.from_numpy(g.transpose(0, 4, 1, 2, 3).copy())
+    ref = conv3d_weight(xt, (cout, cin, 3, 3, 3), gt, padding=1)
+    ref_flat = np.zeros((cout, kpad), dtype=np.float32)
+    ref_flat[:, :27 * cin] = ref.numpy().transpose(0, 2, 3, 4, 1).reshape(cout, -1)
+    got = dw.cpu().numpy()
+    scale = np.abs(ref_flat).max()
+    np.testing.assert_allclose(got, ref_flat, rtol=1e-4, atol=1e-5 * scale)
+    np.testing.assert_allclose(db.cpu().numpy(), g.reshape(-1, cout).sum(0), rtol=1e-4,
+                               atol=1e-4 * np.abs(g).sum(0).max())
+    assert (got[:, 27 * cin:] == 0).all()
+
+
+@pytest.mark.parametrize("shape", [(1, 8, 8, 8, 16, 16), (2, 6, 5, 7, 48, 16), (1, 4, 6, 4, 96, 32),
+                                   (1, 4, 4, 4, 192, 64), (1, 2, 4, 4, 64, 128),
+                                   (1, 4, 4, 4, 128, 64), (1, 4, 4, 4, 32, 16)])
+def test_conv3d_data_gradient_matches_oracle(gpu, shape):
+    import torch
+    from torch.nn.grad import conv3d_input
+
+    n, d, h, w, cin, cout = shape
+    rng = np.random.default_rng(11 + cin + cout)
+    wt, kpad = _weights(rng, cin, cout)
+    g = bf16(rng.normal(size=(n, d, h, w, cout)))
+    kpad_d = kpad_for(cout)
+    lib = _lib.load()
+    dwt = _dev(wt, torch.bfloat16)
+    wd = torch.zeros((cin, kpad_d), dtype=torch.bfloat16, device=gpu)
+    assert lib.pmd_flip_weights(dwt.data_ptr(), wd.data_ptr(), cin, cout, kpad, kpad_d, None) == 0
+    gx = torch.empty((n, d, h, w, cin), dtype=torch.bfloat16, device=gpu)
+    dg = _dev(g, torch.bfloat16)
+    assert lib.pmd_conv3d(dg.data_ptr(), wd.data_ptr(), None, gx.data_ptr(), n, d, h, w, cout, cin,
+                          kpad_d, 0, None) == 0
+    w5 = wt[:, :27 * cin].reshape(cout, 3, 3, 3, cin).transpose(0, 4, 1, 2, 3).copy()
+    ref = conv3d_input((n, cin, d, h, w), torch.from_numpy(w5),
+                       torch.from_numpy(g.transpose(0, 4, 1, 2, 3).copy()), padding=1)
+    ref = ref.numpy().transpose(0, 2, 3, 4, 1)
+    got = gx.float().cpu().numpy()
+    np.testing.assert_allclose(got, ref, rtol=BF16_REL, atol=1e-5 * np.abs(ref).max())
+
+
+def test_pool_upcat_and_their_gradients(gpu):
+    import torch
+    import torch.nn.functional as F
+
+    rng = np.random.default_rng(3)
+    n, d, h, w, c_up, c_skip = 2, 8, 4, 6, 16, 8
+    lib = _lib.load()
+    x = bf16(rng.normal(size=(n, d, h, w, c_skip)))
+    dx = _dev(x, torch.bfloat16)
+    y = torch.empty((n, d // 2, h // 2, w // 2, c_skip), dtype=torch.bfloat16, device=gpu)
+    assert lib.pmd_avgpool(dx.data_ptr(), y.data_ptr(), n, d, h, w, c_skip, None) == 0
+    ref = F.avg_pool3d(torch.from_numpy(x.transpose(0, 4, 1, 2, 3).copy()), 2).numpy().transpose(0, 2, 3, 4, 1)
+    np.testing.assert_allclose(y.float().cpu().numpy(), ref, rtol=BF16_REL, atol=1e-6)
+
+    gy = bf16(rng.normal(size=tuple(y.shape)))
+    prior = bf16(rng.normal(size=x.shape))
+    gx = _dev(prior, torch.bfloat16)
+    assert lib.pmd_avgpool_grad(_dev(gy, torch.bfloat16).data_ptr(), gx.data_ptr(), n, d, h, w,
+                                c_skip, 1, None) == 0
+    up = np.repeat(np.repeat(np.repeat(gy, 2, 1), 2, 2), 2, 3) / 8.0
+    np.testing.assert_allclose(gx.float().cpu().numpy(), prior + up, rtol=BF16_REL, atol=1e-6)
+
+    upin = bf16(rng.normal(size=(n, d // 2, h // 2, w // 2, c_up)))
+    dup = _dev(upin, torch.bfloat16)
+    out = torch.empty((n, d, h, w, c_up + c_skip), dtype=torch.bfloat16, device=gpu)
+    assert lib.pmd_upcat(dup.data_ptr(), dx.data_ptr(), out.data_ptr(), n, d, h, w, c_up, c_skip,
+                         None) == 0
+    ref = np.concatenate([np.repeat(np.repeat(np.repeat(upin, 2, 1), 2, 2), 2, 3), x], axis=-1)
+    np.testing.assert_array_equal(out.float().cpu().numpy(), ref)
+
+    gout = bf16(rng.normal(size=ref.shape))
+    dgout = _dev(gout, torch.bfloat16)
+    gup = torch.empty_like(dup)
+    gskip = torch.empty_like(dx)
+    assert lib.pmd_upcat_grad(dgout.data_ptr(), gup.data_ptr(), gskip.data_ptr(), n, d, h, w, c_up,
+                              c_skip, 0, None) == 0
+    ref_up = gout[..., :c_up].reshape(n, d // 2, 2, h // 2, 2, w // 2, 2, c_up).sum((2, 4, 6))
+    np.testing.assert_allclose(gup.float().cpu().numpy(), ref_up, rtol=BF16_REL, atol=1e-5)
+    np.testing.assert_array_equal(gskip.float().cpu().numpy(), gout[..., c_up:])
+
+
+def _batch(rng, b, s):
+    """A smooth positive dose-like field with noise, its clean version, a
+    density and a loss weight; noisy and density are exact in bf16 (the
+    kernels' input rounding)."""
+    z, y, x = np.meshgrid(*(np.arange(s),) * 3, indexing="ij")
+    clean = np.exp(-((x - s / 2) ** 2 + (y - s / 2) ** 2) / (0.1 * s * s)) * np.exp(-z / (2.0 * s))
+    clean = np.ascontiguousarray(np.broadcast_to(clean, (b, s, s, s)), dtype=np.float32)
+    noisy = bf16(clean * (1 + 0.3 * rng.normal(size=clean.shape)))
+    density = bf16(1.0 + 0.2 * rng.random((b, s, s, s)))
+    weight = rng.random((b, s, s, s)).astype(np.float32)
+    return noisy, density, clean, weight
+
+
+def test_unet_gradients_match_oracle(gpu):
+    import torch
+
+    rng = np.random.default_rng(5)
+    params = init_parameters(seed=3)
+    layers, head_w, head_b, _ = layout()
+    params[head_w:head_w + LEVELS[0]] = rng.normal(0, 0.5, LEVELS[0])  # non-zero head: gradients flow
+    params[head_b] = 0.01
+    for l in layers:  # the kernels read bf16 convolution weights: give the oracle the same
+        sl = slice(l.w_off, l.w_off + l.cout * l.kpad)
+        params[sl] = bf16(params[sl])
+    noisy, density, clean, weight = _batch(rng, 2, 16)
+    net = UNet3D(gpu, params=params, loss_lambda=0.5)
+    loss, grad = net.gradients(_dev(noisy, torch.float32), _dev(density, torch.float32),
+                               _dev(clean, torch.float32), _dev(weight, torch.float32))
+    torch.cuda.synchronize()
+    got = grad.cpu().numpy()
+    ref_loss, ref = OracleUNet(params).gradients(torch.from_numpy(noisy), torch.from_numpy(density),
+                                                 torch.from_numpy(clean), torch.from_numpy(weight),
+                                                 0.5)
+    assert abs(float(loss.item()) - ref_loss) <= 0.02 * ref_loss
+    for l in layers:
+        for off, size in ((l.w_off, l.cout * l.kpad), (l.b_off, l.cout)):
+            a, b = got[off:off + size], ref[off:off + size]
+            cos = float(a @ b / (np.linalg.norm(a) * np.linalg.norm(b) + 1e-30))
+            rel = float(np.linalg.norm(a - b) / (np.linalg.norm(b) + 1e-30))
+            assert cos > 0.99 and rel < 0.15, (l.name, off == l.b_off, cos, rel)
+    hw = slice(head_w, head_w + LEVELS[0])
+    np.testing.assert_allclose(got[hw], ref[hw], rtol=0.05, atol=0.02 * np.abs(ref[hw]).max())
+
+
+def test_zero_head_network_is_the_identity_and_training_reduces_the_loss(gpu):
+    import torch
+
+    rng = np.random.default_rng(9)
+    noisy, density, clean, weight = _batch(rng, 2, 16)
+    net = UNet3D(gpu, seed=1, lr=2e-3)
+    args = [_dev(a, torch.float32) for a in (noisy, density, clean, weight)]
+    out = net.predict(args[0], args[1]).cpu().numpy()
+    np.testing.assert_array_equal(out, noisy)  # zero head: prediction = input dose
+    losses = [float(net.train_step(*args).item()) for _ in range(100)]
+    assert np.isfinite(losses).all()
+    assert np.mean(losses[-5:]) < 0.85 * losses[0], losses[::10]
+    p = net.parameters()
+    assert np.isfinite(p).all()
+    for l in layout()[0]:
+        pad = p[l.w_off:l.w_off + l.cout * l.kpad].reshape(l.cout, l.kpad)[:, 27 * l.cin:]
+        assert (pad == 0).all(), l.name  # K padding stays zero through Adam
