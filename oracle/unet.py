@@ -90,7 +90,7 @@ class OracleUNet:
         c0 = LEVELS[0]
         g[self.head_w:self.head_w + c0] = self.hw.grad.numpy()
         g[self.head_b] = self.hb.grad.numpy()[0]
-        return float(loss), g
+        return float(loss.detach()), g
 
 
 def conv3d_reference(x_ndhwc: np.ndarray, w_flat: np.ndarray, bias, cin: int, cout: int,

@@ -219,15 +219,18 @@ def test_zero_head_network_is_the_identity_and_training_reduces_the_loss(gpu):
 
     rng = np.random.default_rng(9)
     noisy, density, clean, weight = _batch(rng, 2, 16)
+    target = clean + 0.2  # an offset the network must learn on top of the denoising
     net = UNet3D(gpu, seed=1, lr=2e-3)
-    args = [_dev(a, torch.float32) for a in (noisy, density, clean, weight)]
+    p0 = net.parameters()
+    args = [_dev(a, torch.float32) for a in (noisy, density, target, weight)]
     out = net.predict(args[0], args[1]).cpu().numpy()
     np.testing.assert_array_equal(out, noisy)  # zero head: prediction = input dose
-    losses = [float(net.train_step(*args).item()) for _ in range(100)]
+    losses = [float(net.train_step(*args).item()) for _ in range(150)]
     assert np.isfinite(losses).all()
-    assert np.mean(losses[-5:]) < 0.85 * losses[0], losses[::10]
+    assert np.mean(losses[-5:]) < 0.6 * losses[0], losses[::10]
     p = net.parameters()
     assert np.isfinite(p).all()
     for l in layout()[0]:
-        pad = p[l.w_off:l.w_off + l.cout * l.kpad].reshape(l.cout, l.kpad)[:, 27 * l.cin:]
-        assert (pad == 0).all(), l.name  # K padding stays zero through Adam
+        w, w0 = (q[l.w_off:l.w_off + l.cout * l.kpad].reshape(l.cout, l.kpad) for q in (p, p0))
+        assert (w[:, 27 * l.cin:] == 0).all(), l.name  # K padding stays zero through Adam
+        assert np.abs(w - w0).max() > 1e-3, l.name     # every layer received gradients
