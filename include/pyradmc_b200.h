@@ -244,6 +244,15 @@ int pmc_run_dij(pmc_engine* engine, const pmc_beamlet_desc* source, const int64_
 int pmc_dij_fetch(pmc_engine* engine, int64_t* indptr, int64_t* indices, double* dose,
                   double* sigma);
 
+/* The CSC of the last pmc_run_dij left on the device (no counterpart in the
+ * reference, whose Dij is always assembled on the host): indptr[n_beamlets+1]
+ * is copied into the caller's host buffer, and *indices, *dose, *sigma receive
+ * DEVICE pointers to the nnz entries, owned by the engine and valid until its
+ * next run or pmc_destroy.  For device-side consumers of the Dij (the
+ * denoiser) that would otherwise copy it to the host and back. */
+int pmc_dij_device_view(pmc_engine* engine, int64_t* indptr, const int64_t** indices,
+                        const double** dose, const double** sigma);
+
 int pmc_get_counters(const pmc_engine* engine, pmc_counters* counters);
 
 /* Run the engine's work on the caller's CUDA stream (a cudaStream_t passed as

@@ -97,6 +97,26 @@ int pmd_pack_input(const float* dose, const float* density, const float* colmax,
 int pmd_csc_to_dense(const int64_t* indptr, const int64_t* indices, const double* values,
                      int n_cols, int64_t vox, float* dense, float* colmax, void* stream);
 
+/* The same into float64 (no maximum): for the dense mean and sigma that the
+ * truncation + CSC compaction (pmc_dij_compact_static) consumes. */
+int pmd_csc_to_dense_f64(const int64_t* indptr, const int64_t* indices, const double* values,
+                         int n_cols, int64_t vox, double* dense, void* stream);
+
+/* Windows of a stack of nx*ny*nz volumes (x-major, z fastest): out[c] is the
+ * wx*wy*wz window of volume c (src + c * src_stride; src_stride 0 reads one
+ * shared volume) whose first voxel is (ox, oy, oz) = origins[3c .. 3c+2]
+ * (int32, may lie partly outside; outside reads as zero). */
+int pmd_gather_windows(const float* src, int64_t src_stride, int nx, int ny, int nz,
+                       const int32_t* origins, int n_windows, int wx, int wy, int wz, float* out,
+                       void* stream);
+
+/* The reverse, in dose units: dst[c * dst_stride + voxel] = max(win, 0) *
+ * scale[c] (float64; scale NULL or zero: 1) for every window voxel inside the
+ * volume; voxels outside every window keep their value. */
+int pmd_scatter_windows(const float* win, const float* scale, int nx, int ny, int nz,
+                        const int32_t* origins, int n_windows, int wx, int wy, int wz, double* dst,
+                        int64_t dst_stride, void* stream);
+
 /* Back to dose units: mean[m] = max(out[m], 0) * colmax[m / vox] (float64). */
 int pmd_unscale(const float* out, const float* colmax, int64_t vox, double* mean, int64_t m,
                 void* stream);

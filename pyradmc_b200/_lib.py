@@ -209,6 +209,10 @@ SIGNATURES: dict[str, tuple[object, list]] = {
         [C.c_void_p, C.POINTER(BeamletDesc), _lp, C.POINTER(RunParams), _lp, C.POINTER(Books)],
     ),
     "pmc_dij_fetch": (C.c_int, [C.c_void_p, _lp, _lp, _dp, _dp]),
+    "pmc_dij_device_view": (
+        C.c_int,
+        [C.c_void_p, _lp, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.POINTER(C.c_void_p)],
+    ),
     "pmc_get_counters": (C.c_int, [C.c_void_p, C.POINTER(Counters)]),
     "pmc_set_progress": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     "pmc_set_stream": (C.c_int, [C.c_void_p, C.c_void_p]),
@@ -249,6 +253,9 @@ SIGNATURES.update({
     "pmd_pack_input": (_i, [_v, _v, _v, _l, _i, _v, _v, _l, _v]),
     "pmd_csc_to_dense": (_i, [_v, _v, _v, _i, _l, _v, _v, _v]),
     "pmd_unscale": (_i, [_v, _v, _l, _v, _l, _v]),
+    "pmd_csc_to_dense_f64": (_i, [_v, _v, _v, _i, _l, _v, _v]),
+    "pmd_gather_windows": (_i, [_v, _l, _i, _i, _i, _v, _i, _i, _i, _i, _v, _v]),
+    "pmd_scatter_windows": (_i, [_v, _v, _i, _i, _i, _v, _i, _i, _i, _i, _v, _l, _v]),
 })
 
 PROGRESS_FN = C.CFUNCTYPE(None, C.c_void_p, C.c_int64)

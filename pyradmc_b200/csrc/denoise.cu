@@ -559,6 +559,57 @@ __global__ void unscale_kernel(const float* out, const float* colmax, long long 
     }
 }
 
+// Windows of a stack of volumes (x-major, z fastest): window c of size
+// wx*wy*wz at origin (ox, oy, oz)[c]; voxels outside the volume read as zero.
+__global__ void gather_windows_kernel(const float* src, long long src_stride, int nx, int ny,
+                                      int nz, const int* origins, int wx, int wy, int wz,
+                                      float* out, long long total) {
+    const long long per = (long long)wx * wy * wz;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += stride) {
+        const int c = (int)(i / per);
+        long long r = i - (long long)c * per;
+        const int k = (int)(r % wz); r /= wz;
+        const int j = (int)(r % wy);
+        const int ii = (int)(r / wy);
+        const int x = origins[3 * c] + ii, y = origins[3 * c + 1] + j, z = origins[3 * c + 2] + k;
+        float v = 0.0f;
+        if ((unsigned)x < (unsigned)nx && (unsigned)y < (unsigned)ny && (unsigned)z < (unsigned)nz)
+            v = src[(long long)c * src_stride + ((long long)x * ny + y) * nz + z];
+        out[i] = v;
+    }
+}
+
+__global__ void scatter_windows_kernel(const float* win, const float* scale, int nx, int ny, int nz,
+                                       const int* origins, int wx, int wy, int wz, double* dst,
+                                       long long dst_stride, long long total) {
+    const long long per = (long long)wx * wy * wz;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += stride) {
+        const int c = (int)(i / per);
+        long long r = i - (long long)c * per;
+        const int k = (int)(r % wz); r /= wz;
+        const int j = (int)(r % wy);
+        const int ii = (int)(r / wy);
+        const int x = origins[3 * c] + ii, y = origins[3 * c + 1] + j, z = origins[3 * c + 2] + k;
+        if ((unsigned)x < (unsigned)nx && (unsigned)y < (unsigned)ny && (unsigned)z < (unsigned)nz) {
+            const float sc = scale ? scale[c] : 1.0f;
+            dst[(long long)c * dst_stride + ((long long)x * ny + y) * nz + z] =
+                (double)fmaxf(win[i], 0.0f) * (double)(sc > 0.0f ? sc : 1.0f);
+        }
+    }
+}
+
+// CSC -> dense float64 columns (the caller zeroes dense).
+__global__ void csc_to_dense_f64_kernel(const int64_t* indptr, const int64_t* indices,
+                                        const double* values, long long vox, double* dense) {
+    const int col = blockIdx.y;
+    const long long begin = indptr[col], end = indptr[col + 1];
+    for (long long j = begin + (long long)blockIdx.x * blockDim.x + threadIdx.x; j < end;
+         j += (long long)gridDim.x * blockDim.x)
+        dense[(long long)col * vox + indices[j]] = values[j];
+}
+
 }  // namespace pmd
 
 using namespace pmd;
@@ -738,6 +789,39 @@ int pmd_unscale(const float* out, const float* colmax, int64_t vox, double* mean
                 void* stream) {
     if (vox < 1) return -1;
     unscale_kernel<<<grid_for(m), 256, 0, (cudaStream_t)stream>>>(out, colmax, vox, mean, m);
+    return launched();
+}
+
+int pmd_csc_to_dense_f64(const int64_t* indptr, const int64_t* indices, const double* values,
+                         int n_cols, int64_t vox, double* dense, void* stream) {
+    if (n_cols < 0 || n_cols > 65535 || vox < 1) return -1;
+    if (n_cols == 0) return 0;
+    csc_to_dense_f64_kernel<<<dim3(64, n_cols), 256, 0, (cudaStream_t)stream>>>(indptr, indices,
+                                                                                values, vox, dense);
+    return launched();
+}
+
+int pmd_gather_windows(const float* src, int64_t src_stride, int nx, int ny, int nz,
+                       const int32_t* origins, int n_windows, int wx, int wy, int wz, float* out,
+                       void* stream) {
+    if (nx < 1 || ny < 1 || nz < 1 || wx < 1 || wy < 1 || wz < 1 || n_windows < 0 || src_stride < 0)
+        return -1;
+    const long long total = (long long)n_windows * wx * wy * wz;
+    if (total == 0) return 0;
+    gather_windows_kernel<<<grid_for(total), 256, 0, (cudaStream_t)stream>>>(
+        src, src_stride, nx, ny, nz, origins, wx, wy, wz, out, total);
+    return launched();
+}
+
+int pmd_scatter_windows(const float* win, const float* scale, int nx, int ny, int nz,
+                        const int32_t* origins, int n_windows, int wx, int wy, int wz, double* dst,
+                        int64_t dst_stride, void* stream) {
+    if (nx < 1 || ny < 1 || nz < 1 || wx < 1 || wy < 1 || wz < 1 || n_windows < 0 || dst_stride < 0)
+        return -1;
+    const long long total = (long long)n_windows * wx * wy * wz;
+    if (total == 0) return 0;
+    scatter_windows_kernel<<<grid_for(total), 256, 0, (cudaStream_t)stream>>>(
+        win, scale, nx, ny, nz, origins, wx, wy, wz, dst, dst_stride, total);
     return launched();
 }
 

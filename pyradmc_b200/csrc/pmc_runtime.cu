@@ -1119,6 +1119,16 @@ int pmc_dij_fetch(pmc_engine* e, int64_t* indptr, int64_t* indices, double* dose
     return PMC_OK;
 }
 
+int pmc_dij_device_view(pmc_engine* e, int64_t* indptr, const int64_t** indices,
+                        const double** dose, const double** sigma) {
+    if (!e || !indptr || !indices || !dose || !sigma) return PMC_ERR_INVALID;
+    std::memcpy(indptr, e->dij_indptr.data(), sizeof(int64_t) * e->dij_indptr.size());
+    *indices = (const int64_t*)e->out_idx.p;
+    *dose = (const double*)e->out_dose.p;
+    *sigma = (const double*)e->out_sigma.p;
+    return PMC_OK;
+}
+
 int pmc_set_stream(pmc_engine* e, void* stream) {
     if (!e) return PMC_ERR_INVALID;
     PMC_CUDA(e, cudaStreamSynchronize(e->stream));

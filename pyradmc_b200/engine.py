@@ -23,7 +23,7 @@ import numpy as np
 
 from pyradmc_b200 import _lib, model
 
-__all__ = ["B200Engine", "DIJ_TRUNCATION_RELATIVE", "ECUT_MEV", "PCUT_MEV"]
+__all__ = ["B200Engine", "DIJ_TRUNCATION_RELATIVE", "DeviceDij", "ECUT_MEV", "PCUT_MEV"]
 
 ECUT_MEV = 0.200  # pyradmc/__init__.py:22
 PCUT_MEV = 0.050  # pyradmc/__init__.py:25
@@ -140,6 +140,38 @@ class _Native:
             except Exception:
                 pass
             self.handle = None
+
+
+@dataclass
+class DeviceDij:
+    """A Dij left on the device by :meth:`B200Engine.run_dij_device`.
+
+    ``indptr`` is host memory; ``indices`` (int64), ``dose`` and ``sigma``
+    (float64) are device addresses of ``nnz`` entries owned by the engine and
+    valid until its next run.
+    """
+
+    n_beamlets: int
+    nnz: int
+    indptr: np.ndarray
+    indices: int
+    dose: int
+    sigma: int
+    books: tuple
+    grid_shape: tuple = ()
+    counts: np.ndarray | None = None
+    n_batches: int = 0
+    device: str = "cuda:0"
+
+
+def _device_dij(native: "_Native", n_cols: int, nnz: int, books) -> DeviceDij:
+    indptr = np.zeros(n_cols + 1, dtype=np.int64)
+    ptrs = [C.c_void_p() for _ in range(3)]
+    native.check(native.lib.pmc_dij_device_view(native.handle, _lib.ptr(indptr, C.c_int64),
+                                                *(C.byref(p) for p in ptrs)))
+    return DeviceDij(n_beamlets=n_cols, nnz=nnz, indptr=indptr,
+                     indices=ptrs[0].value or 0, dose=ptrs[1].value or 0, sigma=ptrs[2].value or 0,
+                     books=(books.deposited, books.escaped, books.unscored, books.emitted))
 
 
 @dataclass(frozen=True)
@@ -537,6 +569,52 @@ class B200Engine:
         ``h = j * n_per + r`` exactly.  ``DijResult.n_histories_per_beamlet``
         carries the integer when the counts are equal and the maximum otherwise.
         """
+        return self._run_dij(
+            source, n_histories_per_beamlet, n_batches, seed, pcut=pcut, ecut=ecut,
+            transport_electrons=transport_electrons, truncation=truncation, correlated=correlated,
+            beamlet_group_size=beamlet_group_size, scoring_grid=scoring_grid,
+            scoring_mode=scoring_mode, step_energy_fraction=step_energy_fraction,
+            deposit_resolution_cm=deposit_resolution_cm, msc_model=msc_model, devices=devices,
+            concurrent_batches=concurrent_batches, progress=progress, device_view=False)
+
+    def run_dij_device(self, source, n_histories_per_beamlet, n_batches: int, seed: int,
+                       **kwargs) -> "DeviceDij":
+        """``run_dij`` on this engine's device, leaving the CSC there.
+
+        Same arguments as :meth:`run_dij` (one device, one beamlet group).  The
+        result's device arrays belong to the engine and stay valid until its
+        next run; the denoiser reads them without a host round trip.
+        """
+        if kwargs.get("devices") not in (None, [self.device], (self.device,)):
+            raise ValueError("run_dij_device runs on the engine's own device only")
+        if kwargs.get("beamlet_group_size") not in (None, int(source.n_beamlets)):
+            raise ValueError("run_dij_device runs the beamlets as one group")
+        kwargs.pop("devices", None)
+        return self._run_dij(source, n_histories_per_beamlet, n_batches, seed, device_view=True,
+                             **kwargs)
+
+    def _run_dij(
+        self,
+        source,
+        n_histories_per_beamlet,
+        n_batches: int,
+        seed: int,
+        pcut: float = PCUT_MEV,
+        ecut: float = ECUT_MEV,
+        transport_electrons: bool = True,
+        truncation: float = DIJ_TRUNCATION_RELATIVE,
+        correlated: bool = True,
+        beamlet_group_size: int | None = None,
+        scoring_grid=None,
+        scoring_mode: str = "dose_to_medium",
+        step_energy_fraction: float | None = None,
+        deposit_resolution_cm: float | None = None,
+        msc_model: str = "gs",
+        devices=None,
+        concurrent_batches: int = 1,
+        progress=None,
+        device_view: bool = False,
+    ):
         n_beamlets = int(source.n_beamlets)
         if np.ndim(n_histories_per_beamlet) == 0:
             counts = np.full(n_beamlets, int(n_histories_per_beamlet), dtype=np.int64)
@@ -652,6 +730,8 @@ class B200Engine:
                     finally:
                         lib.pmc_set_progress(native.handle, None, None)
                     native.check(code)
+                    if device_view:
+                        return _device_dij(native, g1 - g0, nnz.value, books), None
                     indptr = np.zeros(g1 - g0 + 1, dtype=np.int64)
                     indices = np.empty(nnz.value, dtype=np.int64)
                     dose = np.empty(nnz.value, dtype=np.float64)
@@ -664,6 +744,14 @@ class B200Engine:
                 totals += np.array([books.deposited, books.escaped, books.unscored, books.emitted])
             return blocks, totals
 
+        if device_view:
+            view, _ = shard(device_list[0])
+            view.grid_shape = (tuple(scoring_grid.shape) if scoring_grid is not None
+                               else tuple(self.grid.shape))
+            view.counts = counts
+            view.n_batches = n_batches
+            view.device = device_list[0]
+            return view
         if len(device_list) == 1:
             results = [shard(device_list[0])]
         else:
