@@ -38,6 +38,19 @@ extern "C" {
 int pmd_conv3d(const void* x, const void* w, const float* bias, void* y, int n, int d, int h,
                int w_, int cin, int cout, int kpad, int relu, void* stream);
 
+/* Selects the convolution kernels of pmd_conv3d: 0 (default) the tensor-memory
+ * kernel (tcgen05.mma, accumulators in TMEM; cout a multiple of 16 up to 192,
+ * cin 8 or a multiple of 16 up to 96) where it applies and the mma.sync
+ * kernel elsewhere; 1 the mma.sync kernel only; 2 the tensor-memory kernel
+ * only (other shapes return -1).  impl < 0 only queries.  Returns the
+ * previous setting.  Process-wide. */
+int pmd_conv3d_impl(int impl);
+
+/* Number of tensor-memory convolution launches whose wait on the tensor cores
+ * ran past its time limit since the last call (their outputs are not valid),
+ * and resets it; -2 when the device cannot be read.  Synchronizes the device. */
+int pmd_conv3d_failures(void);
+
 /* Weight gradient, ADDED into fp32 dw [cout][kpad] (and dbias [cout] when not
  * NULL): dw[co][k] += sum over voxels of g[v][co] * im2col(x)[v][k].
  * cout in {16, 32, 64, 128}.  The sum order is not fixed (fp32 atomics). */

@@ -240,6 +240,8 @@ _f = C.c_float
 SIGNATURES.update({
     "pmd_conv3d": (_i, [_v, _v, _v, _v, _i, _i, _i, _i, _i, _i, _i, _i, _v]),
     "pmd_conv3d_wgrad": (_i, [_v, _v, _v, _v, _i, _i, _i, _i, _i, _i, _i, _v]),
+    "pmd_conv3d_impl": (_i, [_i]),
+    "pmd_conv3d_failures": (_i, []),
     "pmd_flip_weights": (_i, [_v, _v, _i, _i, _i, _i, _v]),
     "pmd_relu_mask": (_i, [_v, _v, _l, _v]),
     "pmd_avgpool": (_i, [_v, _v, _i, _i, _i, _i, _i, _v]),

@@ -612,6 +612,8 @@ __global__ void csc_to_dense_f64_kernel(const int64_t* indptr, const int64_t* in
 
 }  // namespace pmd
 
+#include "denoise_umma.cuh"
+
 using namespace pmd;
 
 namespace {
@@ -644,6 +646,98 @@ void launch_wgrad(const __nv_bfloat16* x, const __nv_bfloat16* g, float* dw, flo
 
 int launched() { return cudaGetLastError() == cudaSuccess ? 0 : -2; }
 
+// Convolution path: 0 = tensor-memory UMMA kernel where it applies, else the
+// mma.sync kernel; 1 = mma.sync only; 2 = UMMA only.
+int g_conv_impl = 0;
+
+constexpr int kSmemPerSM = 233472;      // bytes of shared memory per SM
+constexpr int kSmemPerBlockMax = 232448;
+constexpr int kSmemReserved = 1024;     // per resident block
+
+// Tile plan of the UMMA kernel; false when the shape is outside it (cout a
+// multiple of 16 up to 192, cin 8 or a multiple of 16 up to 96).
+bool umma_plan(const ConvShape& s, UmmaConv& u, int& smem, int& ctas_per_sm) {
+    if (s.cout % 16 || s.cout < 16 || s.cout > 192) return false;
+    if (!(s.cin == 8 || (s.cin % 16 == 0 && s.cin <= 96))) return false;
+    const int cpt = s.cin / 8;
+    u.s = s;
+    u.tz = s.cin <= 48 ? 2 : 1;
+    const int npos = (u.tz + 2) * kUHY * kUHX;
+    u.plane_bytes = (unsigned)npos * 16;
+    u.halo_bytes = u.plane_bytes * cpt;
+    const int extra = 16;  // mbarrier + tensor-memory address
+    const int all_chunks = 27 * cpt + (s.cin == 8 ? 1 : 0);
+    const int base = (int)u.halo_bytes + kUSlack + extra;
+    const int per_tap = cpt * s.cout * 16;
+    if (base + all_chunks * s.cout * 16 <= kSmemPerSM / 2 - kSmemReserved ||
+        base + all_chunks * s.cout * 16 <= kSmemPerBlockMax) {
+        u.taps_per_pass = 27;
+        u.passes = 1;
+        u.w_chunks = (unsigned)all_chunks;
+    } else {
+        if (s.cin == 8) return false;
+        const int taps = (kSmemPerBlockMax - base) / per_tap;
+        if (taps < 1) return false;
+        u.taps_per_pass = taps;
+        u.passes = (27 + taps - 1) / taps;
+        u.w_chunks = (unsigned)(taps * cpt);
+    }
+    smem = base + (int)u.w_chunks * s.cout * 16;
+    unsigned cols = 32;
+    while (cols < (unsigned)(u.tz * s.cout)) cols <<= 1;
+    u.tmem_cols = cols;
+    u.tiles_d = (s.d + u.tz - 1) / u.tz;
+    u.tiles_h = (s.h + kUTY - 1) / kUTY;
+    u.tiles_w = (s.w + kUTX - 1) / kUTX;
+    const long long tiles = (long long)s.n * u.tiles_d * u.tiles_h * u.tiles_w;
+    if (tiles > (1LL << 30)) return false;
+    u.n_tiles = (int)tiles;
+    // resident blocks per SM: shared memory, and at most 512 tensor-memory
+    // columns in all (enforced through the shared-memory request, so that an
+    // allocation never waits on a block that holds its columns until it exits)
+    int by_smem = kSmemPerSM / (smem + kSmemReserved);
+    const int by_tmem = 512 / (int)cols;
+    if (by_smem > by_tmem) {
+        smem = kSmemPerSM / by_tmem - kSmemReserved;
+        if (smem > kSmemPerBlockMax) smem = kSmemPerBlockMax;
+        by_smem = kSmemPerSM / (smem + kSmemReserved);
+    }
+    ctas_per_sm = by_smem < 4 ? by_smem : 4;  // the kernel's launch bounds
+    return ctas_per_sm >= 1;
+}
+
+template <int N>
+int launch_umma(const __nv_bfloat16* x, const __nv_bfloat16* w, const float* bias, __nv_bfloat16* y,
+                ConvShape s, int relu, cudaStream_t st) {
+    UmmaConv u{};
+    int smem = 0, per_sm = 0;
+    if (!umma_plan(s, u, smem, per_sm)) return -1;
+    int dev = 0, sms = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+        return -2;
+    if (cudaFuncSetAttribute(conv3d_umma_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             smem) != cudaSuccess)
+        return -2;
+    const int grid = u.n_tiles < sms * per_sm ? u.n_tiles : sms * per_sm;
+    conv3d_umma_kernel<N><<<grid, 128, smem, st>>>(x, w, bias, y, u, relu);
+    return launched();
+}
+
+int dispatch_umma(const __nv_bfloat16* x, const __nv_bfloat16* w, const float* bias,
+                  __nv_bfloat16* y, ConvShape s, int relu, cudaStream_t st) {
+    switch (s.cout) {
+        case 16: return launch_umma<16>(x, w, bias, y, s, relu, st);
+        case 32: return launch_umma<32>(x, w, bias, y, s, relu, st);
+        case 48: return launch_umma<48>(x, w, bias, y, s, relu, st);
+        case 64: return launch_umma<64>(x, w, bias, y, s, relu, st);
+        case 96: return launch_umma<96>(x, w, bias, y, s, relu, st);
+        case 128: return launch_umma<128>(x, w, bias, y, s, relu, st);
+        case 192: return launch_umma<192>(x, w, bias, y, s, relu, st);
+        default: return -1;
+    }
+}
+
 }  // namespace
 
 extern "C" {
@@ -657,6 +751,12 @@ int pmd_conv3d(const void* x, const void* w, const float* bias, void* y, int n, 
     auto W = (const __nv_bfloat16*)w;
     auto Y = (__nv_bfloat16*)y;
     cudaStream_t st = (cudaStream_t)stream;
+    if (g_conv_impl != 1) {
+        UmmaConv u{};
+        int smem = 0, per_sm = 0;
+        if (umma_plan(s, u, smem, per_sm)) return dispatch_umma(X, W, bias, Y, s, relu, st);
+        if (g_conv_impl == 2) return -1;
+    }
     switch (cout) {
         case 8: launch_conv<8>(X, W, bias, Y, s, relu, st); break;
         case 16: launch_conv<16>(X, W, bias, Y, s, relu, st); break;
@@ -669,6 +769,20 @@ int pmd_conv3d(const void* x, const void* w, const float* bias, void* y, int n, 
         default: return -1;
     }
     return launched();
+}
+
+int pmd_conv3d_impl(int impl) {
+    const int previous = g_conv_impl;
+    if (impl >= 0 && impl <= 2) g_conv_impl = impl;
+    return previous;
+}
+
+int pmd_conv3d_failures(void) {
+    int n = 0;
+    if (cudaMemcpyFromSymbol(&n, g_umma_failures, sizeof(int)) != cudaSuccess) return -2;
+    const int zero = 0;
+    if (cudaMemcpyToSymbol(g_umma_failures, &zero, sizeof(int)) != cudaSuccess) return -2;
+    return n;
 }
 
 int pmd_conv3d_wgrad(const void* x, const void* g, float* dw, float* dbias, int n, int d, int h,

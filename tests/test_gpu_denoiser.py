@@ -234,3 +234,64 @@ def test_zero_head_network_is_the_identity_and_training_reduces_the_loss(gpu):
         w, w0 = (q[l.w_off:l.w_off + l.cout * l.kpad].reshape(l.cout, l.kpad) for q in (p, p0))
         assert (w[:, 27 * l.cin:] == 0).all(), l.name  # K padding stays zero through Adam
         assert np.abs(w - w0).max() > 1e-3, l.name     # every layer received gradients
+
+
+UMMA_SHAPES = [
+    # (n, d, h, w, cin, cout): partial tiles in every dimension, cin = 8 tap
+    # pairing, one- and multi-pass weights, every N the network uses
+    (1, 4, 16, 8, 8, 16),
+    (1, 3, 20, 12, 16, 16),
+    (2, 5, 17, 9, 48, 16),
+    (1, 4, 16, 16, 16, 48),
+    (1, 2, 18, 10, 32, 32),
+    (1, 3, 16, 8, 32, 96),
+    (1, 3, 18, 10, 96, 32),
+    (1, 2, 16, 16, 64, 64),
+    (1, 2, 8, 8, 64, 192),
+    (1, 2, 8, 8, 64, 128),
+]
+
+
+@pytest.mark.parametrize("shape", UMMA_SHAPES)
+def test_tensor_memory_convolution_matches_oracle(gpu, shape):
+    """The tcgen05/TMEM kernel (forced) against the oracle, and against the
+    mma.sync kernel on the same operands."""
+    import torch
+
+    n, d, h, w, cin, cout = shape
+    rng = np.random.default_rng(100 + sum(shape))
+    x = bf16(rng.normal(size=(n, d, h, w, cin)))
+    wt, kpad = _weights(rng, cin, cout)
+    bias = rng.normal(size=cout).astype(np.float32)
+    lib = _lib.load()
+    dx, dw, db = _dev(x, torch.bfloat16), _dev(wt, torch.bfloat16), _dev(bias, torch.float32)
+    ref = conv3d_reference(x, wt, bias, cin, cout, kpad, True)
+    outs = {}
+    previous = lib.pmd_conv3d_impl(-1)
+    try:
+        for impl in (2, 1):
+            lib.pmd_conv3d_impl(impl)
+            y = torch.full((n, d, h, w, cout), float("nan"), dtype=torch.bfloat16, device=gpu)
+            assert lib.pmd_conv3d(dx.data_ptr(), dw.data_ptr(), db.data_ptr(), y.data_ptr(), n, d, h,
+                                  w, cin, cout, kpad, 1, None) == 0
+            torch.cuda.synchronize()
+            outs[impl] = y.float().cpu().numpy()
+    finally:
+        lib.pmd_conv3d_impl(previous)
+    assert lib.pmd_conv3d_failures() == 0
+    for impl, got in outs.items():
+        assert np.isfinite(got).all(), impl
+        np.testing.assert_allclose(got, ref, rtol=BF16_REL, atol=1e-5 * np.abs(ref).max(),
+                                   err_msg=f"impl {impl}")
+    # both accumulate the same products in fp32: at most a bf16 rounding step apart
+    np.testing.assert_allclose(outs[2], outs[1], rtol=2 * BF16_REL, atol=1e-5 * np.abs(ref).max())
+
+
+def test_tensor_memory_path_rejects_what_it_does_not_cover(gpu):
+    lib = _lib.load()
+    previous = lib.pmd_conv3d_impl(2)
+    try:  # cin = 128 is outside the tensor-memory kernel: nothing launched
+        assert lib.pmd_conv3d(None, None, None, None, 1, 2, 2, 2, 128, 128, kpad_for(128), 1,
+                              None) == -1
+    finally:
+        lib.pmd_conv3d_impl(previous)
