@@ -668,9 +668,8 @@ bool umma_plan(const ConvShape& s, UmmaConv& u, int& smem, int& ctas_per_sm) {
     const int extra = 16;  // mbarrier + tensor-memory address
     const int all_chunks = 27 * cpt + (s.cin == 8 ? 1 : 0);
     const int base = (int)u.halo_bytes + kUSlack + extra;
-    const int per_tap = cpt * s.cout * 16;
-    if (base + all_chunks * s.cout * 16 <= kSmemPerSM / 2 - kSmemReserved ||
-        base + all_chunks * s.cout * 16 <= kSmemPerBlockMax) {
+    const int per_tap = cpt * s.cout * 16 + cpt * 8;  // weights + descriptor table entries
+    if (base + all_chunks * (s.cout * 16 + 8) <= kSmemPerBlockMax) {
         u.taps_per_pass = 27;
         u.passes = 1;
         u.w_chunks = (unsigned)all_chunks;
@@ -682,7 +681,8 @@ bool umma_plan(const ConvShape& s, UmmaConv& u, int& smem, int& ctas_per_sm) {
         u.passes = (27 + taps - 1) / taps;
         u.w_chunks = (unsigned)(taps * cpt);
     }
-    smem = base + (int)u.w_chunks * s.cout * 16;
+    u.k_steps = (u.w_chunks + 1) / 2;
+    smem = base + (int)u.w_chunks * s.cout * 16 + (int)u.k_steps * 16;
     unsigned cols = 32;
     while (cols < (unsigned)(u.tz * s.cout)) cols <<= 1;
     u.tmem_cols = cols;
@@ -706,34 +706,31 @@ bool umma_plan(const ConvShape& s, UmmaConv& u, int& smem, int& ctas_per_sm) {
     return ctas_per_sm >= 1;
 }
 
-template <int N>
+template <int CPT>
 int launch_umma(const __nv_bfloat16* x, const __nv_bfloat16* w, const float* bias, __nv_bfloat16* y,
-                ConvShape s, int relu, cudaStream_t st) {
-    UmmaConv u{};
-    int smem = 0, per_sm = 0;
-    if (!umma_plan(s, u, smem, per_sm)) return -1;
+                const UmmaConv& u, int smem, int per_sm, int relu, cudaStream_t st) {
     int dev = 0, sms = 0;
     if (cudaGetDevice(&dev) != cudaSuccess ||
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
         return -2;
-    if (cudaFuncSetAttribute(conv3d_umma_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    if (cudaFuncSetAttribute(conv3d_umma_kernel<CPT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              smem) != cudaSuccess)
         return -2;
     const int grid = u.n_tiles < sms * per_sm ? u.n_tiles : sms * per_sm;
-    conv3d_umma_kernel<N><<<grid, 128, smem, st>>>(x, w, bias, y, u, relu);
+    conv3d_umma_kernel<CPT><<<grid, 128, smem, st>>>(x, w, bias, y, u, relu);
     return launched();
 }
 
 int dispatch_umma(const __nv_bfloat16* x, const __nv_bfloat16* w, const float* bias,
-                  __nv_bfloat16* y, ConvShape s, int relu, cudaStream_t st) {
-    switch (s.cout) {
-        case 16: return launch_umma<16>(x, w, bias, y, s, relu, st);
-        case 32: return launch_umma<32>(x, w, bias, y, s, relu, st);
-        case 48: return launch_umma<48>(x, w, bias, y, s, relu, st);
-        case 64: return launch_umma<64>(x, w, bias, y, s, relu, st);
-        case 96: return launch_umma<96>(x, w, bias, y, s, relu, st);
-        case 128: return launch_umma<128>(x, w, bias, y, s, relu, st);
-        case 192: return launch_umma<192>(x, w, bias, y, s, relu, st);
+                  __nv_bfloat16* y, const UmmaConv& u, int smem, int per_sm, int relu,
+                  cudaStream_t st) {
+    switch (u.s.cin / 8) {
+        case 1: return launch_umma<1>(x, w, bias, y, u, smem, per_sm, relu, st);
+        case 2: return launch_umma<2>(x, w, bias, y, u, smem, per_sm, relu, st);
+        case 4: return launch_umma<4>(x, w, bias, y, u, smem, per_sm, relu, st);
+        case 6: return launch_umma<6>(x, w, bias, y, u, smem, per_sm, relu, st);
+        case 8: return launch_umma<8>(x, w, bias, y, u, smem, per_sm, relu, st);
+        case 12: return launch_umma<12>(x, w, bias, y, u, smem, per_sm, relu, st);
         default: return -1;
     }
 }
@@ -752,9 +749,11 @@ int pmd_conv3d(const void* x, const void* w, const float* bias, void* y, int n, 
     auto Y = (__nv_bfloat16*)y;
     cudaStream_t st = (cudaStream_t)stream;
     if (g_conv_impl != 1) {
+        // auto: the tensor-memory kernel where its weights stay resident (one pass)
         UmmaConv u{};
         int smem = 0, per_sm = 0;
-        if (umma_plan(s, u, smem, per_sm)) return dispatch_umma(X, W, bias, Y, s, relu, st);
+        if (umma_plan(s, u, smem, per_sm) && (g_conv_impl == 2 || u.passes == 1))
+            return dispatch_umma(X, W, bias, Y, u, smem, per_sm, relu, st);
         if (g_conv_impl == 2) return -1;
     }
     switch (cout) {

@@ -40,6 +40,7 @@ struct UmmaConv {
     int tiles_d, tiles_h, tiles_w, n_tiles;
     unsigned halo_bytes, plane_bytes;
     unsigned w_chunks;  // weight chunks staged per pass (incl. the cin = 8 pad partner)
+    unsigned k_steps;   // K steps (16-wide) per pass: descriptor table entries
     unsigned tmem_cols;
 };
 
@@ -128,18 +129,22 @@ __device__ __forceinline__ uint32_t tap_offset(int t) {
     return (uint32_t)(((t / 9) * kUHY * kUHX + ((t / 3) % 3) * kUHX + t % 3) * 16);
 }
 
-template <int N>
+// CPT = cin / 8, the 8-channel chunks (halo planes) per tap.
+template <int CPT>
 __global__ void __launch_bounds__(128, 4)
 conv3d_umma_kernel(const __nv_bfloat16* __restrict__ x, const __nv_bfloat16* __restrict__ wt,
                    const float* __restrict__ bias, __nv_bfloat16* __restrict__ y, UmmaConv u,
                    int relu) {
     extern __shared__ __align__(1024) unsigned char smem[];
     const ConvShape& s = u.s;
+    const int N = s.cout;
+    constexpr int cpt = CPT;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int cpt = s.cin / 8;  // 8-channel chunks (halo planes) per tap
     unsigned char* halo = smem;
     unsigned char* wbuf = smem + u.halo_bytes + kUSlack;
-    uint64_t* mbar_p = reinterpret_cast<uint64_t*>(wbuf + (size_t)u.w_chunks * N * 16);
+    // per-pass descriptor table: A (slice 0) and B descriptor of every K step
+    uint64_t* dtab = reinterpret_cast<uint64_t*>(wbuf + (size_t)u.w_chunks * N * 16);
+    uint64_t* mbar_p = dtab + 2 * u.k_steps;
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mbar_p + 1);
     const uint32_t halo_s = smem_u32(halo), w_s = smem_u32(wbuf), mbar = smem_u32(mbar_p);
 
@@ -196,6 +201,7 @@ conv3d_umma_kernel(const __nv_bfloat16* __restrict__ x, const __nv_bfloat16* __r
             const int t1 = min(27, t0 + u.taps_per_pass);
             const int j0 = t0 * cpt;
             const int j1 = t1 * cpt;
+            const int k_begin = j0 / 2, k_end = (j1 + 1) / 2;
             if (u.passes > 1 || !weights_resident) {
                 const int n_chunks = (int)u.w_chunks < (j1 - j0 + (j1 - j0) % 2) ? (int)u.w_chunks
                                                                                : (j1 - j0 + (j1 - j0) % 2);
@@ -203,6 +209,16 @@ conv3d_umma_kernel(const __nv_bfloat16* __restrict__ x, const __nv_bfloat16* __r
                     const int n = i % N, jj = i / N;
                     cp_async16(wbuf + ((size_t)jj * N + n) * 16,
                                wt + (long long)n * s.kpad + (long long)(j0 + jj) * 8, true);
+                }
+                for (int k = k_begin + tid; k < k_end; k += blockDim.x) {
+                    const int j = 2 * k;
+                    const int tap = j / cpt, q = j % cpt;
+                    const uint32_t a_addr = halo_s + (uint32_t)q * u.plane_bytes + tap_offset(tap);
+                    uint32_t a_lbo = u.plane_bytes;
+                    if (cpt == 1) a_lbo = tap + 1 < 27 ? tap_offset(tap + 1) - tap_offset(tap) : 16u;
+                    dtab[2 * (k - k_begin)] = umma_smem_desc(a_addr, a_lbo, kUHX * 16);
+                    dtab[2 * (k - k_begin) + 1] =
+                        umma_smem_desc(w_s + (uint32_t)(j - j0) * N * 16, N * 16, 128);
                 }
                 weights_resident = true;
             }
@@ -212,20 +228,14 @@ conv3d_umma_kernel(const __nv_bfloat16* __restrict__ x, const __nv_bfloat16* __r
             __syncthreads();
             if (tid == 0) {
                 tc_fence_after();
-                const int k_begin = j0 / 2, k_end = (j1 + 1) / 2;
+                const int n_k = k_end - k_begin;
+                // slice sl reads the halo kUHY * kUHX rows further: add to the start-address field
+                constexpr uint64_t slice_inc = (uint64_t)(kUHY * kUHX * 16) >> 4;
                 for (int sl = 0; sl < u.tz; ++sl) {
-                    for (int k = k_begin; k < k_end; ++k) {
-                        const int j = 2 * k;
-                        const int tap = j / cpt, q = j % cpt;
-                        const uint32_t a_addr = halo_s + (uint32_t)q * u.plane_bytes +
-                                                (uint32_t)(sl * kUHY * kUHX * 16) + tap_offset(tap);
-                        uint32_t a_lbo = u.plane_bytes;
-                        if (cpt == 1) a_lbo = tap + 1 < 27 ? tap_offset(tap + 1) - tap_offset(tap) : 16u;
-                        const uint32_t b_addr = w_s + (uint32_t)(j - j0) * N * 16;
-                        umma_bf16(tmem + (uint32_t)(sl * N), umma_smem_desc(a_addr, a_lbo, kUHX * 16),
-                                  umma_smem_desc(b_addr, N * 16, 128), idesc,
-                                  (pass > 0 || k > k_begin) ? 1u : 0u);
-                    }
+                    const uint32_t d_tmem = tmem + (uint32_t)(sl * N);
+                    for (int k = 0; k < n_k; ++k)
+                        umma_bf16(d_tmem, dtab[2 * k] + slice_inc * (uint64_t)sl, dtab[2 * k + 1],
+                                  idesc, (pass > 0 || k > 0) ? 1u : 0u);
                 }
                 umma_commit(mbar);
             }
@@ -244,7 +254,6 @@ conv3d_umma_kernel(const __nv_bfloat16* __restrict__ x, const __nv_bfloat16* __r
             const bool ok = z < s.d && yg < s.h && xg < s.w;
             __nv_bfloat16* out = y + ((((long long)nb * s.d + (ok ? z : 0)) * s.h + (ok ? yg : 0)) * s.w +
                                       (ok ? xg : 0)) * N;
-#pragma unroll
             for (int c = 0; c < N / 16; ++c) {
                 float v[16];
                 tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(sl * N + c * 16), v);
