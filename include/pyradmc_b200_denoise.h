@@ -61,18 +61,21 @@ int pmd_conv3d_wgrad(const void* x, const void* g, float* dw, float* dbias, int 
  * bf16 [cin][kpad_d], columns past 27 * cout zero. */
 int pmd_flip_weights(const void* w, void* wd, int cin, int cout, int kpad, int kpad_d, void* stream);
 
-/* ReLU backward in place: g[i] = 0 where y[i] <= 0 (n elements). */
+/* ReLU backward in place: g[i] = 0 where y[i] <= 0 (n elements, a multiple
+ * of 8). */
 int pmd_relu_mask(void* g, const void* y, int64_t n, void* stream);
 
 /* 2x2x2 average pooling of x [n, d, h, w, c] into y [n, d/2, h/2, w/2, c], and
- * its gradient (written, or added onto gx when accumulate != 0). */
+ * its gradient (written, or added onto gx when accumulate != 0).  c a multiple
+ * of 8; d, h, w even; fewer than 2^31 elements. */
 int pmd_avgpool(const void* x, void* y, int n, int d, int h, int w, int c, void* stream);
 int pmd_avgpool_grad(const void* gy, void* gx, int n, int d, int h, int w, int c, int accumulate,
                      void* stream);
 
 /* Decoder join: out [n, d, h, w, c_up + c_skip] = concat(nearest-upsample x2 of
  * up [n, d/2, h/2, w/2, c_up], skip), and its gradient (the skip part written,
- * or added onto gskip when accumulate != 0). */
+ * or added onto gskip when accumulate != 0).  c_up, c_skip multiples of 8;
+ * d, h, w even; fewer than 2^31 elements. */
 int pmd_upcat(const void* up, const void* skip, void* out, int n, int d, int h, int w, int c_up,
               int c_skip, void* stream);
 int pmd_upcat_grad(const void* gout, void* gup, void* gskip, int n, int d, int h, int w, int c_up,
@@ -80,7 +83,7 @@ int pmd_upcat_grad(const void* gout, void* gup, void* gskip, int n, int d, int h
 
 /* Output head: out[m] = base[m] + b[0] + sum_c w[c] * f[m][c] over m voxels
  * (fp32; base may be NULL), and its gradient: df = g w^T (bf16), dw += f^T g,
- * db += sum g (c <= 64). */
+ * db += sum g.  c in {8, 16, 32, 64}. */
 int pmd_head(const void* f, const float* w, const float* b, const float* base, float* out,
              int64_t m, int c, void* stream);
 int pmd_head_grad(const void* f, const float* w, const float* g, void* df, float* dw, float* db,

@@ -308,11 +308,40 @@ conv3d_wgrad_kernel(const __nv_bfloat16* __restrict__ x, const __nv_bfloat16* __
 }
 
 // ---- element-wise and data-movement kernels -------------------------------------------
-// ReLU backward in place: g <- g * (y > 0).
-__global__ void relu_mask_kernel(__nv_bfloat16* g, const __nv_bfloat16* y, long long n) {
+// 16-byte vectors of 8 bf16 channels.
+union Pack8 {
+    uint4 u;
+    __nv_bfloat162 h[4];
+};
+__device__ __forceinline__ void unpack8(uint4 v, float* f) {
+    Pack8 p;
+    p.u = v;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const float2 t = __bfloat1622float2(p.h[i]);
+        f[2 * i] = t.x;
+        f[2 * i + 1] = t.y;
+    }
+}
+__device__ __forceinline__ uint4 pack8(const float* f) {
+    Pack8 p;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) p.h[i] = __floats2bfloat162_rn(f[2 * i], f[2 * i + 1]);
+    return p.u;
+}
+
+// ReLU backward in place: g <- g * (y > 0), 8 channels per thread (n8 vectors).
+__global__ void relu_mask_kernel(uint4* g, const uint4* y, long long n8) {
     const long long stride = (long long)gridDim.x * blockDim.x;
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
-        if (!(__bfloat162float(y[i]) > 0.0f)) g[i] = __float2bfloat16(0.0f);
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n8; i += stride) {
+        float gv[8], yv[8];
+        unpack8(g[i], gv);
+        unpack8(__ldg(y + i), yv);
+#pragma unroll
+        for (int k = 0; k < 8; ++k)
+            if (!(yv[k] > 0.0f)) gv[k] = 0.0f;
+        g[i] = pack8(gv);
+    }
 }
 
 // Weights for the data gradient: Wd[ci][tap' * cout + co] = W[co][(26 - tap') * cin + ci].
@@ -331,113 +360,144 @@ __global__ void flip_weights_kernel(const __nv_bfloat16* w, __nv_bfloat16* wd, i
     }
 }
 
-// 2x2x2 average pooling, NDHWC; and its gradient (each input voxel gets 1/8).
-__global__ void avgpool_kernel(const __nv_bfloat16* x, __nv_bfloat16* y, int n, int d, int h, int w,
-                               int c) {
+// 2x2x2 average pooling, NDHWC, one 8-channel vector per thread (c8 = c / 8
+// vectors per voxel; 32-bit indices: the host bounds the element counts).
+__global__ void avgpool_kernel(const uint4* x, uint4* y, int n, int d, int h, int w, int c8) {
     const int d2 = d / 2, h2 = h / 2, w2 = w / 2;
-    const long long total = (long long)n * d2 * h2 * w2 * c;
-    const long long stride = (long long)gridDim.x * blockDim.x;
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += stride) {
-        long long t = i;
-        const int ch = (int)(t % c); t /= c;
-        const int xx = (int)(t % w2); t /= w2;
-        const int yy = (int)(t % h2); t /= h2;
-        const int zz = (int)(t % d2);
-        const int nn = (int)(t / d2);
-        float s = 0.0f;
-        for (int dz = 0; dz < 2; ++dz)
-            for (int dy = 0; dy < 2; ++dy)
-                for (int dx = 0; dx < 2; ++dx)
-                    s += __bfloat162float(
-                        x[((((long long)nn * d + 2 * zz + dz) * h + 2 * yy + dy) * w + 2 * xx + dx) * c + ch]);
-        y[i] = __float2bfloat16(0.125f * s);
+    const int total = n * d2 * h2 * w2 * c8;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
+        int t = i;
+        const int cc = t % c8; t /= c8;
+        const int xx = t % w2; t /= w2;
+        const int yy = t % h2; t /= h2;
+        const int zz = t % d2;
+        const int nn = t / d2;
+        const int v0 = ((nn * d + 2 * zz) * h + 2 * yy) * w + 2 * xx;
+        float acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
+        for (int o = 0; o < 8; ++o) {
+            float f[8];
+            unpack8(__ldg(x + (size_t)(v0 + (o >> 2) * h * w + ((o >> 1) & 1) * w + (o & 1)) * c8 + cc), f);
+#pragma unroll
+            for (int k = 0; k < 8; ++k) acc[k] += f[k];
+        }
+#pragma unroll
+        for (int k = 0; k < 8; ++k) acc[k] *= 0.125f;
+        y[i] = pack8(acc);
     }
 }
 
-__global__ void avgpool_grad_kernel(const __nv_bfloat16* gy, __nv_bfloat16* gx, int n, int d, int h,
-                                    int w, int c, int accumulate) {
-    const long long total = (long long)n * d * h * w * c;
-    const long long stride = (long long)gridDim.x * blockDim.x;
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += stride) {
-        long long t = i;
-        const int ch = (int)(t % c); t /= c;
-        const int xx = (int)(t % w); t /= w;
-        const int yy = (int)(t % h); t /= h;
-        const int zz = (int)(t % d);
-        const int nn = (int)(t / d);
-        const float v = 0.125f * __bfloat162float(
-            gy[((((long long)nn * (d / 2) + zz / 2) * (h / 2) + yy / 2) * (w / 2) + xx / 2) * c + ch]);
-        gx[i] = __float2bfloat16(accumulate ? v + __bfloat162float(gx[i]) : v);
+__global__ void avgpool_grad_kernel(const uint4* gy, uint4* gx, int n, int d, int h, int w, int c8,
+                                    int accumulate) {
+    const int total = n * d * h * w * c8;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
+        int t = i;
+        const int cc = t % c8; t /= c8;
+        const int xx = t % w; t /= w;
+        const int yy = t % h; t /= h;
+        const int zz = t % d;
+        const int nn = t / d;
+        float v[8];
+        unpack8(__ldg(gy + (size_t)(((nn * (d / 2) + zz / 2) * (h / 2) + yy / 2) * (w / 2) + xx / 2) * c8 + cc), v);
+#pragma unroll
+        for (int k = 0; k < 8; ++k) v[k] *= 0.125f;
+        if (accumulate) {
+            float o[8];
+            unpack8(gx[i], o);
+#pragma unroll
+            for (int k = 0; k < 8; ++k) v[k] += o[k];
+        }
+        gx[i] = pack8(v);
     }
 }
 
-// Nearest 2x upsampling of `up` (c_up channels) into channels [0, c_up) of a
-// concatenated tensor whose channels [c_up, c_up + c_skip) copy the skip input.
-__global__ void upcat_kernel(const __nv_bfloat16* up, const __nv_bfloat16* skip, __nv_bfloat16* out,
-                             int n, int d, int h, int w, int c_up, int c_skip) {
-    const int c = c_up + c_skip;
-    const long long total = (long long)n * d * h * w * c;
-    const long long stride = (long long)gridDim.x * blockDim.x;
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += stride) {
-        long long t = i;
-        const int ch = (int)(t % c); t /= c;
-        const long long vox = t;
-        const int xx = (int)(t % w); t /= w;
-        const int yy = (int)(t % h); t /= h;
-        const int zz = (int)(t % d);
-        const int nn = (int)(t / d);
-        __nv_bfloat16 v;
-        if (ch < c_up)
-            v = up[((((long long)nn * (d / 2) + zz / 2) * (h / 2) + yy / 2) * (w / 2) + xx / 2) * c_up + ch];
-        else
-            v = skip[vox * c_skip + (ch - c_up)];
+// Nearest 2x upsampling of `up` (cu8 vectors per voxel) into the first
+// vectors of a concatenated tensor whose remaining cs8 vectors copy `skip`.
+__global__ void upcat_kernel(const uint4* up, const uint4* skip, uint4* out, int n, int d, int h, int w,
+                             int cu8, int cs8) {
+    const int c8 = cu8 + cs8;
+    const int total = n * d * h * w * c8;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
+        const int cc = i % c8;
+        const int vox = i / c8;
+        uint4 v;
+        if (cc < cu8) {
+            int t = vox;
+            const int xx = t % w; t /= w;
+            const int yy = t % h; t /= h;
+            const int zz = t % d;
+            const int nn = t / d;
+            v = __ldg(up + (size_t)(((nn * (d / 2) + zz / 2) * (h / 2) + yy / 2) * (w / 2) + xx / 2) * cu8 + cc);
+        } else {
+            v = __ldg(skip + (size_t)vox * cs8 + (cc - cu8));
+        }
         out[i] = v;
     }
 }
 
 // Gradient of upcat: the up part sums its 8 children; the skip part is copied
 // (added onto an existing skip gradient when `accumulate`).
-__global__ void upcat_grad_kernel(const __nv_bfloat16* gout, __nv_bfloat16* gup, __nv_bfloat16* gskip,
-                                  int n, int d, int h, int w, int c_up, int c_skip, int accumulate) {
-    const int c = c_up + c_skip;
+__global__ void upcat_grad_kernel(const uint4* gout, uint4* gup, uint4* gskip, int n, int d, int h,
+                                  int w, int cu8, int cs8, int accumulate) {
+    const int c8 = cu8 + cs8;
     const int d2 = d / 2, h2 = h / 2, w2 = w / 2;
-    const long long n_up = (long long)n * d2 * h2 * w2 * c_up;
-    const long long n_skip = (long long)n * d * h * w * c_skip;
-    const long long stride = (long long)gridDim.x * blockDim.x;
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n_up + n_skip; i += stride) {
+    const int n_up = n * d2 * h2 * w2 * cu8;
+    const int n_skip = n * d * h * w * cs8;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n_up + n_skip; i += gridDim.x * blockDim.x) {
         if (i < n_up) {
-            long long t = i;
-            const int ch = (int)(t % c_up); t /= c_up;
-            const int xx = (int)(t % w2); t /= w2;
-            const int yy = (int)(t % h2); t /= h2;
-            const int zz = (int)(t % d2);
-            const int nn = (int)(t / d2);
-            float s = 0.0f;
-            for (int dz = 0; dz < 2; ++dz)
-                for (int dy = 0; dy < 2; ++dy)
-                    for (int dx = 0; dx < 2; ++dx)
-                        s += __bfloat162float(
-                            gout[((((long long)nn * d + 2 * zz + dz) * h + 2 * yy + dy) * w + 2 * xx + dx) * c + ch]);
-            gup[i] = __float2bfloat16(s);
+            int t = i;
+            const int cc = t % cu8; t /= cu8;
+            const int xx = t % w2; t /= w2;
+            const int yy = t % h2; t /= h2;
+            const int zz = t % d2;
+            const int nn = t / d2;
+            const int v0 = ((nn * d + 2 * zz) * h + 2 * yy) * w + 2 * xx;
+            float acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
+            for (int o = 0; o < 8; ++o) {
+                float f[8];
+                unpack8(__ldg(gout + (size_t)(v0 + (o >> 2) * h * w + ((o >> 1) & 1) * w + (o & 1)) * c8 + cc), f);
+#pragma unroll
+                for (int k = 0; k < 8; ++k) acc[k] += f[k];
+            }
+            gup[i] = pack8(acc);
         } else {
-            const long long j = i - n_up;
-            const long long vox = j / c_skip;
-            const int ch = (int)(j % c_skip);
-            const float v = __bfloat162float(gout[vox * c + c_up + ch]);
-            gskip[j] = __float2bfloat16(accumulate ? v + __bfloat162float(gskip[j]) : v);
+            const int j = i - n_up;
+            const int vox = j / cs8, cc = j % cs8;
+            uint4 v = __ldg(gout + (size_t)vox * c8 + cu8 + cc);
+            if (accumulate) {
+                float a[8], b[8];
+                unpack8(v, a);
+                unpack8(gskip[j], b);
+#pragma unroll
+                for (int k = 0; k < 8; ++k) a[k] += b[k];
+                v = pack8(a);
+            }
+            gskip[j] = v;
         }
     }
 }
 
 // Head: out[m] = base[m] + b + sum_c w[c] f[m][c] (a 1x1x1 conv to one channel,
 // added to the noisy input dose: the network predicts a correction).
-__global__ void head_kernel(const __nv_bfloat16* f, const float* w, const float* b, const float* base,
-                            float* out, long long m_total, int c) {
+template <int C>
+__global__ void head_kernel(const uint4* f, const float* w, const float* b, const float* base,
+                            float* out, long long m_total) {
+    float wl[C];
+#pragma unroll
+    for (int k = 0; k < C; ++k) wl[k] = __ldg(w + k);
+    const float bias = __ldg(b);
     const long long stride = (long long)gridDim.x * blockDim.x;
     for (long long m = (long long)blockIdx.x * blockDim.x + threadIdx.x; m < m_total; m += stride) {
-        float s = b[0] + (base ? base[m] : 0.0f);
-        for (int k = 0; k < c; ++k) s += w[k] * __bfloat162float(f[m * c + k]);
-        out[m] = s;
+        float acc = bias + (base ? base[m] : 0.0f);
+#pragma unroll
+        for (int c = 0; c < C / 8; ++c) {
+            float v[8];
+            unpack8(__ldg(f + m * (C / 8) + c), v);
+#pragma unroll
+            for (int k = 0; k < 8; ++k) acc += wl[c * 8 + k] * v[k];
+        }
+        out[m] = acc;
     }
 }
 
@@ -462,21 +522,34 @@ __global__ void loss_kernel(const float* pred, const float* target, const float*
 }
 
 // Head backward: dF[m][c] = g[m] w[c] (bf16), dW[c] += sum_m g[m] f[m][c], db += sum_m g[m].
-__global__ void head_grad_kernel(const __nv_bfloat16* f, const float* w, const float* g,
-                                 __nv_bfloat16* df, float* dw, float* db, long long m_total, int c) {
-    float lw[64];
-    for (int k = 0; k < c; ++k) lw[k] = 0.0f;
+template <int C>
+__global__ void head_grad_kernel(const uint4* f, const float* w, const float* g, uint4* df,
+                                 float* dw, float* db, long long m_total) {
+    float wl[C], lw[C];
+#pragma unroll
+    for (int k = 0; k < C; ++k) {
+        wl[k] = __ldg(w + k);
+        lw[k] = 0.0f;
+    }
     float lb = 0.0f;
     const long long stride = (long long)gridDim.x * blockDim.x;
     for (long long m = (long long)blockIdx.x * blockDim.x + threadIdx.x; m < m_total; m += stride) {
         const float gm = g[m];
         lb += gm;
-        for (int k = 0; k < c; ++k) {
-            lw[k] += gm * __bfloat162float(f[m * c + k]);
-            df[m * c + k] = __float2bfloat16(gm * w[k]);
+#pragma unroll
+        for (int c = 0; c < C / 8; ++c) {
+            float v[8], o[8];
+            unpack8(__ldg(f + m * (C / 8) + c), v);
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                lw[c * 8 + k] += gm * v[k];
+                o[k] = gm * wl[c * 8 + k];
+            }
+            df[m * (C / 8) + c] = pack8(o);
         }
     }
-    for (int k = 0; k < c; ++k) {
+#pragma unroll
+    for (int k = 0; k < C; ++k) {
         float v = lw[k];
 #pragma unroll
         for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
@@ -646,6 +719,9 @@ void launch_wgrad(const __nv_bfloat16* x, const __nv_bfloat16* g, float* dw, flo
 
 int launched() { return cudaGetLastError() == cudaSuccess ? 0 : -2; }
 
+// The vectorized element-wise kernels index with 32-bit integers.
+bool fits32(long long elements) { return elements < (1LL << 31); }
+
 // Convolution path: 0 = tensor-memory UMMA kernel where it applies, else the
 // mma.sync kernel; 1 = mma.sync only; 2 = UMMA only.
 int g_conv_impl = 0;
@@ -810,57 +886,74 @@ int pmd_flip_weights(const void* w, void* wd, int cin, int cout, int kpad, int k
 }
 
 int pmd_relu_mask(void* g, const void* y, int64_t n, void* stream) {
-    relu_mask_kernel<<<grid_for(n), 256, 0, (cudaStream_t)stream>>>((__nv_bfloat16*)g,
-                                                                    (const __nv_bfloat16*)y, n);
+    if (n % 8) return -1;
+    relu_mask_kernel<<<grid_for(n / 8), 256, 0, (cudaStream_t)stream>>>((uint4*)g, (const uint4*)y,
+                                                                        n / 8);
     return launched();
 }
 
 int pmd_avgpool(const void* x, void* y, int n, int d, int h, int w, int c, void* stream) {
-    if (d % 2 || h % 2 || w % 2) return -1;
-    avgpool_kernel<<<grid_for((long long)n * d * h * w * c / 8), 256, 0, (cudaStream_t)stream>>>(
-        (const __nv_bfloat16*)x, (__nv_bfloat16*)y, n, d, h, w, c);
+    if (d % 2 || h % 2 || w % 2 || c % 8 || !fits32((long long)n * d * h * w * c)) return -1;
+    avgpool_kernel<<<grid_for((long long)n * d * h * w * c / 64), 256, 0, (cudaStream_t)stream>>>(
+        (const uint4*)x, (uint4*)y, n, d, h, w, c / 8);
     return launched();
 }
 
 int pmd_avgpool_grad(const void* gy, void* gx, int n, int d, int h, int w, int c, int accumulate,
                      void* stream) {
-    if (d % 2 || h % 2 || w % 2) return -1;
-    avgpool_grad_kernel<<<grid_for((long long)n * d * h * w * c), 256, 0, (cudaStream_t)stream>>>(
-        (const __nv_bfloat16*)gy, (__nv_bfloat16*)gx, n, d, h, w, c, accumulate);
+    if (d % 2 || h % 2 || w % 2 || c % 8 || !fits32((long long)n * d * h * w * c)) return -1;
+    avgpool_grad_kernel<<<grid_for((long long)n * d * h * w * c / 8), 256, 0, (cudaStream_t)stream>>>(
+        (const uint4*)gy, (uint4*)gx, n, d, h, w, c / 8, accumulate);
     return launched();
 }
 
 int pmd_upcat(const void* up, const void* skip, void* out, int n, int d, int h, int w, int c_up,
               int c_skip, void* stream) {
-    if (d % 2 || h % 2 || w % 2 || c_skip < 1) return -1;
-    upcat_kernel<<<grid_for((long long)n * d * h * w * (c_up + c_skip)), 256, 0, (cudaStream_t)stream>>>(
-        (const __nv_bfloat16*)up, (const __nv_bfloat16*)skip, (__nv_bfloat16*)out, n, d, h, w, c_up,
-        c_skip);
+    if (d % 2 || h % 2 || w % 2 || c_skip < 8 || c_up < 8 || c_up % 8 || c_skip % 8 ||
+        !fits32((long long)n * d * h * w * (c_up + c_skip)))
+        return -1;
+    upcat_kernel<<<grid_for((long long)n * d * h * w * (c_up + c_skip) / 8), 256, 0,
+                   (cudaStream_t)stream>>>((const uint4*)up, (const uint4*)skip, (uint4*)out, n, d,
+                                           h, w, c_up / 8, c_skip / 8);
     return launched();
 }
 
 int pmd_upcat_grad(const void* gout, void* gup, void* gskip, int n, int d, int h, int w, int c_up,
                    int c_skip, int accumulate, void* stream) {
-    if (d % 2 || h % 2 || w % 2 || c_skip < 1) return -1;
-    const long long total = (long long)n * d * h * w * c_skip + (long long)n * d * h * w * c_up / 8;
+    if (d % 2 || h % 2 || w % 2 || c_skip < 8 || c_up < 8 || c_up % 8 || c_skip % 8 ||
+        !fits32((long long)n * d * h * w * (c_up + c_skip)))
+        return -1;
+    const long long total = ((long long)n * d * h * w * c_skip + (long long)n * d * h * w * c_up / 8) / 8;
     upcat_grad_kernel<<<grid_for(total), 256, 0, (cudaStream_t)stream>>>(
-        (const __nv_bfloat16*)gout, (__nv_bfloat16*)gup, (__nv_bfloat16*)gskip, n, d, h, w, c_up,
-        c_skip, accumulate);
+        (const uint4*)gout, (uint4*)gup, (uint4*)gskip, n, d, h, w, c_up / 8, c_skip / 8, accumulate);
     return launched();
 }
 
 int pmd_head(const void* f, const float* w, const float* b, const float* base, float* out,
              int64_t m, int c, void* stream) {
-    head_kernel<<<grid_for(m), 256, 0, (cudaStream_t)stream>>>((const __nv_bfloat16*)f, w, b, base,
-                                                                out, m, c);
+    cudaStream_t st = (cudaStream_t)stream;
+    switch (c) {
+        case 8: head_kernel<8><<<grid_for(m), 256, 0, st>>>((const uint4*)f, w, b, base, out, m); break;
+        case 16: head_kernel<16><<<grid_for(m), 256, 0, st>>>((const uint4*)f, w, b, base, out, m); break;
+        case 32: head_kernel<32><<<grid_for(m), 256, 0, st>>>((const uint4*)f, w, b, base, out, m); break;
+        case 64: head_kernel<64><<<grid_for(m), 256, 0, st>>>((const uint4*)f, w, b, base, out, m); break;
+        default: return -1;
+    }
     return launched();
 }
 
 int pmd_head_grad(const void* f, const float* w, const float* g, void* df, float* dw, float* db,
                   int64_t m, int c, void* stream) {
-    if (c > 64) return -1;
-    head_grad_kernel<<<grid_for(m), 256, 0, (cudaStream_t)stream>>>(
-        (const __nv_bfloat16*)f, w, g, (__nv_bfloat16*)df, dw, db, m, c);
+    cudaStream_t st = (cudaStream_t)stream;
+    auto F = (const uint4*)f;
+    auto DF = (uint4*)df;
+    switch (c) {
+        case 8: head_grad_kernel<8><<<grid_for(m), 256, 0, st>>>(F, w, g, DF, dw, db, m); break;
+        case 16: head_grad_kernel<16><<<grid_for(m), 256, 0, st>>>(F, w, g, DF, dw, db, m); break;
+        case 32: head_grad_kernel<32><<<grid_for(m), 256, 0, st>>>(F, w, g, DF, dw, db, m); break;
+        case 64: head_grad_kernel<64><<<grid_for(m), 256, 0, st>>>(F, w, g, DF, dw, db, m); break;
+        default: return -1;
+    }
     return launched();
 }
 
