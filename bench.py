@@ -263,6 +263,112 @@ def algorithmic_bytes(c: dict) -> float:
             + 48.0 * c["queue_pushes"] + 48.0 * pops)
 
 
+DENOISER_WEIGHTS = ROOT / "pyradmc_b200" / "data" / "denoiser_unet.npz"
+REF_HISTORIES = 8_000_000     # per beamlet: the high-statistics judge of the denoiser's error
+LADDER = (1 / 4, 1 / 2, 1.0, 2.0, 4.0, 8.0)  # history scales tried for MC + denoiser
+
+
+def denoiser_leg(args, engine, source, counts, stream, device, plain_s_at_2pct):
+    """s per Dij at 2 % for MC + denoiser on the benchmark Dij.
+
+    Untimed: a REF_HISTORIES-per-beamlet reference, then the smallest history
+    scale of LADDER (times the benchmark's per-beamlet counts) whose denoised
+    columns reach a sigma-equivalent error <= 2 % against it.  Timed (CUDA
+    events on the engine's stream): ``run_dij_denoised`` at that scale, from
+    transport to the host CSC."""
+    import torch
+
+    from pyradmc_b200 import _lib
+    from pyradmc_b200 import denoise_dij as D
+    from pyradmc_b200.denoiser import UNet3D, forward_flops_per_voxel, kpad_for
+
+    if not DENOISER_WEIGHTS.exists():
+        return {"unavailable": f"no trained weights at {DENOISER_WEIGHTS.relative_to(ROOT)}"}
+    net = UNet3D.load(DENOISER_WEIGHTS, device=device)
+    shape = tuple(engine.grid.shape)
+    window = D.inference_window(shape, 64)
+    rho = torch.from_numpy(np.ascontiguousarray(engine.grid.density, dtype=np.float32).ravel()).to(device)
+    ref = engine.run_dij_device(source, REF_HISTORIES, N_BATCHES, SEED + 977, truncation=0.0)
+    ref_dose, _, ref_sigma = D.dense_columns(ref, device, with_sigma=True)
+    ladder, chosen = [], None
+    for g in LADDER:
+        c = np.maximum(N_BATCHES, np.round(counts * g / N_BATCHES).astype(np.int64) * N_BATCHES)
+        view = engine.run_dij_device(source, c, N_BATCHES, SEED + 31, truncation=0.0)
+        dose, colmax, sg = D.dense_columns(view, device, with_sigma=True)
+        den = D.denoise_dense(net, dose, colmax, rho, shape, sigma=sg, window=window)
+        e_den = float(np.nanmean(D.sigma_equivalent_error(den, ref_dose, ref_sigma)))
+        e_mc = float(np.nanmean(D.sigma_equivalent_error(dose, ref_dose, ref_sigma)))
+        ladder.append({"scale": g, "histories": int(c.sum()), "sigma_eq_denoised": e_den,
+                       "sigma_eq_plain": e_mc})
+        del den, dose, sg
+        if e_den <= 0.02:
+            chosen = (g, c)
+            break
+    del ref_dose, ref_sigma
+    if chosen is None:
+        return {"reached_2pct": False, "ladder": ladder,
+                "reference_histories_per_beamlet": REF_HISTORIES}
+    g, c = chosen
+    kw = dict(n_histories_per_beamlet=c, n_batches=N_BATCHES, seed=SEED)
+    for _ in range(max(1, args.warmup)):
+        D.run_dij_denoised(engine, net, source, truncation=1e-3, **kw)
+    times, launches0 = [], net.launches
+    torch.cuda.synchronize()
+    for _ in range(args.steps):
+        start = torch.cuda.Event(enable_timing=True)
+        end = torch.cuda.Event(enable_timing=True)
+        start.record(stream)
+        dij = D.run_dij_denoised(engine, net, source, truncation=1e-3, **kw)
+        end.record(stream)
+        end.synchronize()
+        times.append(start.elapsed_time(end) / 1e3)
+    unet_launches = (net.launches - launches0) / args.steps
+    s_den = float(np.median(times))
+
+    # the dominant convolution (decoder level 0, 48 -> 16 channels, tensor memory)
+    lib = _lib.load()
+    b, (wx, wy, wz) = 16, window
+    x = torch.randn((b, wx, wy, wz, 48), device=device).to(torch.bfloat16)
+    wt = (0.05 * torch.randn((16, kpad_for(48)), device=device)).to(torch.bfloat16)
+    y = torch.empty((b, wx, wy, wz, 16), device=device, dtype=torch.bfloat16)
+    conv = lambda: lib.pmd_conv3d(x.data_ptr(), wt.data_ptr(), None, y.data_ptr(), b, wx, wy, wz,  # noqa: E731
+                                  48, 16, kpad_for(48), 1, stream.cuda_stream)
+    for _ in range(3):
+        conv()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(10):
+        conv()
+    e1.record(stream)
+    e1.synchronize()
+    conv_s = e0.elapsed_time(e1) / 10 / 1e3
+    conv_tflops = 2.0 * b * wx * wy * wz * 27 * 48 * 16 / conv_s / 1e12
+    unet_vox = len(c) * wx * wy * wz
+    peaks_path = ROOT / "MEASURED_PEAKS.json"
+    peaks = json.loads(peaks_path.read_text()) if peaks_path.exists() else {}
+    bf16_peak = float(peaks.get("bf16_tflops", 1590.0))
+    return {
+        "reached_2pct": True,
+        "s_per_dij_at_2pct": s_den,
+        "plain_s_per_dij_at_2pct": plain_s_at_2pct,
+        "speedup_vs_plain": plain_s_at_2pct / s_den,
+        "history_scale": g,
+        "histories_per_dij": int(c.sum()),
+        "sigma_eq_denoised": ladder[-1]["sigma_eq_denoised"],
+        "sigma_eq_plain_same_histories": ladder[-1]["sigma_eq_plain"],
+        "reference_histories_per_beamlet": REF_HISTORIES,
+        "ladder": ladder,
+        "window": list(window),
+        "unet_launches_per_dij": unet_launches,
+        "unet_forward_flops_per_dij": forward_flops_per_voxel() * unet_vox,
+        "nnz": int(dij.indptr[-1]),
+        "roofline": {"bound": "tensor", "kernel": "conv3d_umma_kernel (decoder level 0, 48->16)",
+                     "achieved": conv_tflops, "peak": bf16_peak, "unit": "TFLOP/s",
+                     "frac": conv_tflops / bf16_peak,
+                     "peak_source": "measured" if "bf16_tflops" in peaks else "fallback"},
+    }
+
+
 def b200_arm(args, world, rank, local):
     import torch
 
@@ -326,6 +432,10 @@ def b200_arm(args, world, rank, local):
     e2e_value = world * histories * args.steps / (e2e_total / 1e3)
 
     c = counters[-1]
+    sigma_pre = phantoms.per_beamlet_sigma(dij)
+    s_at_2pct_pre = total_ms / args.steps / 1e3 * (sigma_pre / 0.02) ** 2
+    den = None if args.no_denoiser else denoiser_leg(args, engine, source, counts, stream, device,
+                                                     s_at_2pct_pre)
     transport_s = c["transport_ms"] / 1e3
     achieved = algorithmic_bytes(c) / transport_s / 1e9
     sigma = phantoms.per_beamlet_sigma(dij)
@@ -358,7 +468,7 @@ def b200_arm(args, world, rank, local):
         "s_per_dij": s_per_dij,
         "per_beamlet_sigma": sigma,
         "s_per_dij_at_2pct_sigma": s_at_2pct,
-        "denoiser": None,
+        "denoiser": den,
         "e2e": {"value": e2e_value, "unit": "histories/s",
                 "h2d_bytes_per_step": int(np.median(h2d)), "d2h_bytes_per_step": int(np.median(d2h))},
         "roofline": {
@@ -398,6 +508,8 @@ def main() -> int:
                          "ncu cannot profile kernels inside graphs with conditional nodes)")
     ap.add_argument("--no-cpu-baseline", action="store_true",
                     help="skip the CPU baseline leg (profiling runs)")
+    ap.add_argument("--no-denoiser", action="store_true",
+                    help="skip the MC + denoiser leg (profiling runs)")
     args = ap.parse_args()
     global WORKLOAD
     WORKLOAD = args.workload

@@ -101,10 +101,12 @@ int pmd_adam(float* p, const float* g, float* m, float* v, void* p16, int64_t n,
 
 /* Network input, 8 channels [m][8]: dose[m] / colmax[m / vox] (colmax NULL:
  * no scaling; a zero maximum scales by 1), density[m % vox] when
- * density_shared != 0 else density[m], and six zero channels.  base (fp32,
- * may be NULL) receives the scaled dose. */
-int pmd_pack_input(const float* dose, const float* density, const float* colmax, int64_t vox,
-                   int density_shared, void* x, float* base, int64_t m, void* stream);
+ * density_shared != 0 else density[m], sigma[m] (the dose's Monte Carlo
+ * standard error; NULL: zero) on the dose's scale, and five zero channels.
+ * base (fp32, may be NULL) receives the scaled dose. */
+int pmd_pack_input(const float* dose, const float* density, const float* sigma,
+                   const float* colmax, int64_t vox, int density_shared, void* x, float* base,
+                   int64_t m, void* stream);
 
 /* Dense columns from a CSC matrix: dense[col * vox + indices[j]] = values[j]
  * (float) for j in [indptr[col], indptr[col + 1]); the rest of dense must be

@@ -56,12 +56,14 @@ class OracleUNet:
     def _conv(self, x, name):
         return F.relu(F.conv3d(x, self.w[name], self.b[name], padding=1))
 
-    def forward(self, dose: torch.Tensor, density: torch.Tensor) -> torch.Tensor:
-        """dose, density [B, D, H, W] -> prediction [B, D, H, W]."""
+    def forward(self, dose: torch.Tensor, density: torch.Tensor, sigma=None) -> torch.Tensor:
+        """dose, density, sigma (optional) [B, D, H, W] -> prediction [B, D, H, W]."""
         b = dose.shape[0]
         x = torch.zeros((b, IN_CHANNELS) + tuple(dose.shape[1:]), dtype=torch.float32)
         x[:, 0] = dose
         x[:, 1] = density
+        if sigma is not None:
+            x[:, 2] = sigma
         e0 = self._conv(self._conv(x, "enc0a"), "enc0b")
         e1 = self._conv(self._conv(F.avg_pool3d(e0, 2), "enc1a"), "enc1b")
         e2 = self._conv(self._conv(F.avg_pool3d(e1, 2), "enc2a"), "enc2b")
@@ -78,9 +80,9 @@ class OracleUNet:
         w = 1.0 + lam * (weight if weight is not None else torch.zeros_like(target))
         return (torch.abs(pred - target) * w).mean()
 
-    def gradients(self, dose, density, target, weight, lam: float):
+    def gradients(self, dose, density, target, weight, lam: float, sigma=None):
         """(loss, flat fp32 gradient in the kernels' parameter layout)."""
-        pred = self.forward(dose, density)
+        pred = self.forward(dose, density, sigma)
         loss = self.loss(pred, target, weight, lam)
         loss.backward()
         g = np.zeros_like(self.flat)

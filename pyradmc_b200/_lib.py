@@ -252,7 +252,7 @@ SIGNATURES.update({
     "pmd_head_grad": (_i, [_v, _v, _v, _v, _v, _v, _l, _i, _v]),
     "pmd_loss": (_i, [_v, _v, _v, _f, _v, _v, _l, _v]),
     "pmd_adam": (_i, [_v, _v, _v, _v, _v, _l, _f, _f, _f, _f, _i, _v]),
-    "pmd_pack_input": (_i, [_v, _v, _v, _l, _i, _v, _v, _l, _v]),
+    "pmd_pack_input": (_i, [_v, _v, _v, _v, _l, _i, _v, _v, _l, _v]),
     "pmd_csc_to_dense": (_i, [_v, _v, _v, _i, _l, _v, _v, _v]),
     "pmd_unscale": (_i, [_v, _v, _l, _v, _l, _v]),
     "pmd_csc_to_dense_f64": (_i, [_v, _v, _v, _i, _l, _v, _v]),

@@ -579,10 +579,11 @@ __global__ void adam_kernel(float* p, const float* g, float* m, float* v, __nv_b
 }
 
 // Network input: channel 0 the column-normalized dose, channel 1 the density,
-// 2..7 zero; one 16-byte store per voxel.
-__global__ void pack_input_kernel(const float* dose, const float* density, const float* colmax,
-                                  long long vox, int density_shared, __nv_bfloat16* x, float* base,
-                                  long long m_total) {
+// channel 2 the dose's Monte Carlo sigma on the same scale, 3..7 zero; one
+// 16-byte store per voxel.
+__global__ void pack_input_kernel(const float* dose, const float* density, const float* sigma,
+                                  const float* colmax, long long vox, int density_shared,
+                                  __nv_bfloat16* x, float* base, long long m_total) {
     const long long stride = (long long)gridDim.x * blockDim.x;
     for (long long m = (long long)blockIdx.x * blockDim.x + threadIdx.x; m < m_total; m += stride) {
         float scale = 1.0f;
@@ -592,13 +593,15 @@ __global__ void pack_input_kernel(const float* dose, const float* density, const
         }
         const float v = dose[m] * scale;
         const float rho = density[density_shared ? m % vox : m];
+        const float sg = sigma ? sigma[m] * scale : 0.0f;
         if (base) base[m] = v;
         union {
             uint4 u;
             __nv_bfloat162 h[4];
         } pk;
         pk.h[0] = __floats2bfloat162_rn(v, rho);
-        pk.h[1] = pk.h[2] = pk.h[3] = __floats2bfloat162_rn(0.0f, 0.0f);
+        pk.h[1] = __floats2bfloat162_rn(sg, 0.0f);
+        pk.h[2] = pk.h[3] = __floats2bfloat162_rn(0.0f, 0.0f);
         *reinterpret_cast<uint4*>(x + m * 8) = pk.u;
     }
 }
@@ -974,11 +977,12 @@ int pmd_adam(float* p, const float* g, float* m, float* v, void* p16, int64_t n,
     return launched();
 }
 
-int pmd_pack_input(const float* dose, const float* density, const float* colmax, int64_t vox,
-                   int density_shared, void* x, float* base, int64_t m, void* stream) {
+int pmd_pack_input(const float* dose, const float* density, const float* sigma,
+                   const float* colmax, int64_t vox, int density_shared, void* x, float* base,
+                   int64_t m, void* stream) {
     if (vox < 1) return -1;
     pack_input_kernel<<<grid_for(m), 256, 0, (cudaStream_t)stream>>>(
-        dose, density, colmax, vox, density_shared, (__nv_bfloat16*)x, base, m);
+        dose, density, sigma, colmax, vox, density_shared, (__nv_bfloat16*)x, base, m);
     return launched();
 }
 

@@ -126,21 +126,24 @@ def scatter(win, scale, grid_shape, origins, dst) -> None:
 class PairSet:
     """Training pairs on the device, each [N, wx, wy, wz] float32: the
     low-history input and the high-history target (both divided by the input
-    column's maximum), the target's sigma on the same scale, the density, and
-    the loss weight."""
+    column's maximum), the target's sigma on the same scale, the density, the
+    loss weight, and the input's Monte Carlo sigma."""
 
     inputs: object
     targets: object
     sigma: object
     density: object
     weight: object
+    noise: object  # the input's Monte Carlo sigma, on the input's scale
 
     def __len__(self) -> int:
         return int(self.inputs.shape[0])
 
     def subset(self, idx) -> "PairSet":
-        return PairSet(*(t[idx] for t in (self.inputs, self.targets, self.sigma, self.density,
-                                          self.weight)))
+        return PairSet(*(getattr(self, f)[idx] for f in PAIR_FIELDS))
+
+
+PAIR_FIELDS = ("inputs", "targets", "sigma", "density", "weight", "noise")
 
 
 def make_pairs(grid, cross_sections, source, *, n_low, n_high: int, n_batches: int,
@@ -163,7 +166,7 @@ def make_pairs(grid, cross_sections, source, *, n_low, n_high: int, n_batches: i
     sets = []
     for k, n in enumerate(np.atleast_1d(n_low)):
         lo = engine.run_dij_device(source, int(n), n_batches, seed + 31 * k, truncation=0.0)
-        lo_dose, lo_max, _ = dense_columns(lo, device)
+        lo_dose, lo_max, lo_sigma = dense_columns(lo, device, with_sigma=True)
         n_cols = lo.n_beamlets
         z0 = rng.integers(0, max(shape[2] - window[2], 0) + 1, size=n_cols)
         origins = lateral_origins(hi_dose, shape, window, z0)
@@ -172,8 +175,9 @@ def make_pairs(grid, cross_sections, source, *, n_low, n_high: int, n_batches: i
         t = gather(hi_dose, shape, origins, window) * scale
         s = gather(hi_sigma, shape, origins, window) * scale
         d = gather(rho, shape, origins, window, shared=True)
-        sets.append(PairSet(x, t, s, d, loss_weight(t, s, precision)))
-        del lo_dose
+        e = gather(lo_sigma, shape, origins, window) * scale
+        sets.append(PairSet(x, t, s, d, loss_weight(t, s, precision), e))
+        del lo_dose, lo_sigma
     del hi_dose, hi_sigma
     engine.drop_uploads()
     return concat(sets)
@@ -181,8 +185,7 @@ def make_pairs(grid, cross_sections, source, *, n_low, n_high: int, n_batches: i
 
 def concat(sets: list[PairSet]) -> PairSet:
     torch = _torch()
-    return PairSet(*(torch.cat([getattr(p, f) for p in sets]) for f in
-                     ("inputs", "targets", "sigma", "density", "weight")))
+    return PairSet(*(torch.cat([getattr(p, f) for p in sets]) for f in PAIR_FIELDS))
 
 
 def train(net: UNet3D, pairs: PairSet, *, steps: int, batch: int = 4, seed: int = 0,
@@ -200,7 +203,8 @@ def train(net: UNet3D, pairs: PairSet, *, steps: int, batch: int = 4, seed: int 
             net.lr = lr0 * (lr_final / lr0) ** (step / max(steps - 1, 1))
         idx = torch.randint(0, n, (batch,), generator=g).to(net.device)
         acc += net.train_step(pairs.inputs[idx].contiguous(), pairs.density[idx].contiguous(),
-                              pairs.targets[idx].contiguous(), pairs.weight[idx].contiguous())[0]
+                              pairs.targets[idx].contiguous(), pairs.weight[idx].contiguous(),
+                              pairs.noise[idx].contiguous())[0]
         if (step + 1) % log_every == 0:
             history.append(float(acc.item()) / log_every)
             acc.zero_()
@@ -220,15 +224,17 @@ def inference_window(grid_shape, lateral: int = 64) -> tuple[int, int, int]:
     return wx, wy, -(-nz // 8) * 8
 
 
-def denoise_dense(net: UNet3D, dose, colmax, density, grid_shape, *, window=None,
-                  chunk: int = 16):
+def denoise_dense(net: UNet3D, dose, colmax, density, grid_shape, *, sigma=None, window=None,
+                  chunk: int = 16, out=None):
     """Denoised dense columns, float64 [C, vox]: the Monte Carlo columns
-    (float32 dose [C, vox] with their maxima) with every column's window
-    replaced by the network's estimate.  `density` is the shared [vox] volume."""
+    (float32 dose [C, vox] with their maxima and, optionally, their sigma; or
+    `out`, float64, written in place) with every column's window replaced by
+    the network's estimate.  `density` is the shared [vox] volume."""
     torch = _torch()
     window = window or inference_window(grid_shape)
     origins = lateral_origins(dose, grid_shape, window)
-    out = dose.to(torch.float64)
+    if out is None:
+        out = dose.to(torch.float64)
     n = dose.shape[0]
     for c0 in range(0, n, chunk):
         c1 = min(c0 + chunk, n)
@@ -236,8 +242,9 @@ def denoise_dense(net: UNet3D, dose, colmax, density, grid_shape, *, window=None
         org = origins[idx].contiguous()
         x = gather(dose[idx].contiguous(), grid_shape, org, window)
         rho = gather(density, grid_shape, org, window, shared=True)
+        sg = None if sigma is None else gather(sigma[idx].contiguous(), grid_shape, org, window)
         cm = colmax[idx].contiguous()
-        y = net.predict(x, rho, colmax=cm)
+        y = net.predict(x, rho, colmax=cm, sigma=sg)
         scatter(y[: c1 - c0], cm[: c1 - c0], grid_shape, org[: c1 - c0].contiguous(),
                 out[c0:c1])
     return out
@@ -268,6 +275,45 @@ def compact(mean, sigma, truncation: float):
     indptr = np.zeros(n_cols + 1, dtype=np.int64)
     np.cumsum(counts.cpu().numpy(), out=indptr[1:])
     return indptr, idx[:k].cpu().numpy(), dose[:k].cpu().numpy(), sig[:k].cpu().numpy()
+
+
+def run_dij_denoised(engine, net: UNet3D | None, source, n_histories_per_beamlet, n_batches: int,
+                     seed: int, *, truncation: float = 1.0e-3, lateral: int = 64, chunk: int = 16):
+    """A Dij from low-history Monte Carlo plus the denoiser: the engine runs the
+    beamlets (``run_dij_device``), every column's window around its beamlet is
+    replaced by the network's estimate, and the dense columns are truncated and
+    compacted to CSC on the device.  The per-entry sigma is the Monte Carlo
+    sigma of the input run.  With ``net`` None this is plain Monte Carlo
+    (``engine.run_dij``), the method's fallback."""
+    import torch
+
+    from .engine import ENERGY_QUANTUM_MEV, _result_types
+
+    if net is None:
+        return engine.run_dij(source, n_histories_per_beamlet, n_batches, seed,
+                              truncation=truncation)
+    view = engine.run_dij_device(source, n_histories_per_beamlet, n_batches, seed, truncation=0.0)
+    device = torch.device(view.device)
+    shape = tuple(view.grid_shape)
+    dose, colmax, sigma32 = dense_columns(view, device, with_sigma=True)
+    mean, sigma = dense_columns_f64(view, device)
+    rho = torch.from_numpy(np.ascontiguousarray(engine.grid.density, dtype=np.float32).ravel()).to(device)
+    denoise_dense(net, dose, colmax, rho, shape, sigma=sigma32,
+                  window=inference_window(shape, lateral), chunk=chunk, out=mean)
+    del dose, sigma32
+    indptr, indices, dose_v, sigma_v = compact(mean, sigma, truncation)
+    deposited, escaped, unscored, emitted = view.books
+    counts = np.asarray(view.counts)
+    _, _, DijResult = _result_types()
+    return DijResult(
+        grid_shape=shape, n_beamlets=view.n_beamlets,
+        n_histories_per_beamlet=int(counts.max()), n_batches=n_batches, truncation=truncation,
+        indptr=indptr, indices=indices, dose=dose_v, sigma=sigma_v,
+        energy_emitted=float(emitted) * ENERGY_QUANTUM_MEV,
+        energy_deposited=float(deposited) * ENERGY_QUANTUM_MEV,
+        energy_escaped=float(escaped) * ENERGY_QUANTUM_MEV,
+        energy_unscored=float(unscored) * ENERGY_QUANTUM_MEV,
+        correlated=True)
 
 
 # ---- error against high-statistics Monte Carlo ------------------------------------------

@@ -1,8 +1,9 @@
 """3D U-Net denoiser of Dij columns, trained and run on the project's own kernels.
 
 No counterpart in pyRadMC (the reference has no learned component).  The network
-maps a low-history dose column, normalized by its maximum, plus the density to
-an estimate of the high-history column; plain Monte Carlo stays its fallback and
+maps a low-history dose column and its Monte Carlo sigma, both normalized by
+the column's maximum, plus the density to an estimate of the high-history
+column; plain Monte Carlo stays its fallback and
 the judge of its error.
 
 Architecture: four levels of 16-32-64-128 channels.  Each level is two 3x3x3
@@ -29,7 +30,7 @@ import numpy as np
 
 from . import _lib
 
-IN_CHANNELS = 8          # dose, density, six zero channels (16-byte voxel rows)
+IN_CHANNELS = 8          # dose, density, MC sigma, five zero channels (16-byte voxel rows)
 LEVELS = (16, 32, 64, 128)
 ALIGN = 64               # parameter blocks start on 64-element boundaries
 
@@ -285,12 +286,15 @@ class UNet3D:
         self.launches += 1
 
     # ---- passes ---------------------------------------------------------------------
-    def pack(self, ws: _Workspace, dose, density, colmax=None, density_shared: bool = False) -> None:
-        """Network input from float32 device tensors: dose [B, D, H, W] (scaled by
-        1 / colmax[b] when colmax is given) and density ([D, H, W] shared by the
-        batch when density_shared, else [B, D, H, W])."""
+    def pack(self, ws: _Workspace, dose, density, colmax=None, density_shared: bool = False,
+             sigma=None) -> None:
+        """Network input from float32 device tensors: dose [B, D, H, W] and its
+        Monte Carlo sigma (optional; both scaled by 1 / colmax[b] when colmax is
+        given) and density ([D, H, W] shared by the batch when density_shared,
+        else [B, D, H, W])."""
         vox = ws.m // ws.shape[0]
         _check(self.lib.pmd_pack_input(dose.data_ptr(), density.data_ptr(),
+                                       None if sigma is None else sigma.data_ptr(),
                                        None if colmax is None else colmax.data_ptr(), vox,
                                        int(density_shared), ws.x0.data_ptr(), ws.base.data_ptr(),
                                        ws.m, self._stream()), "pack input")
@@ -385,30 +389,30 @@ class UNet3D:
         self.launches += 1
 
     # ---- public ---------------------------------------------------------------------
-    def gradients(self, dose, density, target, weight=None):
+    def gradients(self, dose, density, target, weight=None, sigma=None):
         """Loss and flat parameter gradient (device tensors) for one batch,
         without updating the parameters."""
         ws = self.workspace(tuple(dose.shape))
         self.grad.zero_()
         ws.loss.zero_()
-        self.pack(ws, dose, density)
+        self.pack(ws, dose, density, sigma=sigma)
         self.forward(ws)
         self.loss(ws, target, weight)
         self.backward(ws)
         return ws.loss, self.grad
 
-    def train_step(self, dose, density, target, weight=None):
+    def train_step(self, dose, density, target, weight=None, sigma=None):
         """One Adam step on a batch; returns the batch loss (device scalar,
         before the step)."""
-        loss, _ = self.gradients(dose, density, target, weight)
+        loss, _ = self.gradients(dose, density, target, weight, sigma)
         self.adam()
         return loss
 
-    def predict(self, dose, density, colmax=None, density_shared: bool = False):
+    def predict(self, dose, density, colmax=None, density_shared: bool = False, sigma=None):
         """Denoised, normalized dose [B, D, H, W] (a view of the workspace,
         overwritten by the next call of the same shape)."""
         ws = self.workspace(tuple(dose.shape))
-        self.pack(ws, dose, density, colmax, density_shared)
+        self.pack(ws, dose, density, colmax, density_shared, sigma)
         self.forward(ws)
         return ws.out.view(dose.shape)
 

@@ -3,8 +3,9 @@
 ``python -m pyradmc_b200.train_denoiser --out weights.npz`` builds the training
 set of the denoiser workload: seeded CT-like phantoms (128^3 at 2.5 mm, water
 plus 6-12 random ellipsoids), a 10x10 lattice of 5x5 mm 6 MV beamlets on each,
-every column run at ``--n-low`` and ``--n-high`` histories per beamlet, cropped
-to 64^3 windows around the beamlet; then trains the U-Net with Adam on the
+every column run at each ``--n-low`` count and at ``--n-high`` histories per
+beamlet, cropped to 64^3 windows around the beamlet (input: the low-history
+dose and its Monte Carlo sigma, plus the density); then trains the U-Net with Adam on the
 device (the project's own forward and backward kernels) and evaluates it on a
 held-out phantom against high-statistics Monte Carlo.  One JSON line with the
 loss curve and the evaluation goes to stdout.
@@ -63,15 +64,15 @@ def evaluate(net: UNet3D, n_levels, n_ref: int, n_batches: int, device: str, lat
     out = {"n_ref": n_ref, "levels": []}
     for n in n_levels:
         run = engine.run_dij_device(fan, int(n), n_batches, 7 + int(n), truncation=0.0)
-        dose, colmax, _ = D.dense_columns(run, device)
+        dose, colmax, sg = D.dense_columns(run, device, with_sigma=True)
         plain = D.sigma_equivalent_error(dose, ref_dose, ref_sigma)
         level = {"n_per_beamlet": int(n), "plain": float(np.nanmean(plain))}
         for lateral in laterals:
             window = D.inference_window(shape, lateral)
-            D.denoise_dense(net, dose, colmax, rho, shape, window=window)  # warm-up
+            D.denoise_dense(net, dose, colmax, rho, shape, sigma=sg, window=window)  # warm-up
             torch.cuda.synchronize()
             t0 = time.perf_counter()
-            den = D.denoise_dense(net, dose, colmax, rho, shape, window=window)
+            den = D.denoise_dense(net, dose, colmax, rho, shape, sigma=sg, window=window)
             torch.cuda.synchronize()
             t_den = time.perf_counter() - t0
             denoised = D.sigma_equivalent_error(den, ref_dose, ref_sigma)
@@ -79,7 +80,7 @@ def evaluate(net: UNet3D, n_levels, n_ref: int, n_batches: int, device: str, lat
             level[f"denoise_s_w{lateral}"] = t_den
             del den
         out["levels"].append(level)
-        del dose
+        del dose, sg
     return out
 
 
@@ -88,18 +89,19 @@ def main(argv=None) -> int:
     ap.add_argument("--out", required=True, help="weights file (.npz)")
     ap.add_argument("--device", default="cuda:0")
     ap.add_argument("--phantoms", type=int, default=40)
-    ap.add_argument("--n-low", default="10000", help="comma-separated input history counts")
+    ap.add_argument("--n-low", default="10000,30000,100000",
+                    help="comma-separated input history counts")
     ap.add_argument("--n-high", type=int, default=1_000_000)
     ap.add_argument("--n-batches", type=int, default=10)
-    ap.add_argument("--steps", type=int, default=6000)
+    ap.add_argument("--steps", type=int, default=16000)
     ap.add_argument("--batch", type=int, default=4)
     ap.add_argument("--lr", type=float, default=1.0e-3)
     ap.add_argument("--lr-final", type=float, default=1.0e-4)
     ap.add_argument("--loss-lambda", type=float, default=50.0)
     ap.add_argument("--init", default=None, help="start from these weights")
-    ap.add_argument("--eval-levels", default="10000,30000,100000")
+    ap.add_argument("--eval-levels", default="10000,30000,100000,300000")
     ap.add_argument("--n-ref", type=int, default=4_000_000)
-    ap.add_argument("--eval-lateral", default="32,64")
+    ap.add_argument("--eval-lateral", default="64")
     args = ap.parse_args(argv)
 
     def log(msg):

@@ -195,14 +195,16 @@ def test_unet_gradients_match_oracle(gpu):
         sl = slice(l.w_off, l.w_off + l.cout * l.kpad)
         params[sl] = bf16(params[sl])
     noisy, density, clean, weight = _batch(rng, 2, 16)
+    sigma = bf16(0.3 * clean)  # the Monte Carlo sigma channel
     net = UNet3D(gpu, params=params, loss_lambda=0.5)
     loss, grad = net.gradients(_dev(noisy, torch.float32), _dev(density, torch.float32),
-                               _dev(clean, torch.float32), _dev(weight, torch.float32))
+                               _dev(clean, torch.float32), _dev(weight, torch.float32),
+                               _dev(sigma, torch.float32))
     torch.cuda.synchronize()
     got = grad.cpu().numpy()
     ref_loss, ref = OracleUNet(params).gradients(torch.from_numpy(noisy), torch.from_numpy(density),
                                                  torch.from_numpy(clean), torch.from_numpy(weight),
-                                                 0.5)
+                                                 0.5, torch.from_numpy(sigma))
     assert abs(float(loss.item()) - ref_loss) <= 0.02 * ref_loss
     for l in layers:
         for off, size in ((l.w_off, l.cout * l.kpad), (l.b_off, l.cout)):
