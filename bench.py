@@ -162,26 +162,30 @@ def barrier(world):
         dist.barrier()
 
 
-def all_max(world, values):
+def _reduce(world, values, op):
     if world == 1:
         return list(values)
     import torch
     import torch.distributed as dist
 
-    t = torch.tensor(values, dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    device = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor(values, dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=getattr(dist.ReduceOp, op))
     return t.tolist()
+
+
+def all_max(world, values):
+    return _reduce(world, values, "MAX")
 
 
 def all_sum(world, values):
-    if world == 1:
-        return list(values)
-    import torch
-    import torch.distributed as dist
+    return _reduce(world, values, "SUM")
 
-    t = torch.tensor(values, dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.SUM)
-    return t.tolist()
+
+def weak_scaling_value(world: int, histories_per_rank: int, steps: int, max_total_ms: float) -> float:
+    """Whole-job histories/s: every rank ran `steps` Dijs of its own; the job
+    takes as long as its slowest rank."""
+    return world * histories_per_rank * steps / (max_total_ms / 1e3)
 
 
 # ---- the CPU baseline -----------------------------------------------------------------
@@ -378,6 +382,11 @@ def b200_arm(args, world, rank, local):
     torch.cuda.set_device(local)
     grid, xs, source, counts = workload(rank)
     engine = B200Engine(grid, xs, device=device, use_graph=not args.no_graph)
+    tune_report = None
+    if not args.no_autotune:
+        from pyradmc_b200 import autotune
+
+        engine, tune_report = autotune.tune(engine, source, counts, N_BATCHES, SEED, repeats=1)
     stream = torch.cuda.Stream(device=device)  # an explicit stream: the legacy default is 0
     torch.cuda.set_stream(stream)
     engine.use_stream(stream.cuda_stream)
@@ -409,7 +418,7 @@ def b200_arm(args, world, rank, local):
         torch.cuda.synchronize()
         barrier(world)
     total_ms = all_max(world, [sum(step_ms)])[0]
-    value = world * histories * args.steps / (total_ms / 1e3)
+    value = weak_scaling_value(world, histories, args.steps, total_ms)
 
     # end to end from host data: uploads and readback inside the timed region
     e2e_ms, h2d, d2h = [], [], []
@@ -429,7 +438,7 @@ def b200_arm(args, world, rank, local):
     torch.cuda.synchronize()
     barrier(world)
     e2e_total = all_max(world, [sum(e2e_ms)])[0]
-    e2e_value = world * histories * args.steps / (e2e_total / 1e3)
+    e2e_value = weak_scaling_value(world, histories, args.steps, e2e_total)
 
     c = counters[-1]
     sigma_pre = phantoms.per_beamlet_sigma(dij)
@@ -464,7 +473,11 @@ def b200_arm(args, world, rank, local):
         "vs_baseline": None,
         "dtype": "f32 transport, int64 scoring, f64 statistics",
         "data": "synthetic (seeded phantom and beamlet counts)",
-        "config": config_dict(counts, "256 MB buffer written between timed steps (flush)"),
+        "config": {**config_dict(counts, "256 MB buffer written between timed steps (flush)"),
+                   "launch": {"block_size": engine.block_size, "blocks_per_sm": engine.blocks_per_sm,
+                              "chunk_size": engine.chunk_size,
+                              "autotuned": tune_report is not None,
+                              "tune_cached": None if tune_report is None else tune_report["cached"]}},
         "s_per_dij": s_per_dij,
         "per_beamlet_sigma": sigma,
         "s_per_dij_at_2pct_sigma": s_at_2pct,
@@ -510,6 +523,8 @@ def main() -> int:
                     help="skip the CPU baseline leg (profiling runs)")
     ap.add_argument("--no-denoiser", action="store_true",
                     help="skip the MC + denoiser leg (profiling runs)")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="default launch shape instead of the autotuned one")
     args = ap.parse_args()
     global WORKLOAD
     WORKLOAD = args.workload

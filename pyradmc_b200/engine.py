@@ -23,7 +23,8 @@ import numpy as np
 
 from pyradmc_b200 import _lib, model
 
-__all__ = ["B200Engine", "DIJ_TRUNCATION_RELATIVE", "DeviceDij", "ECUT_MEV", "PCUT_MEV"]
+__all__ = ["B200Engine", "DIJ_TRUNCATION_RELATIVE", "DeviceDij", "ECUT_MEV", "PCUT_MEV",
+           "column_shards", "merge_shards"]
 
 ECUT_MEV = 0.200  # pyradmc/__init__.py:22
 PCUT_MEV = 0.050  # pyradmc/__init__.py:25
@@ -162,6 +163,60 @@ class DeviceDij:
     counts: np.ndarray | None = None
     n_batches: int = 0
     device: str = "cuda:0"
+
+
+def column_shards(counts, world: int) -> list[tuple[int, int]]:
+    """Contiguous Dij column ranges, one per rank, with near-equal history totals
+    (some empty when there are more ranks than columns)."""
+    c = np.asarray(counts, dtype=np.int64)
+    if world < 1:
+        raise ValueError(f"need at least one rank, got {world}")
+    cum = np.cumsum(c)
+    total = int(cum[-1]) if c.size else 0
+    bounds = [0]
+    for r in range(1, world):
+        target = total * r / world
+        j = int(np.searchsorted(cum, target))  # first column whose running total reaches target
+        if j < c.size and j > 0 and abs(cum[j - 1] - target) <= abs(cum[j] - target):
+            j -= 1
+        bounds.append(min(max(bounds[-1], j + 1), c.size))
+    bounds.append(int(c.size))
+    return list(zip(bounds[:-1], bounds[1:]))
+
+
+def merge_shards(parts):
+    """One Dij from ``(DijResult, (first, stop))`` shards that cover every column
+    once (in any order): the CSC concatenated in column order, energies summed."""
+    parts = sorted(parts, key=lambda p: p[1][0])
+    if not parts:
+        raise ValueError("no shards to merge")
+    expect = 0
+    for _, (a, b) in parts:
+        if a != expect or b < a:
+            raise ValueError(f"shards do not tile the columns: expected {expect}, got ({a}, {b})")
+        expect = b
+    first = parts[0][0]
+    indptr = [np.zeros(1, dtype=np.int64)]
+    base = 0
+    for dij, _ in parts:
+        indptr.append(np.asarray(dij.indptr[1:], dtype=np.int64) + base)
+        base += int(dij.indptr[-1])
+    _, _, DijResult = _result_types()
+    real = [d for d, (a, b) in parts if b > a]
+    return DijResult(
+        grid_shape=first.grid_shape, n_beamlets=expect,
+        n_histories_per_beamlet=max(int(d.n_histories_per_beamlet) for d in real),
+        n_batches=first.n_batches, truncation=first.truncation,
+        indptr=np.concatenate(indptr),
+        indices=np.concatenate([np.asarray(d.indices, dtype=np.int64) for d, _ in parts]),
+        dose=np.concatenate([np.asarray(d.dose) for d, _ in parts]),
+        sigma=np.concatenate([np.asarray(d.sigma) for d, _ in parts]),
+        energy_emitted=sum(float(d.energy_emitted) for d in real),
+        energy_deposited=sum(float(d.energy_deposited) for d in real),
+        energy_escaped=sum(float(d.energy_escaped) for d in real),
+        energy_unscored=sum(float(d.energy_unscored) for d in real),
+        correlated=first.correlated, scoring_mode=first.scoring_mode,
+        provenance=first.provenance)
 
 
 def _device_dij(native: "_Native", n_cols: int, nnz: int, books) -> DeviceDij:
@@ -577,6 +632,23 @@ class B200Engine:
             deposit_resolution_cm=deposit_resolution_cm, msc_model=msc_model, devices=devices,
             concurrent_batches=concurrent_batches, progress=progress, device_view=False)
 
+    def run_dij_shard(self, source, n_histories_per_beamlet, n_batches: int, seed: int, *,
+                      rank: int, world: int, **kwargs):
+        """This rank's share of a Dij computed by `world` processes (one GPU
+        each): ``(DijResult of columns first..stop-1, (first, stop))`` from
+        :func:`column_shards`.  Beamlets keep their global history numbers, so
+        the shards are bit-identical to the same columns of the whole Dij and
+        :func:`merge_shards` rebuilds it; no data-path collective is needed."""
+        n = int(source.n_beamlets)
+        counts = (np.full(n, int(n_histories_per_beamlet), dtype=np.int64)
+                  if np.ndim(n_histories_per_beamlet) == 0
+                  else np.asarray(n_histories_per_beamlet, dtype=np.int64))
+        if not 0 <= rank < world:
+            raise ValueError(f"rank {rank} outside a world of {world}")
+        span = column_shards(counts, world)[rank]
+        dij = self._run_dij(source, counts, n_batches, seed, columns=span, **kwargs)
+        return dij, span
+
     def run_dij_device(self, source, n_histories_per_beamlet, n_batches: int, seed: int,
                        **kwargs) -> "DeviceDij":
         """``run_dij`` on this engine's device, leaving the CSC there.
@@ -614,6 +686,7 @@ class B200Engine:
         concurrent_batches: int = 1,
         progress=None,
         device_view: bool = False,
+        columns: tuple[int, int] | None = None,
     ):
         n_beamlets = int(source.n_beamlets)
         if np.ndim(n_histories_per_beamlet) == 0:
@@ -650,11 +723,16 @@ class B200Engine:
         name = _type_name(source)
         offsets = np.zeros(n_beamlets, dtype=np.int64)
         np.cumsum(counts[:-1], out=offsets[1:])
+        col_lo, col_hi = (0, n_beamlets) if columns is None else (int(columns[0]), int(columns[1]))
+        if not 0 <= col_lo <= col_hi <= n_beamlets:
+            raise ValueError(f"column range {columns} outside 0..{n_beamlets}")
+        if columns is not None and len(device_list) > 1:
+            raise ValueError("a column range runs on one device")
         if name == "BeamletGridSource":
             bounds = np.array([source.beamlet_bounds(j) for j in range(n_beamlets)], dtype=np.float64)
             per = dict(x_lo=bounds[:, 0], x_extent=bounds[:, 1] - bounds[:, 0],
                        y_lo=bounds[:, 2], y_extent=bounds[:, 3] - bounds[:, 2])
-            energy_emitted = float(np.sum(counts)) * source.max_energy
+            energy_emitted = float(np.sum(counts[col_lo:col_hi])) * source.max_energy
         elif name == "SpectralBeamletSource":
             per = dict(centers=np.asarray(source.centers, dtype=np.float64).reshape(n_beamlets, 3))
             energy_emitted = None
@@ -670,8 +748,10 @@ class B200Engine:
         )
         emitter = _progress_emitter(progress, int(np.sum(counts)))
         group = beamlet_group_size or n_beamlets
-        group_starts = list(range(0, n_beamlets, group)) if len(device_list) > 1 else [0]
-        span = group if len(device_list) > 1 else n_beamlets
+        group_starts = list(range(0, n_beamlets, group)) if len(device_list) > 1 else [col_lo]
+        span = group if len(device_list) > 1 else col_hi - col_lo
+        if col_hi == col_lo:
+            group_starts = []
         pending = deque(group_starts)
         pending_lock = threading.Lock()
 
@@ -686,7 +766,7 @@ class B200Engine:
             totals = np.zeros(4, dtype=np.int64)
             tick = _lib.PROGRESS_FN(lambda _u, n: emitter.tick(int(n)))
             while (g0 := next_group()) is not None:
-                g1 = min(g0 + span, n_beamlets)
+                g1 = min(g0 + span, col_hi)
                 sl = slice(g0, g1)
                 desc = _lib.BeamletDesc(n_beamlets=g1 - g0)
                 keep = []
@@ -766,12 +846,17 @@ class B200Engine:
             idx_all.append(i)
             dose_all.append(d)
             sig_all.append(s)
-        col_counts = np.concatenate(counts_all)
-        indptr = np.zeros(n_beamlets + 1, dtype=np.int64)
+        n_out = col_hi - col_lo
+        col_counts = np.concatenate(counts_all) if counts_all else np.zeros(0, dtype=np.int64)
+        indptr = np.zeros(n_out + 1, dtype=np.int64)
         np.cumsum(col_counts, out=indptr[1:])
 
-        def joined(parts):  # one block (one device) needs no copy
+        def joined(parts, dtype=np.float64):  # one block (one device) needs no copy
+            if not parts:
+                return np.zeros(0, dtype=dtype)
             return parts[0] if len(parts) == 1 else np.concatenate(parts)
+
+        counts = counts[col_lo:col_hi] if n_out else counts[:1]
 
         if energy_emitted is None:
             energy_emitted = float(totals[3]) * ENERGY_QUANTUM_MEV
@@ -780,12 +865,12 @@ class B200Engine:
         equal = bool(np.all(counts == counts[0]))
         return DijResult(
             grid_shape=shape,
-            n_beamlets=n_beamlets,
+            n_beamlets=n_out,
             n_histories_per_beamlet=int(counts[0]) if equal else int(counts.max()),
             n_batches=n_batches,
             truncation=truncation,
             indptr=indptr,
-            indices=joined(idx_all),
+            indices=joined(idx_all, np.int64),
             dose=joined(dose_all),
             sigma=joined(sig_all),
             energy_emitted=energy_emitted,
