@@ -288,6 +288,7 @@ def denoiser_leg(args, engine, source, counts, stream, device, plain_s_at_2pct):
 
     if not DENOISER_WEIGHTS.exists():
         return {"unavailable": f"no trained weights at {DENOISER_WEIGHTS.relative_to(ROOT)}"}
+    torch.cuda.empty_cache()  # the engine allocates outside torch's cache
     net = UNet3D.load(DENOISER_WEIGHTS, device=device)
     shape = tuple(engine.grid.shape)
     window = D.inference_window(shape, 64)

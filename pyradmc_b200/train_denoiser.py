@@ -36,6 +36,8 @@ def phantom(seed: int):
 
 
 def build_pairs(n_phantoms: int, n_low, n_high: int, n_batches: int, device: str, log):
+    import torch
+
     sets = []
     for i in range(n_phantoms):
         t0 = time.perf_counter()
@@ -43,6 +45,7 @@ def build_pairs(n_phantoms: int, n_low, n_high: int, n_batches: int, device: str
         sets.append(D.make_pairs(grid, xs, fan, n_low=n_low, n_high=n_high, n_batches=n_batches,
                                  seed=20260726 + 101 * i, device=device,
                                  rng=np.random.default_rng(i)))
+        torch.cuda.empty_cache()
         log(f"phantom {i}: {len(sets[-1])} pairs in {time.perf_counter() - t0:.1f} s")
     return D.concat(sets)
 
@@ -99,6 +102,8 @@ def main(argv=None) -> int:
     ap.add_argument("--lr-final", type=float, default=1.0e-4)
     ap.add_argument("--loss-lambda", type=float, default=50.0)
     ap.add_argument("--init", default=None, help="start from these weights")
+    ap.add_argument("--eval-only", action="store_true",
+                    help="evaluate the --init weights without training")
     ap.add_argument("--eval-levels", default="10000,30000,100000,300000")
     ap.add_argument("--n-ref", type=int, default=4_000_000)
     ap.add_argument("--eval-lateral", default="64")
@@ -107,22 +112,27 @@ def main(argv=None) -> int:
     def log(msg):
         print(msg, file=sys.stderr, flush=True)
 
-    t0 = time.perf_counter()
+    import torch
+
     n_low = [int(v) for v in args.n_low.split(",") if v]
-    pairs = build_pairs(args.phantoms, n_low, args.n_high, args.n_batches, args.device, log)
-    n_pairs = len(pairs)
-    t_data = time.perf_counter() - t0
+    n_pairs, t_data, t_train, history = 0, 0.0, 0.0, []
     if args.init:
         net = UNet3D.load(args.init, device=args.device, lr=args.lr, loss_lambda=args.loss_lambda)
     else:
         net = UNet3D(args.device, seed=0, lr=args.lr, loss_lambda=args.loss_lambda)
-    t0 = time.perf_counter()
-    history = D.train(net, pairs, steps=args.steps, batch=args.batch, lr_final=args.lr_final,
-                      log_every=max(args.steps // 40, 1), log=log)
-    t_train = time.perf_counter() - t0
-    net.save(args.out)
-    del pairs
+    if not args.eval_only:
+        t0 = time.perf_counter()
+        pairs = build_pairs(args.phantoms, n_low, args.n_high, args.n_batches, args.device, log)
+        n_pairs = len(pairs)
+        t_data = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        history = D.train(net, pairs, steps=args.steps, batch=args.batch, lr_final=args.lr_final,
+                          log_every=max(args.steps // 40, 1), log=log)
+        t_train = time.perf_counter() - t0
+        net.save(args.out)
+        del pairs
     net.release_workspaces()
+    torch.cuda.empty_cache()  # the engine allocates outside torch's cache
     levels = [int(v) for v in args.eval_levels.split(",") if v]
     laterals = [int(v) for v in args.eval_lateral.split(",") if v]
     ev = evaluate(net, levels, args.n_ref, args.n_batches, args.device, laterals)
