@@ -387,7 +387,10 @@ def b200_arm(args, world, rank, local):
     if not args.no_autotune:
         from pyradmc_b200 import autotune
 
-        engine, tune_report = autotune.tune(engine, source, counts, N_BATCHES, SEED, repeats=1)
+        # probe the workload itself: shorter probes favour lower residency than
+        # the full Dij wants
+        engine, tune_report = autotune.tune(engine, source, counts, N_BATCHES, SEED,
+                                            fraction=1.0, repeats=1)
     stream = torch.cuda.Stream(device=device)  # an explicit stream: the legacy default is 0
     torch.cuda.set_stream(stream)
     engine.use_stream(stream.cuda_stream)

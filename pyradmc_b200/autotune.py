@@ -41,17 +41,21 @@ _lock = threading.Lock()
 
 @dataclass(frozen=True)
 class LaunchShape:
-    block_size: int
+    """None fields leave the engine's default (256 threads, occupancy-limited
+    residency, 16 primaries per resident thread)."""
+
+    block_size: int | None
     blocks_per_sm: int | None
-    chunk_size: int
+    chunk_size: int | None
 
     def as_dict(self) -> dict:
         return dataclasses.asdict(self)
 
 
 def candidates(sm_count: int) -> list[LaunchShape]:
-    """The tuner's search space on a device with `sm_count` SMs."""
-    out = []
+    """The tuner's search space on a device with `sm_count` SMs; the engine's
+    default shape comes first, so tuning never picks a slower one."""
+    out = [LaunchShape(None, None, None)]
     for bs in BLOCK_SIZES:
         for per_sm in BLOCKS_PER_SM:
             for m in CHUNK_PER_THREAD:

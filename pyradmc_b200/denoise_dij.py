@@ -189,14 +189,18 @@ def concat(sets: list[PairSet]) -> PairSet:
 
 
 def train(net: UNet3D, pairs: PairSet, *, steps: int, batch: int = 4, seed: int = 0,
-          lr_final: float | None = None, log_every: int = 100, log=None) -> list[float]:
+          lr_final: float | None = None, log_every: int = 100, log=None,
+          keep_best: bool = True) -> list[float]:
     """Adam steps over random mini-batches of the pairs; returns the mean loss of
     every ``log_every`` steps.  With lr_final the learning rate decays
-    geometrically from net.lr to lr_final."""
+    geometrically from net.lr to lr_final.  With keep_best the network ends
+    with the parameters of the interval whose mean loss was lowest (a late
+    divergence cannot lose a good network)."""
     torch = _torch()
     g = torch.Generator(device="cpu").manual_seed(seed)
     lr0 = net.lr
     history, acc = [], torch.zeros((), device=net.device)
+    best, best_params = float("inf"), None
     n = len(pairs)
     for step in range(steps):
         if lr_final is not None:
@@ -208,9 +212,14 @@ def train(net: UNet3D, pairs: PairSet, *, steps: int, batch: int = 4, seed: int 
         if (step + 1) % log_every == 0:
             history.append(float(acc.item()) / log_every)
             acc.zero_()
+            if keep_best and history[-1] < best:
+                best, best_params = history[-1], net.p32.clone()
             if log is not None:
                 log(f"step {step + 1}: loss {history[-1]:.5f} lr {net.lr:.2e}")
     net.lr = lr0
+    if best_params is not None:
+        net.p32.copy_(best_params)
+        net.p16.copy_(best_params.to(net.p16.dtype))
     return history
 
 

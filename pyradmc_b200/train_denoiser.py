@@ -98,8 +98,8 @@ def main(argv=None) -> int:
     ap.add_argument("--n-batches", type=int, default=10)
     ap.add_argument("--steps", type=int, default=16000)
     ap.add_argument("--batch", type=int, default=4)
-    ap.add_argument("--lr", type=float, default=1.0e-3)
-    ap.add_argument("--lr-final", type=float, default=1.0e-4)
+    ap.add_argument("--lr", type=float, default=3.0e-4)
+    ap.add_argument("--lr-final", type=float, default=3.0e-5)
     ap.add_argument("--loss-lambda", type=float, default=50.0)
     ap.add_argument("--init", default=None, help="start from these weights")
     ap.add_argument("--eval-only", action="store_true",

@@ -34,17 +34,20 @@ def _dij(seed=0):
 def _fake_timer(calls):
     def timer(engine, source, counts, n_batches, seed):
         calls.append((engine.block_size, engine.blocks_per_sm, engine.chunk_size, int(counts.sum())))
-        t = abs(engine.block_size - 192) + (0 if engine.blocks_per_sm is None else 5)
-        t += abs(engine.chunk_size - 16 * 148 * 3 * engine.block_size) / 1e6
+        bs = engine.block_size or 256
+        chunk = engine.chunk_size or 16 * 148 * 3 * bs
+        t = abs(bs - 192) + (0 if engine.blocks_per_sm is None else 5)
+        t += abs(chunk - 16 * 148 * 3 * bs) / 1e6
         return 1.0 + t, _dij()
     return timer
 
 
 def test_search_space_covers_every_knob():
     shapes = T.candidates(148)
-    assert len(shapes) == len(T.BLOCK_SIZES) * len(T.BLOCKS_PER_SM) * len(T.CHUNK_PER_THREAD)
-    assert {s.block_size for s in shapes} == set(T.BLOCK_SIZES)
-    assert all(s.chunk_size * 16 < 2 ** 31 for s in shapes)  # queue index range at queue_factor 16
+    assert len(shapes) == 1 + len(T.BLOCK_SIZES) * len(T.BLOCKS_PER_SM) * len(T.CHUNK_PER_THREAD)
+    assert shapes[0] == T.LaunchShape(None, None, None)  # the engine's default competes too
+    assert {s.block_size for s in shapes[1:]} == set(T.BLOCK_SIZES)
+    assert all(s.chunk_size * 16 < 2 ** 31 for s in shapes[1:])  # queue index range at factor 16
 
 
 def test_probe_counts_are_positive_batch_multiples():
@@ -62,6 +65,7 @@ def test_tuner_picks_the_fastest_shape_and_caches_it(tmp_path):
     assert (tuned.block_size, tuned.blocks_per_sm) == (192, None)
     assert tuned.chunk_size == 16 * 148 * 3 * 192
     assert not report["cached"] and len(report["timings"]) == len(T.candidates(148))
+    assert report["timings"][0]["block_size"] is None  # the default was timed
     assert all(c[3] == 100 * 20_000 for c in calls)  # probes run a tenth of the histories
     again, report2 = T.tune(engine, source, np.full(100, 200_000), 10, 1, cache=cache,
                             timer=_fake_timer([]), sm_count=148, device_name="B200")
@@ -75,7 +79,7 @@ def test_tuner_refuses_a_shape_that_changes_the_dij(tmp_path):
     engine = FakeEngine(grid=SimpleNamespace(shape=(8, 8, 8)))
 
     def timer(e, source, counts, n_batches, seed):
-        return 1.0, _dij(seed=1 if e.block_size == 256 else 0)
+        return 1.0, _dij(seed=1 if e.block_size == 192 else 0)
 
     with pytest.raises(RuntimeError, match="scheduling-inert"):
         T.tune(engine, SimpleNamespace(n_beamlets=1), [100], 10, 1, cache=None, timer=timer,
