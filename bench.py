@@ -374,6 +374,51 @@ def denoiser_leg(args, engine, source, counts, stream, device, plain_s_at_2pct):
     }
 
 
+def conv_arm(args, local):
+    """``--workload conv``: the denoiser's dominant convolution (decoder level 0,
+    48 -> 16 channels, one inference chunk of 16 windows of 64 x 64 x 128) on
+    both kernel paths; the case the tensor-memory kernel's ncu captures use."""
+    import torch
+
+    from pyradmc_b200 import _lib
+    from pyradmc_b200.denoiser import kpad_for
+
+    device = f"cuda:{local}"
+    torch.cuda.set_device(local)
+    lib = _lib.load()
+    b, d, h, w, cin, cout = 16, 64, 64, 128, 48, 16
+    stream = torch.cuda.Stream(device=device)
+    torch.cuda.set_stream(stream)
+    gen = torch.Generator(device=device).manual_seed(SEED)
+    x = torch.randn((b, d, h, w, cin), device=device, generator=gen).to(torch.bfloat16)
+    wt = (0.05 * torch.randn((cout, kpad_for(cin)), device=device, generator=gen)).to(torch.bfloat16)
+    y = torch.empty((b, d, h, w, cout), device=device, dtype=torch.bfloat16)
+    flops = 2.0 * b * d * h * w * 27 * cin * cout
+    peaks_path = ROOT / "MEASURED_PEAKS.json"
+    peaks = json.loads(peaks_path.read_text()) if peaks_path.exists() else {}
+    peak = float(peaks.get("bf16_tflops", 1590.0))
+    out = {"workload": "conv3d 48->16, 16 x 64 x 64 x 128 voxels, bf16/fp32", "flops": flops}
+    previous = lib.pmd_conv3d_impl(-1)
+    for name, impl in (("tensor_memory", 2), ("mma_sync", 1)):
+        lib.pmd_conv3d_impl(impl)
+        for _ in range(args.warmup):
+            assert lib.pmd_conv3d(x.data_ptr(), wt.data_ptr(), None, y.data_ptr(), b, d, h, w, cin,
+                                  cout, kpad_for(cin), 1, stream.cuda_stream) == 0
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            lib.pmd_conv3d(x.data_ptr(), wt.data_ptr(), None, y.data_ptr(), b, d, h, w, cin, cout,
+                           kpad_for(cin), 1, stream.cuda_stream)
+        e1.record(stream)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1) / args.steps
+        out[name] = {"ms": ms, "tflops": flops / ms / 1e9, "frac_of_measured_bf16": flops / ms / 1e9 / peak}
+    lib.pmd_conv3d_impl(previous)
+    out["failures"] = lib.pmd_conv3d_failures()
+    print(json.dumps(out), flush=True)
+    return 0
+
+
 def b200_arm(args, world, rank, local):
     import torch
 
@@ -518,8 +563,9 @@ def main() -> int:
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("b200", "reference"), default="b200")
-    ap.add_argument("--workload", choices=("dij100", "dij10"), default="dij100",
-                    help="dij10: the reduced case used for ncu captures")
+    ap.add_argument("--workload", choices=("dij100", "dij10", "conv"), default="dij100",
+                    help="dij10: the reduced transport case of the ncu captures; conv: the "
+                         "denoiser's dominant convolution alone")
     ap.add_argument("--no-graph", action="store_true",
                     help="drain batches with the host loop instead of the CUDA graph (bit-identical; "
                          "ncu cannot profile kernels inside graphs with conditional nodes)")
@@ -536,6 +582,8 @@ def main() -> int:
     try:
         if args.impl == "reference":
             return reference_arm(args, world, rank)
+        if args.workload == "conv":
+            return conv_arm(args, local)
         return b200_arm(args, world, rank, local)
     finally:
         if world > 1:
