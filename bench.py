@@ -414,6 +414,27 @@ def conv_arm(args, local):
         ms = e0.elapsed_time(e1) / args.steps
         out[name] = {"ms": ms, "tflops": flops / ms / 1e9, "frac_of_measured_bf16": flops / ms / 1e9 / peak}
     lib.pmd_conv3d_impl(previous)
+
+    # one inference chunk of the whole network (16 windows, the committed weights)
+    from pyradmc_b200.denoiser import UNet3D, forward_flops_per_voxel
+
+    net = UNet3D.load(DENOISER_WEIGHTS, device=device)
+    dose = torch.rand((b, d, h, w), device=device, generator=gen)
+    rho = torch.ones((b, d, h, w), device=device)
+    for _ in range(args.warmup):
+        net.predict(dose, rho, sigma=0.1 * dose)
+    sg = 0.1 * dose
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    launches = net.launches
+    e0.record(stream)
+    for _ in range(args.steps):
+        net.predict(dose, rho, sigma=sg)
+    e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    flops_net = forward_flops_per_voxel() * b * d * h * w
+    out["unet_chunk"] = {"ms": ms, "tflops": flops_net / ms / 1e9,
+                         "launches": (net.launches - launches) / args.steps}
     out["failures"] = lib.pmd_conv3d_failures()
     print(json.dumps(out), flush=True)
     return 0
