@@ -184,8 +184,15 @@ def make_pairs(grid, cross_sections, source, *, n_low, n_high: int, n_batches: i
 
 
 def concat(sets: list[PairSet]) -> PairSet:
+    """One PairSet from many, field by field, releasing each field of the parts
+    as soon as it is joined (peak memory: the parts plus one joined field)."""
     torch = _torch()
-    return PairSet(*(torch.cat([getattr(p, f) for p in sets]) for f in PAIR_FIELDS))
+    out = {}
+    for f in PAIR_FIELDS:
+        out[f] = torch.cat([getattr(p, f) for p in sets])
+        for p in sets:
+            setattr(p, f, None)
+    return PairSet(**out)
 
 
 def train(net: UNet3D, pairs: PairSet, *, steps: int, batch: int = 4, seed: int = 0,
