@@ -399,7 +399,7 @@ def conv_arm(args, local):
     peak = float(peaks.get("bf16_tflops", 1590.0))
     out = {"workload": "conv3d 48->16, 16 x 64 x 64 x 128 voxels, bf16/fp32", "flops": flops}
     previous = lib.pmd_conv3d_impl(-1)
-    for name, impl in (("tensor_memory", 2), ("mma_sync", 1)):
+    for name, impl in (("tensor_memory_pipelined", 3), ("tensor_memory", 2), ("mma_sync", 1)):
         lib.pmd_conv3d_impl(impl)
         for _ in range(args.warmup):
             assert lib.pmd_conv3d(x.data_ptr(), wt.data_ptr(), None, y.data_ptr(), b, d, h, w, cin,

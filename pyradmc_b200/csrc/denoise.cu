@@ -725,8 +725,9 @@ int launched() { return cudaGetLastError() == cudaSuccess ? 0 : -2; }
 // The vectorized element-wise kernels index with 32-bit integers.
 bool fits32(long long elements) { return elements < (1LL << 31); }
 
-// Convolution path: 0 = tensor-memory UMMA kernel where it applies, else the
-// mma.sync kernel; 1 = mma.sync only; 2 = UMMA only.
+// Convolution path: 0 = the pipelined tensor-memory kernel where it applies,
+// else the single-buffered one, else the mma.sync kernel; 1 = mma.sync only;
+// 2 = single-buffered tensor-memory kernel only; 3 = pipelined only.
 int g_conv_impl = 0;
 
 constexpr int kSmemPerSM = 233472;      // bytes of shared memory per SM
@@ -785,6 +786,58 @@ bool umma_plan(const ConvShape& s, UmmaConv& u, int& smem, int& ctas_per_sm) {
     return ctas_per_sm >= 1;
 }
 
+// Plan of the pipelined variant: the single-pass plan with two halo buffers
+// (each with its slack) and two accumulators; false when they do not fit.
+bool umma_pipe_plan(const ConvShape& s, UmmaConv& u, int& smem, int& ctas_per_sm) {
+    int base_smem = 0, base_per_sm = 0;
+    if (!umma_plan(s, u, base_smem, base_per_sm) || u.passes != 1) return false;
+    const int extra = 16;
+    smem = 2 * ((int)u.halo_bytes + kUSlack) + (int)u.w_chunks * s.cout * 16 + (int)u.k_steps * 16 + extra;
+    if (smem > kSmemPerBlockMax || 2 * u.tz * s.cout > 512) return false;
+    unsigned cols = 32;
+    while (cols < (unsigned)(2 * u.tz * s.cout)) cols <<= 1;
+    u.tmem_cols = cols;
+    int by_smem = kSmemPerSM / (smem + kSmemReserved);
+    const int by_tmem = 512 / (int)cols;
+    if (by_smem > by_tmem) {
+        smem = kSmemPerSM / by_tmem - kSmemReserved;
+        if (smem > kSmemPerBlockMax) smem = kSmemPerBlockMax;
+        by_smem = kSmemPerSM / (smem + kSmemReserved);
+    }
+    ctas_per_sm = by_smem < 4 ? by_smem : 4;
+    return ctas_per_sm >= 1;
+}
+
+template <int CPT>
+int launch_umma_pipe(const __nv_bfloat16* x, const __nv_bfloat16* w, const float* bias,
+                     __nv_bfloat16* y, const UmmaConv& u, int smem, int per_sm, int relu,
+                     cudaStream_t st) {
+    int dev = 0, sms = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+        return -2;
+    if (cudaFuncSetAttribute(conv3d_umma_pipe_kernel<CPT>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess)
+        return -2;
+    const int grid = u.n_tiles < sms * per_sm ? u.n_tiles : sms * per_sm;
+    conv3d_umma_pipe_kernel<CPT><<<grid, 128, smem, st>>>(x, w, bias, y, u, relu);
+    return launched();
+}
+
+int dispatch_umma_pipe(const __nv_bfloat16* x, const __nv_bfloat16* w, const float* bias,
+                       __nv_bfloat16* y, const UmmaConv& u, int smem, int per_sm, int relu,
+                       cudaStream_t st) {
+    switch (u.s.cin / 8) {
+        case 1: return launch_umma_pipe<1>(x, w, bias, y, u, smem, per_sm, relu, st);
+        case 2: return launch_umma_pipe<2>(x, w, bias, y, u, smem, per_sm, relu, st);
+        case 4: return launch_umma_pipe<4>(x, w, bias, y, u, smem, per_sm, relu, st);
+        case 6: return launch_umma_pipe<6>(x, w, bias, y, u, smem, per_sm, relu, st);
+        case 8: return launch_umma_pipe<8>(x, w, bias, y, u, smem, per_sm, relu, st);
+        case 12: return launch_umma_pipe<12>(x, w, bias, y, u, smem, per_sm, relu, st);
+        default: return -1;
+    }
+}
+
 template <int CPT>
 int launch_umma(const __nv_bfloat16* x, const __nv_bfloat16* w, const float* bias, __nv_bfloat16* y,
                 const UmmaConv& u, int smem, int per_sm, int relu, cudaStream_t st) {
@@ -827,8 +880,16 @@ int pmd_conv3d(const void* x, const void* w, const float* bias, void* y, int n, 
     auto W = (const __nv_bfloat16*)w;
     auto Y = (__nv_bfloat16*)y;
     cudaStream_t st = (cudaStream_t)stream;
-    if (g_conv_impl != 1) {
-        // auto: the tensor-memory kernel where its weights stay resident (one pass)
+    if (g_conv_impl == 0 || g_conv_impl == 3) {
+        // the pipelined tensor-memory kernel where two halos and the weights fit
+        UmmaConv u{};
+        int smem = 0, per_sm = 0;
+        if (umma_pipe_plan(s, u, smem, per_sm))
+            return dispatch_umma_pipe(X, W, bias, Y, u, smem, per_sm, relu, st);
+        if (g_conv_impl == 3) return -1;
+    }
+    if (g_conv_impl == 0 || g_conv_impl == 2) {
+        // the tensor-memory kernel where its weights stay resident (one pass)
         UmmaConv u{};
         int smem = 0, per_sm = 0;
         if (umma_plan(s, u, smem, per_sm) && (g_conv_impl == 2 || u.passes == 1))
@@ -851,7 +912,7 @@ int pmd_conv3d(const void* x, const void* w, const float* bias, void* y, int n, 
 
 int pmd_conv3d_impl(int impl) {
     const int previous = g_conv_impl;
-    if (impl >= 0 && impl <= 2) g_conv_impl = impl;
+    if (impl >= 0 && impl <= 3) g_conv_impl = impl;
     return previous;
 }
 

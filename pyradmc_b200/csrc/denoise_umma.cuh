@@ -299,4 +299,206 @@ conv3d_umma_kernel(const __nv_bfloat16* __restrict__ x, const __nv_bfloat16* __r
     }
 }
 
+// ---- pipelined variant ---------------------------------------------------------
+// The same tile, halo layout, descriptors and epilogue, with two halo buffers
+// (each followed by its own zeroed slack) and two accumulators in tensor
+// memory: while the MMAs of tile i run, the copies of tile i+1's halo are in
+// flight and the epilogue of tile i-1 reads the other accumulator.  Only warp
+// 0 polls the mbarrier; the other warps wait at the block barrier.  Needs the
+// weights resident (one pass) and 2 * tz * cout <= 512 tensor-memory columns.
+
+__device__ __forceinline__ void umma_tile_origin(const UmmaConv& u, int tile, int& nb, int& z0,
+                                                 int& y0, int& x0) {
+    int t = tile;
+    const int tx = t % u.tiles_w;
+    t /= u.tiles_w;
+    const int ty = t % u.tiles_h;
+    t /= u.tiles_h;
+    const int tzi = t % u.tiles_d;
+    nb = t / u.tiles_d;
+    z0 = tzi * u.tz;
+    y0 = ty * kUTY;
+    x0 = tx * kUTX;
+}
+
+template <int CPT>
+__device__ __forceinline__ void umma_load_halo(const __nv_bfloat16* __restrict__ x, const UmmaConv& u,
+                                               int tile, unsigned char* buf, int tid) {
+    const ConvShape& s = u.s;
+    int nb, z0, y0, x0;
+    umma_tile_origin(u, tile, nb, z0, y0, x0);
+    const int npos = (u.tz + 2) * kUHY * kUHX;
+    const int total = ((npos + 7) / 8) * 8 * CPT;
+    for (int i = tid; i < total; i += blockDim.x) {
+        const int pos = (i / (8 * CPT)) * 8 + (i & 7);
+        const int q = (i >> 3) % CPT;
+        if (pos >= npos) continue;
+        const int xx = pos % kUHX, r = pos / kUHX;
+        const int yy = r % kUHY, zz = r / kUHY;
+        const int z = z0 + zz - 1, yg = y0 + yy - 1, xg = x0 + xx - 1;
+        const bool in = (unsigned)z < (unsigned)s.d && (unsigned)yg < (unsigned)s.h &&
+                        (unsigned)xg < (unsigned)s.w;
+        const __nv_bfloat16* src =
+            in ? x + ((((long long)nb * s.d + z) * s.h + yg) * s.w + xg) * s.cin + q * 8 : x;
+        cp_async16(buf + (size_t)q * u.plane_bytes + (size_t)pos * 16, src, in);
+    }
+}
+
+// One accumulator row (output voxel) per thread: bias, ReLU, bf16 store.
+__device__ __forceinline__ void umma_epilogue(const UmmaConv& u, uint32_t acc, int tile,
+                                              const float* __restrict__ bias,
+                                              __nv_bfloat16* __restrict__ y, int relu, int warp,
+                                              int lane) {
+    const ConvShape& s = u.s;
+    const int N = s.cout;
+    int nb, z0, y0, x0;
+    umma_tile_origin(u, tile, nb, z0, y0, x0);
+    const int r = warp * 32 + lane;
+    const int yg = y0 + r / kUTX, xg = x0 + r % kUTX;
+    for (int sl = 0; sl < u.tz; ++sl) {
+        const int z = z0 + sl;
+        const bool ok = z < s.d && yg < s.h && xg < s.w;
+        __nv_bfloat16* out =
+            y + ((((long long)nb * s.d + (ok ? z : 0)) * s.h + (ok ? yg : 0)) * s.w + (ok ? xg : 0)) * N;
+        for (int c = 0; c < N / 16; ++c) {
+            float v[16];
+            tmem_ld16(acc + ((uint32_t)(warp * 32) << 16) + (uint32_t)(sl * N + c * 16), v);
+            if (ok) {
+                union {
+                    uint4 u4[2];
+                    __nv_bfloat162 h[8];
+                } pk;
+#pragma unroll
+                for (int e = 0; e < 8; ++e) {
+                    float a = v[2 * e], b = v[2 * e + 1];
+                    if (bias) {
+                        a += bias[c * 16 + 2 * e];
+                        b += bias[c * 16 + 2 * e + 1];
+                    }
+                    if (relu) {
+                        a = fmaxf(a, 0.0f);
+                        b = fmaxf(b, 0.0f);
+                    }
+                    pk.h[e] = __floats2bfloat162_rn(a, b);
+                }
+                uint4* o = reinterpret_cast<uint4*>(out + c * 16);
+                o[0] = pk.u4[0];
+                o[1] = pk.u4[1];
+            }
+        }
+    }
+}
+
+template <int CPT>
+__global__ void __launch_bounds__(128, 4)
+conv3d_umma_pipe_kernel(const __nv_bfloat16* __restrict__ x, const __nv_bfloat16* __restrict__ wt,
+                        const float* __restrict__ bias, __nv_bfloat16* __restrict__ y, UmmaConv u,
+                        int relu) {
+    extern __shared__ __align__(1024) unsigned char smem[];
+    const ConvShape& s = u.s;
+    const int N = s.cout;
+    constexpr int cpt = CPT;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const unsigned buf_stride = u.halo_bytes + kUSlack;  // halo + its zeroed slack
+    unsigned char* halo0 = smem;
+    unsigned char* wbuf = smem + 2 * buf_stride;
+    uint64_t* dtab = reinterpret_cast<uint64_t*>(wbuf + (size_t)u.w_chunks * N * 16);
+    uint64_t* mbar_p = dtab + 2 * u.k_steps;
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mbar_p + 1);
+    const uint32_t halo_s = smem_u32(halo0), w_s = smem_u32(wbuf), mbar = smem_u32(mbar_p);
+
+    for (int b = 0; b < 2; ++b)
+        for (int i = tid; i < kUSlack / 4; i += blockDim.x)
+            reinterpret_cast<uint32_t*>(halo0 + b * buf_stride + u.halo_bytes)[i] = 0u;
+    if (tid == 0) mbar_init(mbar, 1);
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         smem_u32(tmem_slot)),
+                     "r"(u.tmem_cols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+    const uint32_t idesc = umma_instr_desc(N);
+    const uint32_t acc_cols = (uint32_t)(u.tz * N);
+
+    // resident weights and the descriptor table (A relative to buffer 0)
+    const int n_chunks = (int)u.w_chunks;
+    for (int i = tid; i < n_chunks * N; i += blockDim.x) {
+        const int n = i % N, jj = i / N;
+        cp_async16(wbuf + ((size_t)jj * N + n) * 16, wt + (long long)n * s.kpad + (long long)jj * 8, true);
+    }
+    const int n_k = (27 * cpt + 1) / 2;
+    for (int k = tid; k < n_k; k += blockDim.x) {
+        const int j = 2 * k;
+        const int tap = j / cpt, q = j % cpt;
+        const uint32_t a_addr = halo_s + (uint32_t)q * u.plane_bytes + tap_offset(tap);
+        uint32_t a_lbo = u.plane_bytes;
+        if (cpt == 1) a_lbo = tap + 1 < 27 ? tap_offset(tap + 1) - tap_offset(tap) : 16u;
+        dtab[2 * k] = umma_smem_desc(a_addr, a_lbo, kUHX * 16);
+        dtab[2 * k + 1] = umma_smem_desc(w_s + (uint32_t)j * N * 16, N * 16, 128);
+    }
+    if ((int)blockIdx.x < u.n_tiles) umma_load_halo<CPT>(x, u, blockIdx.x, halo0, tid);
+    cp_async_commit();
+
+    constexpr uint64_t slice_inc = (uint64_t)(kUHY * kUHX * 16) >> 4;
+    const uint64_t buf_inc = (uint64_t)(buf_stride >> 4);
+    uint32_t phase = 0;
+    int failed = 0, i = 0, prev = -1;
+    for (int tile = blockIdx.x; tile < u.n_tiles; tile += gridDim.x, ++i) {
+        const int b = i & 1;
+        // this tile's halo (and, first time, the weights and table) has landed
+        cp_async_wait<0>();
+        fence_async_smem();
+        tc_fence_before();
+        __syncthreads();
+        if (tid == 0) {
+            tc_fence_after();
+            for (int sl = 0; sl < u.tz; ++sl) {
+                const uint32_t d_tmem = tmem + (uint32_t)b * acc_cols + (uint32_t)(sl * N);
+                const uint64_t a_inc = buf_inc * (uint64_t)b + slice_inc * (uint64_t)sl;
+                for (int k = 0; k < n_k; ++k)
+                    umma_bf16(d_tmem, dtab[2 * k] + a_inc, dtab[2 * k + 1], idesc, k > 0 ? 1u : 0u);
+            }
+            umma_commit(mbar);
+        }
+        // the next tile's halo into the other buffer (its last reader, the MMAs
+        // of the previous tile, completed before the previous wait returned)
+        const int next = tile + gridDim.x;
+        if (next < u.n_tiles) umma_load_halo<CPT>(x, u, next, halo0 + (b ^ 1) * buf_stride, tid);
+        cp_async_commit();
+        // the previous tile's epilogue from the other accumulator
+        if (prev >= 0) {
+            tc_fence_after();
+            umma_epilogue(u, tmem + (uint32_t)(b ^ 1) * acc_cols, prev, bias, y, relu, warp, lane);
+        }
+        const int ok = warp == 0 ? (mbar_wait(mbar, phase) ? 1 : 0) : 1;
+        phase ^= 1u;
+        tc_fence_before();
+        failed = __syncthreads_or(!ok);
+        if (failed) break;
+        prev = tile;
+    }
+    if (!failed && prev >= 0) {
+        tc_fence_after();
+        umma_epilogue(u, tmem + (uint32_t)((i - 1) & 1) * acc_cols, prev, bias, y, relu, warp, lane);
+    }
+    cp_async_wait<0>();
+    if (failed) {
+        if (tid == 0) atomicAdd(&g_umma_failures, 1);
+        if (warp == 0) mbar_wait(mbar, phase ^ 1u);  // one more bounded wait for MMAs in flight
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                     "r"(u.tmem_cols)
+                     : "memory");
+    }
+}
+
 }  // namespace pmd
