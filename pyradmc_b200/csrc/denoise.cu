@@ -725,8 +725,8 @@ int launched() { return cudaGetLastError() == cudaSuccess ? 0 : -2; }
 // The vectorized element-wise kernels index with 32-bit integers.
 bool fits32(long long elements) { return elements < (1LL << 31); }
 
-// Convolution path: 0 = the pipelined tensor-memory kernel where it applies,
-// else the single-buffered one, else the mma.sync kernel; 1 = mma.sync only;
+// Convolution path: 0 = the single-buffered tensor-memory kernel where its
+// weights fit at once, else the mma.sync kernel; 1 = mma.sync only;
 // 2 = single-buffered tensor-memory kernel only; 3 = pipelined only.
 int g_conv_impl = 0;
 
@@ -880,8 +880,9 @@ int pmd_conv3d(const void* x, const void* w, const float* bias, void* y, int n, 
     auto W = (const __nv_bfloat16*)w;
     auto Y = (__nv_bfloat16*)y;
     cudaStream_t st = (cudaStream_t)stream;
-    if (g_conv_impl == 0 || g_conv_impl == 3) {
-        // the pipelined tensor-memory kernel where two halos and the weights fit
+    if (g_conv_impl == 3) {
+        // the pipelined tensor-memory kernel (opt-in: measured slower than two
+        // single-buffered CTAs per SM on the network's layers)
         UmmaConv u{};
         int smem = 0, per_sm = 0;
         if (umma_pipe_plan(s, u, smem, per_sm))

@@ -266,10 +266,11 @@ def denoise_dense(net: UNet3D, dose, colmax, density, grid_shape, *, sigma=None,
     return out
 
 
-def compact(mean, sigma, truncation: float):
+def compact(mean, sigma, truncation: float, to_host: bool = True):
     """Truncation + CSC of dense float64 columns on the device, through the
     allocation-free compaction entry point: (indptr, indices, dose, sigma) on
-    the host."""
+    the host, or (with to_host False) indptr on the host and the entries as
+    device tensors."""
     torch = _torch()
     lib = _lib.load()
     n_cols, vox = mean.shape
@@ -290,17 +291,21 @@ def compact(mean, sigma, truncation: float):
     k = nnz.value
     indptr = np.zeros(n_cols + 1, dtype=np.int64)
     np.cumsum(counts.cpu().numpy(), out=indptr[1:])
+    if not to_host:
+        return indptr, idx[:k], dose[:k], sig[:k]
     return indptr, idx[:k].cpu().numpy(), dose[:k].cpu().numpy(), sig[:k].cpu().numpy()
 
 
 def run_dij_denoised(engine, net: UNet3D | None, source, n_histories_per_beamlet, n_batches: int,
-                     seed: int, *, truncation: float = 1.0e-3, lateral: int = 64, chunk: int = 16):
+                     seed: int, *, truncation: float = 1.0e-3, lateral: int = 64, chunk: int = 16,
+                     to_host: bool = True):
     """A Dij from low-history Monte Carlo plus the denoiser: the engine runs the
     beamlets (``run_dij_device``), every column's window around its beamlet is
     replaced by the network's estimate, and the dense columns are truncated and
     compacted to CSC on the device.  The per-entry sigma is the Monte Carlo
-    sigma of the input run.  With ``net`` None this is plain Monte Carlo
-    (``engine.run_dij``), the method's fallback."""
+    sigma of the input run.  With ``to_host`` False the CSC entries stay on
+    the device (torch tensors in the result).  With ``net`` None this is plain
+    Monte Carlo (``engine.run_dij``), the method's fallback."""
     import torch
 
     from .engine import ENERGY_QUANTUM_MEV, _result_types
@@ -317,7 +322,7 @@ def run_dij_denoised(engine, net: UNet3D | None, source, n_histories_per_beamlet
     denoise_dense(net, dose, colmax, rho, shape, sigma=sigma32,
                   window=inference_window(shape, lateral), chunk=chunk, out=mean)
     del dose, sigma32
-    indptr, indices, dose_v, sigma_v = compact(mean, sigma, truncation)
+    indptr, indices, dose_v, sigma_v = compact(mean, sigma, truncation, to_host=to_host)
     deposited, escaped, unscored, emitted = view.books
     counts = np.asarray(view.counts)
     _, _, DijResult = _result_types()
