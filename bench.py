@@ -280,7 +280,7 @@ def denoiser_leg(args, engine, source, counts, stream, device, plain_s_at_2pct):
     scale of LADDER (times the benchmark's per-beamlet counts) whose denoised
     columns reach a sigma-equivalent error <= 2 % against it.  Timed (CUDA
     events on the engine's stream): ``run_dij_denoised`` at that scale, from
-    transport to the host CSC."""
+    transport to the CSC in HBM (device-resident, like ``value``)."""
     import torch
 
     from pyradmc_b200 import _lib
