@@ -270,14 +270,14 @@ def algorithmic_bytes(c: dict) -> float:
 
 DENOISER_WEIGHTS = ROOT / "pyradmc_b200" / "data" / "denoiser_unet.npz"
 REF_HISTORIES = 8_000_000     # per beamlet: the high-statistics judge of the denoiser's error
-LADDER = (1 / 4, 1 / 2, 1.0, 2.0, 4.0, 8.0)  # history scales tried for MC + denoiser
+LADDER = (1 / 4, 1 / 3, 0.4, 1 / 2, 2 / 3, 1.0, 1.5, 2.0, 3.0, 4.0, 6.0, 8.0)  # scales tried
 
 
 def denoiser_leg(args, engine, source, counts, stream, device, plain_s_at_2pct):
     """s per Dij at 2 % for MC + denoiser on the benchmark Dij.
 
     Untimed: a REF_HISTORIES-per-beamlet reference, then the smallest history
-    scale of LADDER (times the benchmark's per-beamlet counts) whose denoised
+    scale of LADDER (ascending; times the benchmark's per-beamlet counts) whose denoised
     columns reach a sigma-equivalent error <= 2 % against it.  Timed (CUDA
     events on the engine's stream): ``run_dij_denoised`` at that scale, from
     transport to the CSC in HBM (device-resident, like ``value``)."""
