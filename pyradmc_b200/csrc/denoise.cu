@@ -762,6 +762,7 @@ bool umma_plan(const ConvShape& s, UmmaConv& u, int& smem, int& ctas_per_sm) {
         u.w_chunks = (unsigned)(taps * cpt);
     }
     u.k_steps = (u.w_chunks + 1) / 2;
+    u.ystride = s.cout;
     smem = base + (int)u.w_chunks * s.cout * 16 + (int)u.k_steps * 16;
     unsigned cols = 32;
     while (cols < (unsigned)(u.tz * s.cout)) cols <<= 1;
@@ -890,11 +891,28 @@ int pmd_conv3d(const void* x, const void* w, const float* bias, void* y, int n, 
         if (g_conv_impl == 3) return -1;
     }
     if (g_conv_impl == 0 || g_conv_impl == 2) {
-        // the tensor-memory kernel where its weights stay resident (one pass)
+        // the tensor-memory kernel where its weights stay resident (one pass) ...
         UmmaConv u{};
         int smem = 0, per_sm = 0;
         if (umma_plan(s, u, smem, per_sm) && (g_conv_impl == 2 || u.passes == 1))
             return dispatch_umma(X, W, bias, Y, u, smem, per_sm, relu, st);
+        // ... or, in auto mode, in output-channel slices whose weights do
+        if (g_conv_impl == 0) {
+            for (int parts = 2; parts <= 4 && cout / parts >= 16; ++parts) {
+                if (cout % parts || (cout / parts) % 16) continue;
+                ConvShape part = s;
+                part.cout = cout / parts;
+                if (!umma_plan(part, u, smem, per_sm) || u.passes != 1) continue;
+                u.ystride = cout;
+                for (int p = 0; p < parts; ++p) {
+                    const int rc = dispatch_umma(X, W + (long long)p * part.cout * kpad,
+                                                 bias ? bias + p * part.cout : nullptr,
+                                                 Y + p * part.cout, u, smem, per_sm, relu, st);
+                    if (rc) return rc;
+                }
+                return 0;
+            }
+        }
         if (g_conv_impl == 2) return -1;
     }
     switch (cout) {

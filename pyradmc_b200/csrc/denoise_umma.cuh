@@ -42,6 +42,7 @@ struct UmmaConv {
     unsigned w_chunks;  // weight chunks staged per pass (incl. the cin = 8 pad partner)
     unsigned k_steps;   // K steps (16-wide) per pass: descriptor table entries
     unsigned tmem_cols;
+    int ystride;        // channels per voxel of the output tensor (>= cout: a channel slice)
 };
 
 __device__ __forceinline__ uint64_t umma_smem_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
@@ -253,7 +254,7 @@ conv3d_umma_kernel(const __nv_bfloat16* __restrict__ x, const __nv_bfloat16* __r
             const int z = z0 + sl;
             const bool ok = z < s.d && yg < s.h && xg < s.w;
             __nv_bfloat16* out = y + ((((long long)nb * s.d + (ok ? z : 0)) * s.h + (ok ? yg : 0)) * s.w +
-                                      (ok ? xg : 0)) * N;
+                                      (ok ? xg : 0)) * u.ystride;
             for (int c = 0; c < N / 16; ++c) {
                 float v[16];
                 tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(sl * N + c * 16), v);
@@ -359,7 +360,8 @@ __device__ __forceinline__ void umma_epilogue(const UmmaConv& u, uint32_t acc, i
         const int z = z0 + sl;
         const bool ok = z < s.d && yg < s.h && xg < s.w;
         __nv_bfloat16* out =
-            y + ((((long long)nb * s.d + (ok ? z : 0)) * s.h + (ok ? yg : 0)) * s.w + (ok ? xg : 0)) * N;
+            y + ((((long long)nb * s.d + (ok ? z : 0)) * s.h + (ok ? yg : 0)) * s.w + (ok ? xg : 0)) *
+                    u.ystride;
         for (int c = 0; c < N / 16; ++c) {
             float v[16];
             tmem_ld16(acc + ((uint32_t)(warp * 32) << 16) + (uint32_t)(sl * N + c * 16), v);
