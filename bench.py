@@ -554,7 +554,8 @@ def b200_arm(args, world, rank, local):
         "s_per_dij_at_2pct_sigma": s_at_2pct,
         "denoiser": den,
         "e2e": {"value": e2e_value, "unit": "histories/s",
-                "h2d_bytes_per_step": int(np.median(h2d)), "d2h_bytes_per_step": int(np.median(d2h))},
+                "h2d_bytes_per_step": int(np.median(h2d)), "d2h_bytes_per_step": int(np.median(d2h)),
+                "ms_per_step": e2e_total / args.steps},
         "roofline": {
             "bound": "hbm",
             "kernel": "photon_kernel+electron_kernel (transport graph)",

@@ -165,6 +165,22 @@ class DeviceDij:
     device: str = "cuda:0"
 
 
+def _pinned_array(n: int, dtype) -> np.ndarray:
+    """A numpy array in page-locked host memory (torch's caching host allocator,
+    so repeated Dijs reuse the blocks): the CSC readback then runs at the full
+    host link rate instead of through the driver's pageable staging.  Plain
+    numpy memory when pinning is unavailable."""
+    if n >= 1 << 16:
+        try:
+            import torch
+
+            tdt = {np.dtype(np.int64): torch.int64, np.dtype(np.float64): torch.float64}[np.dtype(dtype)]
+            return torch.empty(int(n), dtype=tdt, pin_memory=True).numpy()
+        except Exception:
+            pass
+    return np.empty(n, dtype=dtype)
+
+
 def column_shards(counts, world: int) -> list[tuple[int, int]]:
     """Contiguous Dij column ranges, one per rank, with near-equal history totals
     (some empty when there are more ranks than columns)."""
@@ -813,9 +829,9 @@ class B200Engine:
                     if device_view:
                         return _device_dij(native, g1 - g0, nnz.value, books), None
                     indptr = np.zeros(g1 - g0 + 1, dtype=np.int64)
-                    indices = np.empty(nnz.value, dtype=np.int64)
-                    dose = np.empty(nnz.value, dtype=np.float64)
-                    sigma = np.empty(nnz.value, dtype=np.float64)
+                    indices = _pinned_array(nnz.value, np.int64)
+                    dose = _pinned_array(nnz.value, np.float64)
+                    sigma = _pinned_array(nnz.value, np.float64)
                     native.check(lib.pmc_dij_fetch(native.handle, _lib.ptr(indptr, C.c_int64),
                                                    _lib.ptr(indices, C.c_int64),
                                                    _lib.ptr(dose, C.c_double),
