@@ -40,8 +40,8 @@ int pmd_conv3d(const void* x, const void* w, const float* bias, void* y, int n, 
 
 /* Selects the convolution kernels of pmd_conv3d: 0 (default) the tensor-memory
  * kernel (tcgen05.mma, accumulators in TMEM; cout a multiple of 16 up to 192,
- * cin 8 or a multiple of 16 up to 96) where its weights fit shared memory at
- * once, and the mma.sync kernel elsewhere; 1 the mma.sync kernel only; 2 the
+ * cin 8 or a multiple of 16 up to 96) where its weights are staged in shared
+ * memory in at most two passes, and the mma.sync kernel elsewhere; 1 the mma.sync kernel only; 2 the
  * tensor-memory kernel only; 3 its pipelined variant only (two halo buffers
  * and two accumulators, one CTA per SM; measured slower than the default on
  * this network's layers, kept for larger tiles).  Other shapes return -1.  impl < 0 only queries.  Returns the

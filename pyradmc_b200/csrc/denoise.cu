@@ -726,7 +726,7 @@ int launched() { return cudaGetLastError() == cudaSuccess ? 0 : -2; }
 bool fits32(long long elements) { return elements < (1LL << 31); }
 
 // Convolution path: 0 = the single-buffered tensor-memory kernel where its
-// weights fit at once, else the mma.sync kernel; 1 = mma.sync only;
+// weights are staged in at most two passes, else the mma.sync kernel; 1 = mma.sync only;
 // 2 = single-buffered tensor-memory kernel only; 3 = pipelined only.
 int g_conv_impl = 0;
 
@@ -891,28 +891,13 @@ int pmd_conv3d(const void* x, const void* w, const float* bias, void* y, int n, 
         if (g_conv_impl == 3) return -1;
     }
     if (g_conv_impl == 0 || g_conv_impl == 2) {
-        // the tensor-memory kernel where its weights stay resident (one pass) ...
+        // the tensor-memory kernel where its weights are staged in at most two
+        // passes (measured: beyond that, and for output-channel slices, the
+        // mma.sync kernel is faster)
         UmmaConv u{};
         int smem = 0, per_sm = 0;
-        if (umma_plan(s, u, smem, per_sm) && (g_conv_impl == 2 || u.passes == 1))
+        if (umma_plan(s, u, smem, per_sm) && (g_conv_impl == 2 || u.passes <= 2))
             return dispatch_umma(X, W, bias, Y, u, smem, per_sm, relu, st);
-        // ... or, in auto mode, in output-channel slices whose weights do
-        if (g_conv_impl == 0) {
-            for (int parts = 2; parts <= 4 && cout / parts >= 16; ++parts) {
-                if (cout % parts || (cout / parts) % 16) continue;
-                ConvShape part = s;
-                part.cout = cout / parts;
-                if (!umma_plan(part, u, smem, per_sm) || u.passes != 1) continue;
-                u.ystride = cout;
-                for (int p = 0; p < parts; ++p) {
-                    const int rc = dispatch_umma(X, W + (long long)p * part.cout * kpad,
-                                                 bias ? bias + p * part.cout : nullptr,
-                                                 Y + p * part.cout, u, smem, per_sm, relu, st);
-                    if (rc) return rc;
-                }
-                return 0;
-            }
-        }
         if (g_conv_impl == 2) return -1;
     }
     switch (cout) {
