@@ -241,7 +241,7 @@ def inference_window(grid_shape, lateral: int = 64) -> tuple[int, int, int]:
 
 
 def denoise_dense(net: UNet3D, dose, colmax, density, grid_shape, *, sigma=None, window=None,
-                  chunk: int = 16, out=None):
+                  chunk: int = 32, out=None):
     """Denoised dense columns, float64 [C, vox]: the Monte Carlo columns
     (float32 dose [C, vox] with their maxima and, optionally, their sigma; or
     `out`, float64, written in place) with every column's window replaced by
@@ -252,6 +252,7 @@ def denoise_dense(net: UNet3D, dose, colmax, density, grid_shape, *, sigma=None,
     if out is None:
         out = dose.to(torch.float64)
     n = dose.shape[0]
+    chunk = -(-n // -(-n // chunk))  # equal chunks of at most `chunk` windows: no padded work
     for c0 in range(0, n, chunk):
         c1 = min(c0 + chunk, n)
         idx = torch.arange(c0, c0 + chunk, device=dose.device).clamp_max(n - 1)  # fixed batch shape
@@ -297,7 +298,7 @@ def compact(mean, sigma, truncation: float, to_host: bool = True):
 
 
 def run_dij_denoised(engine, net: UNet3D | None, source, n_histories_per_beamlet, n_batches: int,
-                     seed: int, *, truncation: float = 1.0e-3, lateral: int = 64, chunk: int = 16,
+                     seed: int, *, truncation: float = 1.0e-3, lateral: int = 64, chunk: int = 32,
                      to_host: bool = True):
     """A Dij from low-history Monte Carlo plus the denoiser: the engine runs the
     beamlets (``run_dij_device``), every column's window around its beamlet is
