@@ -330,6 +330,8 @@ def denoiser_leg(args, engine, source, counts, stream, device, plain_s_at_2pct):
         times.append(start.elapsed_time(end) / 1e3)
     unet_launches = (net.launches - launches0) / args.steps
     s_den = float(np.median(times))
+    stages: dict = {}
+    D.run_dij_denoised(engine, net, source, truncation=1e-3, to_host=False, timings=stages, **kw)
 
     # the dominant convolution (decoder level 0, 48 -> 16 channels, tensor memory)
     lib = _lib.load()
@@ -366,6 +368,7 @@ def denoiser_leg(args, engine, source, counts, stream, device, plain_s_at_2pct):
         "ladder": ladder,
         "window": list(window),
         "unet_launches_per_dij": unet_launches,
+        "stage_ms": stages,
         "unet_forward_flops_per_dij": forward_flops_per_voxel() * unet_vox,
         "nnz": int(dij.indptr[-1]),
         "roofline": {"bound": "tensor", "kernel": "conv3d_umma_kernel (decoder level 0, 48->16)",

@@ -299,7 +299,7 @@ def compact(mean, sigma, truncation: float, to_host: bool = True):
 
 def run_dij_denoised(engine, net: UNet3D | None, source, n_histories_per_beamlet, n_batches: int,
                      seed: int, *, truncation: float = 1.0e-3, lateral: int = 64, chunk: int = 32,
-                     to_host: bool = True):
+                     to_host: bool = True, timings: dict | None = None):
     """A Dij from low-history Monte Carlo plus the denoiser: the engine runs the
     beamlets (``run_dij_device``), every column's window around its beamlet is
     replaced by the network's estimate, and the dense columns are truncated and
@@ -314,16 +314,33 @@ def run_dij_denoised(engine, net: UNet3D | None, source, n_histories_per_beamlet
     if net is None:
         return engine.run_dij(source, n_histories_per_beamlet, n_batches, seed,
                               truncation=truncation)
+    marks = []
+
+    def mark(name):  # CUDA events between the stages, read when `timings` is given
+        if timings is not None:
+            ev = torch.cuda.Event(enable_timing=True)
+            ev.record()
+            marks.append((name, ev))
+
+    mark("start")
     view = engine.run_dij_device(source, n_histories_per_beamlet, n_batches, seed, truncation=0.0)
     device = torch.device(view.device)
     shape = tuple(view.grid_shape)
+    mark("monte_carlo")
     dose, colmax, sigma32 = dense_columns(view, device, with_sigma=True)
     mean, sigma = dense_columns_f64(view, device)
     rho = torch.from_numpy(np.ascontiguousarray(engine.grid.density, dtype=np.float32).ravel()).to(device)
+    mark("dense_columns")
     denoise_dense(net, dose, colmax, rho, shape, sigma=sigma32,
                   window=inference_window(shape, lateral), chunk=chunk, out=mean)
     del dose, sigma32
+    mark("unet")
     indptr, indices, dose_v, sigma_v = compact(mean, sigma, truncation, to_host=to_host)
+    mark("compaction")
+    if timings is not None:
+        marks[-1][1].synchronize()
+        for (_, a), (name, b) in zip(marks, marks[1:]):
+            timings[name] = timings.get(name, 0.0) + a.elapsed_time(b)
     deposited, escaped, unscored, emitted = view.books
     counts = np.asarray(view.counts)
     _, _, DijResult = _result_types()
