@@ -741,7 +741,9 @@ bool umma_plan(const ConvShape& s, UmmaConv& u, int& smem, int& ctas_per_sm) {
     if (!(s.cin == 8 || (s.cin % 16 == 0 && s.cin <= 96))) return false;
     const int cpt = s.cin / 8;
     u.s = s;
-    u.tz = s.cin <= 48 ? 2 : 1;
+    // taller tiles amortize the halo over more MMAs where the halo is small
+    // (measured: 12-18 % faster for cin <= 16, cout 16; slower at cout 32)
+    u.tz = s.cin <= 16 && s.cout <= 16 ? 4 : (s.cin <= 48 ? 2 : 1);
     const int npos = (u.tz + 2) * kUHY * kUHX;
     u.plane_bytes = (unsigned)npos * 16;
     u.halo_bytes = u.plane_bytes * cpt;
