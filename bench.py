@@ -261,7 +261,10 @@ def reference_arm(args, world, rank):
 
 # ---- the B200 arm ---------------------------------------------------------------------
 def algorithmic_bytes(c: dict) -> float:
-    """Transport bytes by event (the per-event figures stated in DESIGN.md)."""
+    """Transport bytes by event: 13 B per Woodcock flight (voxel 5 + majorant 8),
+    +32 B per real interaction (4 channel lookups), 77 B per electron substep
+    (voxel 5 + 7 lookups x 8 + GS 16), 16 B per int64 deposit, 48 B per queue
+    push and 48 B per pop."""
     pops = c["queue_pushes"]
     return (13.0 * c["photon_flights"] + 32.0 * c["photon_interactions"]
             + 77.0 * c["electron_substeps"] + 16.0 * c["deposits"]
@@ -549,12 +552,14 @@ def b200_arm(args, world, rank, local):
         "data": "synthetic (seeded phantom and beamlet counts)",
         "config": {**config_dict(counts, "256 MB buffer written between timed steps (flush)"),
                    "launch": {"block_size": engine.block_size, "blocks_per_sm": engine.blocks_per_sm,
-                              "chunk_size": engine.chunk_size,
+                              "chunk_size": engine.chunk_size, "tail_steps": engine.tail_steps,
+                              "smem_tables": engine.smem_tables,
                               "autotuned": tune_report is not None,
                               "tune_cached": None if tune_report is None else tune_report["cached"]}},
         "s_per_dij": s_per_dij,
         "per_beamlet_sigma": sigma,
         "s_per_dij_at_2pct_sigma": s_at_2pct,
+        "plain_2pct": "extrapolated: measured s per Dij x (per-beamlet sigma / 2 %)^2 (1/sqrt(N) scaling)",
         "denoiser": den,
         "e2e": {"value": e2e_value, "unit": "histories/s",
                 "h2d_bytes_per_step": int(np.median(h2d)), "d2h_bytes_per_step": int(np.median(d2h)),

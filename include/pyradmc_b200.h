@@ -29,7 +29,7 @@
 extern "C" {
 #endif
 
-#define PMC_ABI_VERSION 1
+#define PMC_ABI_VERSION 2
 
 /* Return codes.  The Python host maps them onto the reference's exceptions:
  * INVALID -> ValueError (engine.py:512-550), MAJORANT and QUEUE_OVERFLOW ->
@@ -42,6 +42,7 @@ extern "C" {
 #define PMC_ERR_CUDA (-5)
 #define PMC_ERR_OOM (-6)
 #define PMC_ERR_STATE (-7)
+#define PMC_ERR_CAPACITY (-8) /* a caller-sized output buffer is too small */
 
 /* Particle kinds: pyradmc/transport/particles.py:23-25. */
 #define PMC_PHOTON 0
@@ -57,10 +58,16 @@ extern "C" {
 #define PMC_SRC_SPECTRAL 2
 #define PMC_SRC_UPLOAD 3
 
-/* Beamlet generators: generate_beamlet_lattice (kernels.py:2248) and
- * generate_spectral_beamlets (kernels.py:2322). */
+/* Beamlet generators: generate_beamlet_lattice (kernels.py:2248),
+ * generate_spectral_beamlets (kernels.py:2322), per-beamlet records (fans and
+ * lattice rectangles of any geometry, and per-beamlet mixtures of them:
+ * CompositeBeamletSource, geometry/source.py:239-277), and the host
+ * pre-sampling route of BeamletSource.sample_beamlet_batch
+ * (engine.py:3224-3335 _generate_group_presampled). */
 #define PMC_BEAMLET_LATTICE 0
 #define PMC_BEAMLET_SPECTRAL 1
+#define PMC_BEAMLET_RECORDS 2
+#define PMC_BEAMLET_UPLOAD 3
 
 typedef struct pmc_engine pmc_engine;
 
@@ -123,6 +130,28 @@ typedef struct pmc_source_desc {
     const float* up_weight;
 } pmc_source_desc;
 
+/* One beamlet of a PMC_BEAMLET_RECORDS source: a lattice rectangle
+ * (BeamletGridSource.emit, geometry/source.py:420: two uniforms, +z travel) or
+ * a divergent fan through an aperture (_DivergentFan.emit_through, :479: four
+ * uniforms, energy from the record's spectrum). */
+typedef struct pmc_beamlet_rec {
+    int32_t type;     /* PMC_BEAMLET_LATTICE or PMC_BEAMLET_SPECTRAL */
+    int32_t spectrum; /* fan: index into the descriptor's spectra */
+    double energy, z0;                             /* lattice */
+    double x_lo, x_extent, y_lo, y_extent;         /* lattice */
+    double focal[3], center[3], u_axis[3], v_axis[3]; /* fan (unit axes) */
+    double width_u, width_v;                       /* fan */
+} pmc_beamlet_rec;
+
+/* Host pre-sampling callback of PMC_BEAMLET_UPLOAD: write the n primaries of
+ * column `beamlet` (an index into this call's descriptor) whose transport
+ * streams are keyed key_offset .. key_offset + n - 1, as
+ * BeamletSource.sample_beamlet_batch(seed, key_offset, n, beamlet) does.
+ * position and direction are [n][3]; every primary is a photon.  Return 0, or
+ * non-zero to abort the call with PMC_ERR_INVALID. */
+typedef int (*pmc_sample_fn)(void* user, int32_t beamlet, int64_t key_offset, int64_t n,
+                             float* energy, float* position, float* direction, float* weight);
+
 /* Beamlet source for run_dij (engine.py:948). */
 typedef struct pmc_beamlet_desc {
     int32_t type; /* PMC_BEAMLET_* */
@@ -142,6 +171,19 @@ typedef struct pmc_beamlet_desc {
      * exclusive prefix sum of counts.  Lets a caller run a range of beamlets
      * (one device's share) with the streams the whole matrix would use. */
     const int64_t* history_offsets;
+    /* PMC_BEAMLET_RECORDS: records [n_beamlets][n_components]; with several
+     * components a beamlet is a mixture: one uniform u picks the first
+     * component whose component_cdf entry is >= u, then that record emits. */
+    int32_t n_components;
+    const pmc_beamlet_rec* records;
+    const double* component_cdf;  /* [n_components], ends at 1 */
+    int32_t n_spectra;
+    const int32_t* spectrum_bins; /* [n_spectra] */
+    const double* spectrum_edges; /* concatenated, spectrum_bins[k] + 1 each */
+    const double* spectrum_cdf;   /* concatenated, spectrum_bins[k] each */
+    /* PMC_BEAMLET_UPLOAD */
+    pmc_sample_fn sample;
+    void* sample_user;
 } pmc_beamlet_desc;
 
 /* Run options: the keyword arguments of WarpEngine.run / run_dij plus the
@@ -167,6 +209,11 @@ typedef struct pmc_run_params {
     int32_t blocks_per_sm;  /* transport blocks per SM; 0: auto */
     int32_t use_graph;      /* drain each batch inside one CUDA graph */
     int64_t max_steps;      /* per-particle step cap; 0: default */
+    int32_t tail_steps;     /* steps a particle may take after its round's input ran dry
+                               before it is parked for the next round; 0: default,
+                               < 0: never park */
+    int32_t smem_tables;    /* 1: stage the photon and electron table rows in shared
+                               memory, -1: read them through L1, 0: auto */
 } pmc_run_params;
 
 /* Exact integer energy books of a call, in quanta of 1e-9 MeV
@@ -283,23 +330,29 @@ int pmc_truncate_dense(pmc_engine* engine, const double* mean, const double* sig
 
 /* Allocation-free truncation + CSC compaction.  No counterpart in the
  * reference: it exists for callers that cannot call cudaMalloc (an application
- * whose device memory all comes from its own pool, a process that fixes its
- * footprint at start-up, work recorded into a CUDA graph).  It is the
- * truncation and compaction of pmc_truncate_dense over caller-owned DEVICE
- * buffers, with no allocation of any kind: its scratch is a static device
- * array of about 3.2 MB that every GPU loading the library holds until exit.
+ * whose device memory all comes from its own pool or allocator, or a process
+ * that fixes its device footprint at start-up and forbids allocation after
+ * that).  It is the truncation and compaction of pmc_truncate_dense over
+ * caller-owned DEVICE buffers, with no allocation of any kind: its scratch is
+ * a static device array of about 3.2 MB that every GPU loading the library
+ * holds until exit.
  *   mean, sigma  [n_cols][n_vox] float64 dose means and sigmas (device)
  *   col_counts   [n_cols] int64 kept entries per column (device)
  *   out_*        [out_capacity] CSC rows, doses, sigmas (device)
- *   *nnz         the entry total (host); when it exceeds out_capacity the
- *                call returns PMC_ERR_INVALID without writing out_*
- * Limits: n_cols <= 4096 and n_cols * ceil(n_vox / 4096) <= 262144 (and at
- * most 65535 tiles per column); larger sizes return PMC_ERR_INVALID.
+ *   *nnz         the entry total (host).  When it exceeds out_capacity the
+ *                call returns PMC_ERR_CAPACITY and writes neither out_* nor
+ *                col_counts; retry with out_capacity >= *nnz.  On every
+ *                other failure *nnz is left as it was.
+ * Limits: n_cols <= 4096 and n_cols * ceil(n_vox / 4096) <= 262144; larger
+ * sizes return PMC_ERR_INVALID.
  * Work runs on `stream` (a cudaStream_t, NULL = the default stream) of the
- * current device, and the call returns after it finished.  The first call on a
- * device looks up the scratch array's device address, so make that first call
- * before any stream capture.  All calls share the one array: calls that
- * overlap on the GPU (other threads or streams) race. */
+ * current device.  The call reads the entry total back to the host and
+ * synchronizes `stream` (twice), so it must not be called while `stream` is
+ * being captured into a CUDA graph.  The first call on a device looks up the
+ * scratch array's device address and keeps it for the life of the process; a
+ * cudaDeviceReset of that device invalidates the kept address, so do not call
+ * this entry point after resetting the device.  All calls share the one array:
+ * calls that overlap on the GPU (other threads or streams) race. */
 int pmc_dij_compact_static(const double* mean, const double* sigma, int32_t n_cols,
                            int64_t n_vox, double truncation, int64_t out_capacity,
                            int64_t* col_counts, int64_t* out_indices, double* out_dose,

@@ -33,8 +33,16 @@ def chi2_batched(a, sigma_a, n_a, b, sigma_b, n_b, mask=None) -> dict:
                 chi2_per_dof=chi2 / max(1, int(np.count_nonzero(mask))))
 
 
-def assert_chi2_consistent_batched(a, sigma_a, n_a, b, sigma_b, n_b, alpha=0.01, mask=None):
+RECORDS: list[dict] = []  # every comparison made with a `case` name, for the parity report
+
+
+def assert_chi2_consistent_batched(a, sigma_a, n_a, b, sigma_b, n_b, alpha=0.01, mask=None,
+                                   case: str | None = None):
     r = chi2_batched(a, sigma_a, n_a, b, sigma_b, n_b, mask)
+    if case is not None:
+        RECORDS.append({"case": case, "chi2_per_dof": r["chi2_per_dof"], "p": r["p_value"],
+                        "n_voxels": r["n"], "null_mean_per_dof": r["null_mean"] / max(1, r["n"]),
+                        "passed": r["p_value"] > alpha})
     assert r["p_value"] > alpha, (
         f"chi2={r['chi2']:.1f} vs batched-null mean {r['null_mean']:.1f} (sd {r['null_sd']:.1f}) "
         f"on {r['n']} voxels, p={r['p_value']:.2e} < alpha={alpha}. "

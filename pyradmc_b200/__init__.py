@@ -10,6 +10,8 @@ from pyradmc_b200.engine import B200Engine
 from pyradmc_b200.model import (
     AnalyticWaterTables,
     BeamletGridSource,
+    CompositeBeamletSource,
+    ConcatenatedBeamletSource,
     DijResult,
     ParallelBeamSource,
     PencilBeamSource,
@@ -26,6 +28,8 @@ __all__ = [
     "AnalyticWaterTables",
     "B200Engine",
     "BeamletGridSource",
+    "CompositeBeamletSource",
+    "ConcatenatedBeamletSource",
     "DijResult",
     "ParallelBeamSource",
     "PencilBeamSource",

@@ -21,10 +21,11 @@ PMC_ERR_STEP_CAP = -4
 PMC_ERR_CUDA = -5
 PMC_ERR_OOM = -6
 PMC_ERR_STATE = -7
+PMC_ERR_CAPACITY = -8
 
 PMC_PHOTON, PMC_ELECTRON, PMC_POSITRON = 0, 1, 2
 PMC_SRC_PENCIL, PMC_SRC_PARALLEL, PMC_SRC_SPECTRAL, PMC_SRC_UPLOAD = 0, 1, 2, 3
-PMC_BEAMLET_LATTICE, PMC_BEAMLET_SPECTRAL = 0, 1
+PMC_BEAMLET_LATTICE, PMC_BEAMLET_SPECTRAL, PMC_BEAMLET_RECORDS, PMC_BEAMLET_UPLOAD = 0, 1, 2, 3
 
 _dp = C.POINTER(C.c_double)
 _fp = C.POINTER(C.c_float)
@@ -103,6 +104,30 @@ class SourceDesc(C.Structure):
     ]
 
 
+SAMPLE_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int32, C.c_int64, C.c_int64,
+                        C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_float),
+                        C.POINTER(C.c_float))
+
+
+class BeamletRec(C.Structure):
+    _fields_ = [
+        ("type", C.c_int32),
+        ("spectrum", C.c_int32),
+        ("energy", C.c_double),
+        ("z0", C.c_double),
+        ("x_lo", C.c_double),
+        ("x_extent", C.c_double),
+        ("y_lo", C.c_double),
+        ("y_extent", C.c_double),
+        ("focal", _d3),
+        ("center", _d3),
+        ("u_axis", _d3),
+        ("v_axis", _d3),
+        ("width_u", C.c_double),
+        ("width_v", C.c_double),
+    ]
+
+
 class BeamletDesc(C.Structure):
     _fields_ = [
         ("type", C.c_int32),
@@ -123,6 +148,15 @@ class BeamletDesc(C.Structure):
         ("width_v", C.c_double),
         ("centers", _dp),
         ("history_offsets", _lp),
+        ("n_components", C.c_int32),
+        ("records", C.POINTER(BeamletRec)),
+        ("component_cdf", _dp),
+        ("n_spectra", C.c_int32),
+        ("spectrum_bins", C.POINTER(C.c_int32)),
+        ("spectrum_edges", _dp),
+        ("spectrum_cdf", _dp),
+        ("sample", SAMPLE_FN),
+        ("sample_user", C.c_void_p),
     ]
 
 
@@ -148,6 +182,8 @@ class RunParams(C.Structure):
         ("blocks_per_sm", C.c_int32),
         ("use_graph", C.c_int32),
         ("max_steps", C.c_int64),
+        ("tail_steps", C.c_int32),
+        ("smem_tables", C.c_int32),
     ]
 
 

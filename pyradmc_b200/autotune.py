@@ -1,5 +1,7 @@
 """Autotuner for the persistent transport launch: block size, resident blocks
-per SM and the primaries admitted per transport round.
+per SM, the primaries admitted per transport round, how long a particle may
+outlive its round's input before it is parked for the next round, and whether
+the table rows are staged in shared memory.
 
 The reference sizes its launches with fixed heuristics
 (``pyradmc/backends/warp/engine.py:175-255`` for the history chunk,
@@ -32,9 +34,12 @@ import numpy as np
 DEFAULT_CACHE = Path(os.environ.get("PYRADMC_B200_TUNE_CACHE",
                                     Path.home() / ".cache" / "pyradmc_b200" / "autotune.json"))
 BLOCK_SIZES = (128, 192, 256)
-BLOCKS_PER_SM = (None, 2)          # None: as many as the occupancy calculator allows
+BLOCKS_PER_SM = (None, 2, 3, 4)    # None: as many as the occupancy calculator allows;
+                                   # 3 and 4 also pick the kernels' register budget
 CHUNK_PER_THREAD = (8, 16, 32)     # admitted primaries per resident transport thread
 ASSUMED_BLOCKS_PER_SM = 3          # resident estimate for sizing the chunk candidates
+TAIL_STEPS = (None, 24, 256, 2048, -1)  # None: the library default; -1: never park
+SMEM_TABLES = (None, False)        # None: the library's choice (staged when they fit)
 
 _lock = threading.Lock()
 
@@ -42,25 +47,41 @@ _lock = threading.Lock()
 @dataclass(frozen=True)
 class LaunchShape:
     """None fields leave the engine's default (256 threads, occupancy-limited
-    residency, 16 primaries per resident thread)."""
+    residency, 16 primaries per resident thread, the library's parking
+    threshold and table placement)."""
 
     block_size: int | None
     blocks_per_sm: int | None
     chunk_size: int | None
+    tail_steps: int | None = None
+    smem_tables: bool | None = None
 
     def as_dict(self) -> dict:
         return dataclasses.asdict(self)
 
 
 def candidates(sm_count: int) -> list[LaunchShape]:
-    """The tuner's search space on a device with `sm_count` SMs; the engine's
-    default shape comes first, so tuning never picks a slower one."""
+    """The first search stage on a device with `sm_count` SMs (the launch
+    geometry); the engine's default shape comes first, so tuning never picks a
+    slower one."""
     out = [LaunchShape(None, None, None)]
     for bs in BLOCK_SIZES:
         for per_sm in BLOCKS_PER_SM:
             for m in CHUNK_PER_THREAD:
                 resident = sm_count * (per_sm or ASSUMED_BLOCKS_PER_SM) * bs
                 out.append(LaunchShape(bs, per_sm, int(m * resident)))
+    return out
+
+
+def refinements(best: LaunchShape) -> list[LaunchShape]:
+    """The second stage: the parking threshold and the table placement on top
+    of the best geometry (the best itself first)."""
+    out = [best]
+    for tail in TAIL_STEPS:
+        for smem in SMEM_TABLES:
+            shape = dataclasses.replace(best, tail_steps=tail, smem_tables=smem)
+            if shape not in out:
+                out.append(shape)
     return out
 
 
@@ -132,23 +153,29 @@ def tune(engine, source, counts, n_batches: int, seed: int, *, fraction: float =
     probe = probe_counts(counts, fraction, n_batches)
     report = {"key": key, "cached": False, "probe_histories": int(probe.sum()), "timings": []}
     best, best_t, reference = None, math.inf, None
-    for shape in (shapes or candidates(sms)):
-        trial = dataclasses.replace(engine, **shape.as_dict())
-        times = []
-        for _ in range(repeats):
-            seconds, dij = timer(trial, source, probe, n_batches, seed)
-            times.append(seconds)
-            d = digest(dij)
-            if reference is None:
-                reference = d
-            elif d != reference:
-                raise RuntimeError(f"launch shape {shape} changed the Dij: the transport is not "
-                                   "scheduling-inert")
-        t = float(np.median(times))
-        report["timings"].append({**shape.as_dict(), "seconds": t})
-        if t < best_t:
-            best, best_t = shape, t
-        trial.drop_uploads()
+    timed: dict = {}
+    stages = [shapes] if shapes else [candidates(sms), None]
+    for stage in stages:
+        for shape in (stage if stage is not None else refinements(best)):
+            if shape in timed:
+                continue
+            trial = dataclasses.replace(engine, **shape.as_dict())
+            times = []
+            for _ in range(repeats):
+                seconds, dij = timer(trial, source, probe, n_batches, seed)
+                times.append(seconds)
+                d = digest(dij)
+                if reference is None:
+                    reference = d
+                elif d != reference:
+                    raise RuntimeError(f"launch shape {shape} changed the Dij: the transport is "
+                                       "not scheduling-inert")
+            t = float(np.median(times))
+            timed[shape] = t
+            report["timings"].append({**shape.as_dict(), "seconds": t})
+            if t < best_t:
+                best, best_t = shape, t
+            trial.drop_uploads()
     report["shape"] = best.as_dict()
     if cache is not None:
         store_cache(key, best, cache)

@@ -126,12 +126,13 @@ struct Rng {
 };
 
 // ---- queue slot: one particle, 64 bytes (four 16-byte vectors) --------------
-// meta = kind (bits 0-1) | primary (bit 2) | beamlet << 3.
+// meta = kind (bits 0-1) | primary (bit 2) | beamlet << 3; d.y carries the
+// steps a suspended particle has already taken (0 for a new one).
 struct __align__(16) Slot {
     float4 a;  // energy, weight, x, y
     float4 b;  // z, ux, uy, uz
     uint4 c;   // stream id_lo, id_hi, tag, ctr
-    uint4 d;   // meta, spare
+    uint4 d;   // meta, steps taken, spare
 };
 
 __device__ inline uint32_t pack_meta(int kind, int primary, int beamlet) {
@@ -267,16 +268,28 @@ __device__ __forceinline__ LogIdx log_index(float q, float log_min, float inv_dl
     return r;
 }
 
-__device__ __forceinline__ float lerp1(const float* v, LogIdx li) {
-    return __ldg(v + li.i) * (1.0f - li.w) + __ldg(v + li.i + 1) * li.w;
+// Table reads: kShared selects a copy staged in the block's shared memory
+// (plain loads) over the read-only global path (__ldg, which must never see a
+// shared-memory address).  The values are the same either way.
+template <bool kShared, typename T>
+__device__ __forceinline__ T ld_tab(const T* p) {
+    if constexpr (kShared) return *p;
+    else return __ldg(p);
 }
+
+template <bool kShared = false>
+__device__ __forceinline__ float lerp1(const float* v, LogIdx li) {
+    return ld_tab<kShared>(v + li.i) * (1.0f - li.w) + ld_tab<kShared>(v + li.i + 1) * li.w;
+}
+template <bool kShared = false>
 __device__ __forceinline__ float2 lerp2(const float2* v, LogIdx li) {
-    const float2 a = __ldg(v + li.i), b = __ldg(v + li.i + 1);
+    const float2 a = ld_tab<kShared>(v + li.i), b = ld_tab<kShared>(v + li.i + 1);
     const float u = 1.0f - li.w;
     return make_float2(a.x * u + b.x * li.w, a.y * u + b.y * li.w);
 }
+template <bool kShared = false>
 __device__ __forceinline__ float4 lerp4(const float4* v, LogIdx li) {
-    const float4 a = __ldg(v + li.i), b = __ldg(v + li.i + 1);
+    const float4 a = ld_tab<kShared>(v + li.i), b = ld_tab<kShared>(v + li.i + 1);
     const float u = 1.0f - li.w;
     return make_float4(a.x * u + b.x * li.w, a.y * u + b.y * li.w, a.z * u + b.z * li.w,
                        a.w * u + b.w * li.w);

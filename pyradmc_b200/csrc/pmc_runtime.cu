@@ -37,6 +37,15 @@ struct DevBuf {
     size_t bytes = 0;
 };
 
+// Launch shape of the primary generator and the two transport kernels.
+struct LaunchShape {
+    int grid_ph = 0, grid_el = 0, block = 0;
+    int grid_gen = 0;                 // primary generator, blocks of 256
+    bool smem = false;                // table rows staged in shared memory
+    int occ = 0;                      // register-budget variant (0, 3 or 4)
+    size_t smem_ph = 0, smem_el = 0;  // dynamic shared memory of each kernel
+};
+
 }  // namespace
 
 struct pmc_engine {
@@ -69,7 +78,10 @@ struct pmc_engine {
     // transport buffers
     DevBuf q[4];
     unsigned int q_capacity = 0;
-    DevBuf edep, s1, s2;
+    DevBuf edep, s1, s2;          // [columns][col_stride] quanta and float64 sums
+    DevBuf dirty, touched;        // sector bitmaps of edep / of the sums (pmc_reduce.cuh)
+    bool edep_clean = false;      // every quanta entry is zero (true after a completed run)
+    long long col_stride = 0;     // entries per column of the maps in the current call
     Sched* d_sched = nullptr;
     Counters* d_counters = nullptr;
     GenDesc* d_gen = nullptr;
@@ -84,8 +96,7 @@ struct pmc_engine {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t graph_exec = nullptr;
     cudaGraphConditionalHandle cond = 0;
-    int graph_grid[2] = {0, 0};
-    int graph_block = 0;
+    LaunchShape graph_shape;
     TransportParams graph_params{};
 
     // the CSC of the last Dij: indptr on the host, entries in out_* on the device
@@ -182,27 +193,57 @@ GridInfo make_grid(int nx, int ny, int nz, const double o[3], const double s[3])
     return g;
 }
 
-int transport_launch_shape(pmc_engine* e, const pmc_run_params* p, int* grid_ph, int* grid_el,
-                           int* block) {
+constexpr int kDefaultTailSteps = 96;  // steps after a round runs dry before a particle is parked
+
+// Kernel variants: tables in shared memory or not, and the register budget
+// (resident blocks of 256 per SM: 0 = each kernel's default, else 3 or 4).
+void* photon_fn(bool smem, int occ) {
+    if (occ == 4) return smem ? (void*)photon_kernel<true, 4> : (void*)photon_kernel<false, 4>;
+    return smem ? (void*)photon_kernel<true, 3> : (void*)photon_kernel<false, 3>;
+}
+void* electron_fn(bool smem, int occ) {
+    if (occ == 3) return smem ? (void*)electron_kernel<true, 3> : (void*)electron_kernel<false, 3>;
+    return smem ? (void*)electron_kernel<true, 4> : (void*)electron_kernel<false, 4>;
+}
+
+int transport_launch_shape(pmc_engine* e, const pmc_run_params* p, LaunchShape* L) {
     int bs = p->block_size > 0 ? p->block_size : 256;
     if (bs % 32 != 0 || bs > 256) return fail(e, PMC_ERR_INVALID, "block_size must be a multiple of 32 and <= 256");
+    const size_t rows = (size_t)e->tab.n_materials * (size_t)e->tab.n_points;
+    L->smem_ph = rows * sizeof(float4) + (size_t)e->tab.n_points * sizeof(float);
+    L->smem_el = rows * (sizeof(float4) + sizeof(float2));
+    // auto: stage when both kernels keep their register-limited residency
+    // (one material at 2048 nodes: 40 KB and 48 KB per block)
+    L->smem = p->smem_tables > 0 || (p->smem_tables == 0 && L->smem_ph <= 48 * 1024 && L->smem_el <= 48 * 1024);
+    if (!L->smem) L->smem_ph = L->smem_el = 0;
+    int max_smem = 0;
+    PMC_CUDA(e, cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, e->device));
+    L->occ = (p->blocks_per_sm == 3 || p->blocks_per_sm == 4) ? p->blocks_per_sm : 0;
+    if (L->smem && (L->smem_ph + 1024 > (size_t)max_smem || L->smem_el + 1024 > (size_t)max_smem))
+        return fail(e, PMC_ERR_INVALID, "tables of %d materials do not fit shared memory; use smem_tables=-1",
+                    e->tab.n_materials);
+    PMC_CUDA(e, cudaFuncSetAttribute(photon_fn(L->smem, L->occ), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L->smem_ph));
+    PMC_CUDA(e, cudaFuncSetAttribute(electron_fn(L->smem, L->occ), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L->smem_el));
     int per_sm_ph = 0, per_sm_el = 0;
-    PMC_CUDA(e, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_ph, photon_kernel, bs, 0));
-    PMC_CUDA(e, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_el, electron_kernel, bs, 0));
+    PMC_CUDA(e, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_ph, photon_fn(L->smem, L->occ), bs, L->smem_ph));
+    PMC_CUDA(e, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_el, electron_fn(L->smem, L->occ), bs, L->smem_el));
     if (p->blocks_per_sm > 0) {
         per_sm_ph = std::min(per_sm_ph, p->blocks_per_sm);
         per_sm_el = std::min(per_sm_el, p->blocks_per_sm);
     }
     per_sm_ph = std::max(per_sm_ph, 1);
     per_sm_el = std::max(per_sm_el, 1);
-    *grid_ph = per_sm_ph * e->sm_count;
-    *grid_el = per_sm_el * e->sm_count;
-    *block = bs;
+    int per_sm_gen = 0;
+    PMC_CUDA(e, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_gen, generate_kernel, 256, 0));
+    L->grid_gen = std::max(1, std::min(per_sm_gen, 4)) * e->sm_count;
+    L->grid_ph = per_sm_ph * e->sm_count;
+    L->grid_el = per_sm_el * e->sm_count;
+    L->block = bs;
     return PMC_OK;
 }
 
-// The drain graph: WHILE(remaining) { photon_kernel; electron_kernel }.
-int build_graph(pmc_engine* e, const TransportParams& P, int grid_ph, int grid_el, int block) {
+// The drain graph: WHILE(remaining) { generate_kernel; photon_kernel; electron_kernel }.
+int build_graph(pmc_engine* e, const TransportParams& P, const LaunchShape& L) {
     destroy_graph(e);
     PMC_CUDA(e, cudaGraphCreate(&e->graph, 0));
     PMC_CUDA(e, cudaGraphConditionalHandleCreate(&e->cond, e->graph, 1, cudaGraphCondAssignDefault));
@@ -218,20 +259,24 @@ int build_graph(pmc_engine* e, const TransportParams& P, int grid_ph, int grid_e
     e->graph_params = P;
     void* args[] = {&e->graph_params};
     cudaKernelNodeParams kp{};
-    kp.func = (void*)photon_kernel;
-    kp.gridDim = dim3(grid_ph);
-    kp.blockDim = dim3(block);
+    kp.func = (void*)generate_kernel;
+    kp.gridDim = dim3(L.grid_gen);
+    kp.blockDim = dim3(256);
     kp.sharedMemBytes = 0;
     kp.kernelParams = args;
-    cudaGraphNode_t n_ph, n_el;
-    PMC_CUDA(e, cudaGraphAddKernelNode(&n_ph, body, nullptr, 0, &kp));
-    kp.func = (void*)electron_kernel;
-    kp.gridDim = dim3(grid_el);
+    cudaGraphNode_t n_gen, n_ph, n_el;
+    PMC_CUDA(e, cudaGraphAddKernelNode(&n_gen, body, nullptr, 0, &kp));
+    kp.func = photon_fn(L.smem, L.occ);
+    kp.gridDim = dim3(L.grid_ph);
+    kp.blockDim = dim3(L.block);
+    kp.sharedMemBytes = (unsigned int)L.smem_ph;
+    PMC_CUDA(e, cudaGraphAddKernelNode(&n_ph, body, &n_gen, 1, &kp));
+    kp.func = electron_fn(L.smem, L.occ);
+    kp.gridDim = dim3(L.grid_el);
+    kp.sharedMemBytes = (unsigned int)L.smem_el;
     PMC_CUDA(e, cudaGraphAddKernelNode(&n_el, body, &n_ph, 1, &kp));
     PMC_CUDA(e, cudaGraphInstantiate(&e->graph_exec, e->graph, 0));
-    e->graph_grid[0] = grid_ph;
-    e->graph_grid[1] = grid_el;
-    e->graph_block = block;
+    e->graph_shape = L;
     return PMC_OK;
 }
 
@@ -281,9 +326,10 @@ int check_flags(pmc_engine* e, const Sched& s) {
 }
 
 struct RunPlan {
-    int grid_ph = 0, grid_el = 0, block = 0;
+    LaunchShape shape;
     unsigned long long budget = 0;
     long long max_steps = 0;
+    int tail_steps = 0;
 };
 
 // max_block: the most primaries one batch block of this call holds; admission
@@ -298,10 +344,10 @@ int prepare_transport(pmc_engine* e, const pmc_run_params* p, unsigned long long
     if (e->max_material >= e->tab.n_materials)
         return fail(e, PMC_ERR_INVALID, "material index %d beyond the cross-section source (%d materials)",
                     e->max_material, e->tab.n_materials);
-    int rc = transport_launch_shape(e, p, &plan->grid_ph, &plan->grid_el, &plan->block);
+    int rc = transport_launch_shape(e, p, &plan->shape);
     if (rc) return rc;
     const unsigned long long resident =
-        (unsigned long long)std::max(plan->grid_ph, plan->grid_el) * plan->block;
+        (unsigned long long)std::max(plan->shape.grid_ph, plan->shape.grid_el) * plan->shape.block;
     plan->budget = p->chunk_size > 0 ? (unsigned long long)p->chunk_size : 16ull * resident;
     plan->budget = std::max(1ull, std::min(plan->budget, max_block));
     const int qf = p->queue_factor > 0 ? p->queue_factor : 16;
@@ -317,6 +363,8 @@ int prepare_transport(pmc_engine* e, const pmc_run_params* p, unsigned long long
         e->q_capacity = cap;
     }
     plan->max_steps = p->max_steps > 0 ? p->max_steps : kDefaultMaxSteps;
+    plan->tail_steps = p->tail_steps > 0 ? p->tail_steps
+                       : p->tail_steps < 0 ? 0x7fffffff : kDefaultTailSteps;
     return PMC_OK;
 }
 
@@ -331,6 +379,8 @@ TransportParams make_params(pmc_engine* e, const pmc_run_params* p, const RunPla
     P.sched = e->d_sched;
     P.gen = e->d_gen;
     P.edep = (unsigned long long*)e->edep.p;
+    P.dirty = (unsigned int*)e->dirty.p;
+    P.col_stride = e->col_stride;
     P.counters = e->d_counters;
     P.seed_lo = (uint32_t)(p->seed & 0xffffffffull);
     P.seed_hi = (uint32_t)(p->seed >> 32);
@@ -342,7 +392,8 @@ TransportParams make_params(pmc_engine* e, const pmc_run_params* p, const RunPla
     P.msc_gs = p->msc_gs ? 1 : 0;
     P.dose_to_water = p->dose_to_water ? 1 : 0;
     P.split_n = p->photon_split_n > 1 ? p->photon_split_n : 1;
-    P.max_steps = plan.max_steps;
+    P.max_steps = (int)std::min<long long>(plan.max_steps, 0x7ffffffeLL);
+    P.tail_steps = plan.tail_steps;
     return P;
 }
 
@@ -352,11 +403,16 @@ int run_batch(pmc_engine* e, const pmc_run_params* p, const RunPlan& plan, Trans
     if (block == 0) return PMC_OK;
     const bool graph = p->use_graph != 0;
     if (graph) {
-        const bool same = e->graph_exec && e->graph_grid[0] == plan.grid_ph &&
-                          e->graph_grid[1] == plan.grid_el && e->graph_block == plan.block &&
+        const LaunchShape& g = e->graph_shape;
+        const LaunchShape& L = plan.shape;
+        const bool same = e->graph_exec && g.grid_ph == L.grid_ph && g.grid_el == L.grid_el &&
+                          g.grid_gen == L.grid_gen &&
+                          g.block == L.block && g.smem == L.smem && g.occ == L.occ &&
+                          g.smem_ph == L.smem_ph &&
+                          g.smem_el == L.smem_el &&
                           std::memcmp(&e->graph_params, &P, sizeof P) == 0;
         if (!same) {
-            int rc = build_graph(e, P, plan.grid_ph, plan.grid_el, plan.block);
+            int rc = build_graph(e, P, L);
             if (rc) return rc;
         }
     }
@@ -370,10 +426,15 @@ int run_batch(pmc_engine* e, const pmc_run_params* p, const RunPlan& plan, Trans
         return PMC_OK;
     }
     for (long long round = 0; round < kMaxRounds; ++round) {
-        photon_kernel<<<plan.grid_ph, plan.block, 0, e->stream>>>(P);
-        electron_kernel<<<plan.grid_el, plan.block, 0, e->stream>>>(P);
+        const LaunchShape& L = plan.shape;
+        generate_kernel<<<L.grid_gen, 256, 0, e->stream>>>(P);
+        void* args[] = {&P};
+        PMC_CUDA(e, cudaLaunchKernel(photon_fn(L.smem, L.occ), dim3(L.grid_ph), dim3(L.block), args,
+                                     L.smem_ph, e->stream));
+        PMC_CUDA(e, cudaLaunchKernel(electron_fn(L.smem, L.occ), dim3(L.grid_el), dim3(L.block),
+                                     args, L.smem_el, e->stream));
         PMC_CUDA(e, cudaGetLastError());
-        e->counters.transport_launches += 2;
+        e->counters.transport_launches += 3;
         Sched s;
         int rc = read_sched(e, &s);
         if (rc) return rc;
@@ -382,11 +443,21 @@ int run_batch(pmc_engine* e, const pmc_run_params* p, const RunPlan& plan, Trans
     return PMC_OK;
 }
 
+long long stride_for(long long n_vox) {
+    return (n_vox + kTileVoxels - 1) / kTileVoxels * kTileVoxels;
+}
+
+int reduce_blocks(long long n_tiles) {
+    return (int)((n_tiles + kReduceThreads / 32 - 1) / (kReduceThreads / 32));
+}
+
 int launch_fold(pmc_engine* e, long long n_vox, int group, const double* d_col_nhist) {
-    const dim3 grid((unsigned)((n_vox + kFoldChunk - 1) / kFoldChunk), (unsigned)group);
-    fold_kernel<<<grid, kReduceThreads, 0, e->stream>>>((unsigned long long*)e->edep.p, e->d_mass,
-                                                        d_col_nhist, n_vox, (double*)e->s1.p,
-                                                        (double*)e->s2.p, e->d_total_q);
+    const int tpc = (int)(e->col_stride / kTileVoxels);
+    const long long n_tiles = (long long)tpc * group;
+    fold_sparse_kernel<<<reduce_blocks(n_tiles), kReduceThreads, 0, e->stream>>>(
+        (unsigned long long*)e->edep.p, e->d_mass, d_col_nhist, n_vox, e->col_stride, tpc, n_tiles,
+        (double*)e->s1.p, (double*)e->s2.p, (unsigned int*)e->dirty.p,
+        (unsigned int*)e->touched.p, e->d_total_q);
     PMC_CUDA(e, cudaGetLastError());
     e->counters.reduce_launches += 1;
     return PMC_OK;
@@ -405,9 +476,11 @@ int launch_finalize(pmc_engine* e, long long n_vox, int group, int n_batches) {
     int rc = ensure_colmax(e, group);
     if (rc) return rc;
     PMC_CUDA(e, cudaMemsetAsync(e->d_colmax, 0, sizeof(unsigned long long) * group, e->stream));
-    const int n_tiles = (int)((n_vox + kTileVoxels - 1) / kTileVoxels);
-    finalize_kernel<<<dim3(n_tiles, group), kReduceThreads, 0, e->stream>>>(
-        (double*)e->s1.p, (double*)e->s2.p, n_vox, n_batches, e->d_colmax);
+    const int tpc = (int)(e->col_stride / kTileVoxels);
+    const long long n_tiles = (long long)tpc * group;
+    finalize_sparse_kernel<<<reduce_blocks(n_tiles), kReduceThreads, 0, e->stream>>>(
+        (double*)e->s1.p, (double*)e->s2.p, n_vox, e->col_stride, tpc, n_tiles, n_batches,
+        (const unsigned int*)e->touched.p, e->d_colmax);
     PMC_CUDA(e, cudaGetLastError());
     e->counters.reduce_launches += 1;
     return PMC_OK;
@@ -432,18 +505,18 @@ int grow_keep(pmc_engine* e, DevBuf& b, size_t bytes, size_t keep) {
 // Returns the group's entry total and per-column counts on the host.
 int truncate_count(pmc_engine* e, long long n_vox, int group, double truncation,
                    unsigned long long* nnz, std::vector<long long>* counts) {
-    const int n_tiles = (int)((n_vox + kTileVoxels - 1) / kTileVoxels);
-    const long long n_tc = (long long)n_tiles * group;
+    const int tpc = (int)(e->col_stride / kTileVoxels);
+    const long long n_tc = (long long)tpc * group;
     int rc = ensure(e, e->tile_counts, sizeof(unsigned int) * n_tc);
     if (!rc) rc = ensure(e, e->tile_offsets, sizeof(unsigned long long) * n_tc);
     if (!rc) rc = ensure(e, e->col_counts, sizeof(long long) * group);
     if (rc) return rc;
-    count_kept_kernel<<<dim3(n_tiles, group), kReduceThreads, 0, e->stream>>>(
-        (const double*)e->s1.p, n_vox, n_tiles, truncation, e->d_colmax,
-        (unsigned int*)e->tile_counts.p);
+    count_kept_sparse_kernel<<<reduce_blocks(n_tc), kReduceThreads, 0, e->stream>>>(
+        (const double*)e->s1.p, n_vox, e->col_stride, tpc, n_tc, truncation, e->d_colmax,
+        (const unsigned int*)e->touched.p, (unsigned int*)e->tile_counts.p);
     scan_tiles_kernel<<<1, 1024, 0, e->stream>>>(
         (const unsigned int*)e->tile_counts.p, n_tc, (unsigned long long*)e->tile_offsets.p, group,
-        n_tiles, (long long*)e->col_counts.p, e->d_nnz);
+        tpc, (long long*)e->col_counts.p, e->d_nnz);
     PMC_CUDA(e, cudaGetLastError());
     e->counters.reduce_launches += 2;
     counts->resize(group);
@@ -459,7 +532,8 @@ int truncate_count(pmc_engine* e, long long n_vox, int group, double truncation,
 // the device (earlier groups), in ascending voxel order per column.
 int truncate_compact(pmc_engine* e, long long n_vox, int group, double truncation,
                      unsigned long long nnz, const std::vector<long long>& counts) {
-    const int n_tiles = (int)((n_vox + kTileVoxels - 1) / kTileVoxels);
+    const int tpc = (int)(e->col_stride / kTileVoxels);
+    const long long n_tc = (long long)tpc * group;
     const size_t base = (size_t)e->csc_nnz;
     const size_t total = base + (size_t)nnz;
     int rc = grow_keep(e, e->out_idx, sizeof(long long) * total, sizeof(long long) * base);
@@ -467,11 +541,11 @@ int truncate_compact(pmc_engine* e, long long n_vox, int group, double truncatio
     if (!rc) rc = grow_keep(e, e->out_sigma, sizeof(double) * total, sizeof(double) * base);
     if (rc) return rc;
     if (nnz > 0) {
-        compact_kernel<<<dim3(n_tiles, group), kReduceThreads, 0, e->stream>>>(
-            (const double*)e->s1.p, (const double*)e->s2.p, n_vox, n_tiles, truncation,
-            e->d_colmax, (const unsigned long long*)e->tile_offsets.p,
-            (long long*)e->out_idx.p + base, (double*)e->out_dose.p + base,
-            (double*)e->out_sigma.p + base);
+        compact_sparse_kernel<<<reduce_blocks(n_tc), kReduceThreads, 0, e->stream>>>(
+            (const double*)e->s1.p, (const double*)e->s2.p, n_vox, e->col_stride, tpc, n_tc,
+            truncation, e->d_colmax, (const unsigned int*)e->touched.p,
+            (const unsigned long long*)e->tile_offsets.p, (long long*)e->out_idx.p + base,
+            (double*)e->out_dose.p + base, (double*)e->out_sigma.p + base);
         PMC_CUDA(e, cudaGetLastError());
         e->counters.reduce_launches += 1;
     }
@@ -480,12 +554,41 @@ int truncate_compact(pmc_engine* e, long long n_vox, int group, double truncatio
     return PMC_OK;
 }
 
-int ensure_dense(pmc_engine* e, long long n_entries) {
-    const size_t b = sizeof(double) * (size_t)n_entries;
-    int rc = ensure(e, e->edep, b);
-    if (!rc) rc = ensure(e, e->s1, b);
-    if (!rc) rc = ensure(e, e->s2, b);
+// The [group][stride] maps and their bitmaps, sized for `group` columns of
+// `n_vox` entries.  A freshly allocated quanta map is not yet zero.
+int ensure_maps(pmc_engine* e, int group, long long n_vox) {
+    e->col_stride = stride_for(n_vox);
+    const long long n = e->col_stride * group;
+    if (e->edep.bytes < sizeof(double) * (size_t)n) e->edep_clean = false;
+    int rc = ensure(e, e->edep, sizeof(double) * (size_t)n);
+    if (!rc) rc = ensure(e, e->s1, sizeof(double) * (size_t)n);
+    if (!rc) rc = ensure(e, e->s2, sizeof(double) * (size_t)n);
+    if (!rc) rc = ensure(e, e->dirty, sizeof(unsigned int) * (size_t)(n / kWordEntries));
+    if (!rc) rc = ensure(e, e->touched, sizeof(unsigned int) * (size_t)(n / kWordEntries));
     return rc;
+}
+
+// Start scoring `group` columns: quanta all zero (cleared in bulk only after a
+// run that did not complete), both bitmaps empty.  The float64 sums are not
+// cleared: a sector's first fold writes it whole.
+int begin_maps(pmc_engine* e, int group) {
+    if (!e->edep_clean) {
+        PMC_CUDA(e, cudaMemsetAsync(e->edep.p, 0, e->edep.bytes, e->stream));
+        e->edep_clean = true;
+    }
+    const size_t words = sizeof(unsigned int) * (size_t)(e->col_stride * group / kWordEntries);
+    PMC_CUDA(e, cudaMemsetAsync(e->dirty.p, 0, words, e->stream));
+    PMC_CUDA(e, cudaMemsetAsync(e->touched.p, 0, words, e->stream));
+    e->edep_clean = false;  // until every batch of the call has been folded
+    return PMC_OK;
+}
+
+int fill_bitmap(pmc_engine* e, DevBuf& b, int group, unsigned int v) {
+    const long long words = e->col_stride * group / kWordEntries;
+    fill_u32_kernel<<<std::max(1, (int)std::min<long long>(4 * e->sm_count, (words + 255) / 256)), 256, 0,
+                      e->stream>>>((unsigned int*)b.p, words, v);
+    PMC_CUDA(e, cudaGetLastError());
+    return PMC_OK;
 }
 
 int reset_counters(pmc_engine* e) {
@@ -504,7 +607,7 @@ int finish_counters(pmc_engine* e, pmc_books* books) {
         e->d2h_bytes += (unsigned long long)(sizeof s);
     PMC_CUDA(e, cudaStreamSynchronize(e->stream));
     e->counters.rounds = s.total_rounds;
-    e->counters.kernel_launches += 2 * s.total_rounds + e->counters.reduce_launches;
+    e->counters.kernel_launches += 3 * s.total_rounds + e->counters.reduce_launches;
     e->counters.photon_flights = (int64_t)c.flights;
     e->counters.photon_interactions = (int64_t)c.interactions;
     e->counters.electron_substeps = (int64_t)c.substeps;
@@ -537,6 +640,113 @@ int fill_gen_spectrum(pmc_engine* e, GenDesc& G, int n_bins, const double* edges
     int rc = upload_f32(e, ed, &G.edges);
     if (!rc) rc = upload_f32(e, cd, &G.cdf);
     return rc;
+}
+
+float int_bits(int v) {
+    float f;
+    std::memcpy(&f, &v, sizeof f);
+    return f;
+}
+
+// Append one spectrum as a segment of n_bins + 1 entries starting at the same
+// index in both arrays; returns that index.
+int append_spectrum(std::vector<float>* edges, std::vector<float>* cdf, int n_bins,
+                    const double* e_in, const double* c_in) {
+    const int first = (int)edges->size();
+    for (int k = 0; k <= n_bins; ++k) edges->push_back((float)e_in[k]);
+    for (int k = 0; k < n_bins; ++k) cdf->push_back((float)c_in[k]);
+    cdf->push_back(1.0f);  // unused: keeps the segments aligned
+    return first;
+}
+
+BeamletRec lattice_rec(double energy, double z0, double x_lo, double x_ext, double y_lo, double y_ext) {
+    BeamletRec r{};
+    r.a = make_float4((float)x_lo, (float)x_ext, (float)y_lo, (float)y_ext);
+    r.b = make_float4((float)z0, (float)energy, 0.0f, 0.0f);
+    r.d = make_float4(0.0f, 0.0f, 0.0f, int_bits(0));
+    return r;
+}
+
+BeamletRec fan_rec(const double focal[3], const double center[3], const double u[3], const double v[3],
+                   double width_u, double width_v, int first, int n_bins) {
+    BeamletRec r{};
+    r.a = make_float4((float)focal[0], (float)focal[1], (float)focal[2], (float)width_u);
+    r.b = make_float4((float)center[0], (float)center[1], (float)center[2], (float)width_v);
+    r.c = make_float4((float)u[0], (float)u[1], (float)u[2], int_bits(first));
+    r.d = make_float4((float)v[0], (float)v[1], (float)v[2], int_bits(1 | (n_bins << 1)));
+    return r;
+}
+
+// The per-beamlet records of an in-kernel beamlet source (nothing for the
+// upload route), its mixture selection and its spectra.
+int beamlet_records(pmc_engine* e, const pmc_beamlet_desc* src, std::vector<BeamletRec>* recs,
+                    int* n_comp, std::vector<float>* comp_cdf, std::vector<float>* edges,
+                    std::vector<float>* cdf) {
+    const int n = src->n_beamlets;
+    *n_comp = 1;
+    comp_cdf->assign(1, 1.0f);
+    switch (src->type) {
+        case PMC_BEAMLET_LATTICE:
+            if (!src->x_lo || !src->x_extent || !src->y_lo || !src->y_extent)
+                return fail(e, PMC_ERR_INVALID, "lattice source without bounds");
+            for (int j = 0; j < n; ++j)
+                recs->push_back(lattice_rec(src->energy, src->z0, src->x_lo[j], src->x_extent[j],
+                                            src->y_lo[j], src->y_extent[j]));
+            edges->assign(2, 0.0f);
+            cdf->assign(2, 1.0f);
+            return PMC_OK;
+        case PMC_BEAMLET_SPECTRAL: {
+            if (!src->centers) return fail(e, PMC_ERR_INVALID, "spectral beamlets without centres");
+            if (src->n_bins < 1 || !src->edges || !src->cdf)
+                return fail(e, PMC_ERR_INVALID, "spectral source without a spectrum");
+            const int first = append_spectrum(edges, cdf, src->n_bins, src->edges, src->cdf);
+            for (int j = 0; j < n; ++j)
+                recs->push_back(fan_rec(src->focal, src->centers + 3 * j, src->u_axis, src->v_axis,
+                                        src->width_u, src->width_v, first, src->n_bins));
+            return PMC_OK;
+        }
+        case PMC_BEAMLET_RECORDS: {
+            const int nc = src->n_components;
+            if (nc < 1 || !src->records) return fail(e, PMC_ERR_INVALID, "record source without records");
+            if (nc > 1 && !src->component_cdf)
+                return fail(e, PMC_ERR_INVALID, "a mixture needs its component cdf");
+            std::vector<int> first(std::max(src->n_spectra, 0));
+            for (int k = 0, at = 0; k < src->n_spectra; ++k) {
+                const int nb = src->spectrum_bins[k];
+                if (nb < 1) return fail(e, PMC_ERR_INVALID, "empty spectrum %d", k);
+                first[k] = append_spectrum(edges, cdf, nb, src->spectrum_edges + at + k,
+                                           src->spectrum_cdf + at);
+                at += nb;
+            }
+            if (edges->empty()) {
+                edges->assign(2, 0.0f);
+                cdf->assign(2, 1.0f);
+            }
+            *n_comp = nc;
+            comp_cdf->resize(nc);
+            for (int c = 0; c < nc; ++c) (*comp_cdf)[c] = nc > 1 ? (float)src->component_cdf[c] : 1.0f;
+            for (long long i = 0; i < (long long)n * nc; ++i) {
+                const pmc_beamlet_rec& r = src->records[i];
+                if (r.type == PMC_BEAMLET_LATTICE) {
+                    recs->push_back(lattice_rec(r.energy, r.z0, r.x_lo, r.x_extent, r.y_lo, r.y_extent));
+                } else if (r.type == PMC_BEAMLET_SPECTRAL) {
+                    if (r.spectrum < 0 || r.spectrum >= src->n_spectra)
+                        return fail(e, PMC_ERR_INVALID, "record %lld names spectrum %d of %d", i,
+                                    r.spectrum, src->n_spectra);
+                    recs->push_back(fan_rec(r.focal, r.center, r.u_axis, r.v_axis, r.width_u, r.width_v,
+                                            first[r.spectrum], src->spectrum_bins[r.spectrum]));
+                } else {
+                    return fail(e, PMC_ERR_INVALID, "record %lld has unknown type %d", i, r.type);
+                }
+            }
+            return PMC_OK;
+        }
+        case PMC_BEAMLET_UPLOAD:
+            if (!src->sample) return fail(e, PMC_ERR_INVALID, "upload source without a sampler");
+            return PMC_OK;
+        default:
+            return fail(e, PMC_ERR_INVALID, "unknown beamlet source type %d", src->type);
+    }
 }
 
 }  // namespace
@@ -792,7 +1002,7 @@ int pmc_run_forward(pmc_engine* e, const pmc_source_desc* src, const pmc_run_par
     int rc = prepare_transport(e, p, (unsigned long long)(p->n_histories / p->n_batches), &plan);
     if (rc) return rc;
     const long long n_vox = e->si.n_voxels;
-    rc = ensure_dense(e, n_vox);
+    rc = ensure_maps(e, 1, n_vox);
     if (rc) return rc;
     rc = ensure(e, e->col_nhist, sizeof(double));
     if (rc) return rc;
@@ -872,9 +1082,14 @@ int pmc_run_forward(pmc_engine* e, const pmc_source_desc* src, const pmc_run_par
 
     rc = reset_counters(e);
     if (rc) return rc;
-    PMC_CUDA(e, cudaMemsetAsync(e->edep.p, 0, sizeof(double) * n_vox, e->stream));
+    // The whole dense map goes back to the caller: zero sums, every sector
+    // marked touched (the fold then adds into them, finalize visits them all).
+    rc = begin_maps(e, 1);
+    if (rc) return rc;
     PMC_CUDA(e, cudaMemsetAsync(e->s1.p, 0, sizeof(double) * n_vox, e->stream));
     PMC_CUDA(e, cudaMemsetAsync(e->s2.p, 0, sizeof(double) * n_vox, e->stream));
+    rc = fill_bitmap(e, e->touched, 1, 0xffffffffu);
+    if (rc) return rc;
     PMC_CUDA(e, cudaMemsetAsync(e->d_total_q, 0, sizeof(unsigned long long), e->stream));
     TransportParams P = make_params(e, p, plan);
     float t_tr = 0.0f, t_red = 0.0f;
@@ -911,6 +1126,7 @@ int pmc_run_forward(pmc_engine* e, const pmc_source_desc* src, const pmc_run_par
     PMC_CUDA(e, cudaMemcpyAsync(&total_q, e->d_total_q, sizeof total_q, cudaMemcpyDeviceToHost, e->stream));
         e->d2h_bytes += (unsigned long long)(sizeof total_q);
     PMC_CUDA(e, cudaStreamSynchronize(e->stream));
+    e->edep_clean = true;  // every batch folded: every quanta entry consumed
     float c = 0;
     cudaEventElapsedTime(&c, e->ev[0], e->ev[1]);
     e->counters.transport_ms = t_tr;
@@ -944,19 +1160,27 @@ int pmc_run_dij(pmc_engine* e, const pmc_beamlet_desc* src, const int64_t* count
     int group = p->beamlet_group_size > 0 ? p->beamlet_group_size : 0;
     if (group == 0) {
         // Auto: the largest group whose dense maps (int64 quanta + two float64
-        // sums = 24 bytes per entry) fit half of the free memory.
+        // sums = 24 bytes per entry, plus the two sector bitmaps) fit half of
+        // the free memory, counting the maps this engine already holds.
         size_t free_b = 0, total_b = 0;
         PMC_CUDA(e, cudaMemGetInfo(&free_b, &total_b));
-        const double budget = 0.5 * (double)free_b;
-        group = (int)std::max(1.0, std::floor(budget / (24.0 * (double)n_vox)));
+        const double held = (double)(e->edep.bytes + e->s1.bytes + e->s2.bytes + e->dirty.bytes +
+                                     e->touched.bytes);
+        const double budget = 0.5 * ((double)free_b + held);
+        group = (int)std::max(1.0, std::floor(budget / (24.0625 * (double)stride_for(n_vox))));
         group = std::min(group, std::min(n_beam, 4096));
     }
     group = std::min(group, n_beam);
-    rc = ensure_dense(e, n_vox * group);
+    rc = ensure_maps(e, group, n_vox);
     if (!rc) rc = ensure(e, e->col_nhist, sizeof(double) * group);
     if (rc) return rc;
-    if (src->type != PMC_BEAMLET_LATTICE && src->type != PMC_BEAMLET_SPECTRAL)
-        return fail(e, PMC_ERR_INVALID, "unknown beamlet source type %d", src->type);
+    // Every in-kernel beamlet source becomes per-beamlet records; the upload
+    // route samples each batch on the host through the caller's callback.
+    std::vector<BeamletRec> recs;
+    std::vector<float> comp_cdf, spec_edges, spec_cdf;
+    int n_comp = 1;
+    rc = beamlet_records(e, src, &recs, &n_comp, &comp_cdf, &spec_edges, &spec_cdf);
+    if (rc) return rc;
 
     std::vector<long long> offset(n_beam);
     long long acc = 0;
@@ -992,54 +1216,56 @@ int pmc_run_dij(pmc_engine* e, const pmc_beamlet_desc* src, const int64_t* count
         if (!rc) rc = upload_vec(e, pre, &G.pb_prefix);
         if (!rc) rc = upload_vec(e, off, &G.hist_offset);
         if (rc) return rc;
-        if (src->type == PMC_BEAMLET_LATTICE) {
-            if (!src->x_lo || !src->x_extent || !src->y_lo || !src->y_extent)
-                return fail(e, PMC_ERR_INVALID, "lattice source without bounds");
-            G.type = 1;
-            G.energy = (float)src->energy;
-            G.z0 = (float)src->z0;
-            std::vector<float> a(gs), b(gs), c(gs), d(gs);
-            for (int k = 0; k < gs; ++k) {
-                a[k] = (float)src->x_lo[g0 + k];
-                b[k] = (float)src->x_extent[g0 + k];
-                c[k] = (float)src->y_lo[g0 + k];
-                d[k] = (float)src->y_extent[g0 + k];
-            }
-            rc = upload_f32(e, a, &G.x_lo);
-            if (!rc) rc = upload_f32(e, b, &G.x_ext);
-            if (!rc) rc = upload_f32(e, c, &G.y_lo);
-            if (!rc) rc = upload_f32(e, d, &G.y_ext);
-        } else {
-            if (!src->centers) return fail(e, PMC_ERR_INVALID, "spectral beamlets without centres");
-            G.type = 2;
+        std::vector<float> up_energy, up_pos, up_dir, up_weight;
+        if (src->type == PMC_BEAMLET_UPLOAD) {
+            G.type = 3;
             G.book_emitted = 1;
-            G.fx = (float)src->focal[0]; G.fy = (float)src->focal[1]; G.fz = (float)src->focal[2];
-            G.uax = (float)src->u_axis[0]; G.uay = (float)src->u_axis[1]; G.uaz = (float)src->u_axis[2];
-            G.vax = (float)src->v_axis[0]; G.vay = (float)src->v_axis[1]; G.vaz = (float)src->v_axis[2];
-            G.width_u = (float)src->width_u;
-            G.width_v = (float)src->width_v;
-            std::vector<float> cx(gs), cy(gs), cz(gs);
-            for (int k = 0; k < gs; ++k) {
-                cx[k] = (float)src->centers[3 * (g0 + k)];
-                cy[k] = (float)src->centers[3 * (g0 + k) + 1];
-                cz[k] = (float)src->centers[3 * (g0 + k) + 2];
-            }
-            rc = upload_f32(e, cx, &G.cx);
-            if (!rc) rc = upload_f32(e, cy, &G.cy);
-            if (!rc) rc = upload_f32(e, cz, &G.cz);
-            if (!rc) rc = fill_gen_spectrum(e, G, src->n_bins, src->edges, src->cdf);
+            const size_t n = (size_t)pre[gs];
+            up_energy.resize(n);
+            up_pos.resize(3 * n);
+            up_dir.resize(3 * n);
+            up_weight.resize(n);
+            rc = upload_f32(e, up_energy, &G.up_energy);  // sized once per group, filled per batch
+            if (!rc) rc = upload_f32(e, up_pos, &G.up_pos);
+            if (!rc) rc = upload_f32(e, up_dir, &G.up_dir);
+            if (!rc) rc = upload_f32(e, up_weight, &G.up_weight);
+        } else {
+            G.type = 4;
+            G.book_emitted = 1;
+            G.n_comp = n_comp;
+            std::vector<BeamletRec> slice(recs.begin() + (size_t)g0 * n_comp,
+                                          recs.begin() + (size_t)(g0 + gs) * n_comp);
+            rc = upload_vec(e, slice, &G.recs);
+            if (!rc) rc = upload_f32(e, comp_cdf, &G.comp_cdf);
+            if (!rc) rc = upload_f32(e, spec_edges, &G.edges);
+            if (!rc) rc = upload_f32(e, spec_cdf, &G.cdf);
         }
         if (rc) return rc;
         PMC_CUDA(e, cudaMemcpy(e->d_gen, &G, sizeof G, cudaMemcpyHostToDevice));
     e->h2d_bytes += (unsigned long long)(sizeof G);
         PMC_CUDA(e, cudaMemcpy(e->col_nhist.p, nh.data(), sizeof(double) * gs, cudaMemcpyHostToDevice));
     e->h2d_bytes += (unsigned long long)(sizeof(double) * gs);
-        const long long span = n_vox * gs;
-        PMC_CUDA(e, cudaMemsetAsync(e->edep.p, 0, sizeof(double) * span, e->stream));
-        PMC_CUDA(e, cudaMemsetAsync(e->s1.p, 0, sizeof(double) * span, e->stream));
-        PMC_CUDA(e, cudaMemsetAsync(e->s2.p, 0, sizeof(double) * span, e->stream));
+        rc = begin_maps(e, gs);
+        if (rc) return rc;
         TransportParams P = make_params(e, p, plan);
         for (int b = 0; b < p->n_batches; ++b) {
+            if (G.type == 3) {  // this batch's primaries, sampled on the host
+                for (int k = 0; k < gs; ++k) {
+                    const long long r0 = (long long)b * pb[k];
+                    const long long key = (p->correlated ? 0 : off[k]) + r0;
+                    const size_t at = (size_t)pre[k];
+                    if (src->sample(src->sample_user, g0 + k, key, pb[k], up_energy.data() + at,
+                                    up_pos.data() + 3 * at, up_dir.data() + 3 * at,
+                                    up_weight.data() + at) != 0)
+                        return fail(e, PMC_ERR_INVALID, "the host sampler failed for beamlet %d", g0 + k);
+                }
+                const size_t n = (size_t)pre[gs];
+                PMC_CUDA(e, cudaMemcpyAsync((void*)G.up_energy, up_energy.data(), 4 * n, cudaMemcpyHostToDevice, e->stream));
+                PMC_CUDA(e, cudaMemcpyAsync((void*)G.up_pos, up_pos.data(), 12 * n, cudaMemcpyHostToDevice, e->stream));
+                PMC_CUDA(e, cudaMemcpyAsync((void*)G.up_dir, up_dir.data(), 12 * n, cudaMemcpyHostToDevice, e->stream));
+                PMC_CUDA(e, cudaMemcpyAsync((void*)G.up_weight, up_weight.data(), 4 * n, cudaMemcpyHostToDevice, e->stream));
+                e->h2d_bytes += 32ull * n;
+            }
             PMC_CUDA(e, cudaEventRecord(e->ev[0], e->stream));
             rc = run_batch(e, p, plan, P, b, (unsigned long long)pre[gs]);
             if (rc) return rc;
@@ -1059,6 +1285,7 @@ int pmc_run_dij(pmc_engine* e, const pmc_beamlet_desc* src, const int64_t* count
         if (rc) return rc;
         rc = check_flags(e, s);
         if (rc) return rc;
+        e->edep_clean = true;  // every batch of the group folded: every quanta entry consumed
         // finalize + count + scan, then (after the entry total is known) compact;
         // device time only, the host read of the total in between excluded.
         unsigned long long g_nnz = 0;
@@ -1157,8 +1384,7 @@ int pmc_reduce_dense(pmc_engine* e, const int64_t* quanta, int32_t n_batches, in
     if (!e || !quanta || !voxel_mass || !histories_per_batch || !mean || !sigma) return PMC_ERR_INVALID;
     if (n_batches < 1 || n_cols < 1 || n_vox < 1) return fail(e, PMC_ERR_INVALID, "empty reduction");
     PMC_CUDA(e, cudaSetDevice(e->device));
-    const long long span = (long long)n_cols * n_vox;
-    int rc = ensure_dense(e, span);
+    int rc = ensure_maps(e, n_cols, n_vox);
     if (!rc) rc = ensure(e, e->col_nhist, sizeof(double) * n_cols);
     if (rc) return rc;
     // The reduction runs against the given masses, not the engine's scoring grid.
@@ -1170,21 +1396,23 @@ int pmc_reduce_dense(pmc_engine* e, const int64_t* quanta, int32_t n_batches, in
     PMC_CUDA(e, cudaMemcpy(e->col_nhist.p, histories_per_batch, sizeof(double) * n_cols, cudaMemcpyHostToDevice));
     e->h2d_bytes += (unsigned long long)(sizeof(double) * n_cols);
     e->d_mass = mass;
-    PMC_CUDA(e, cudaMemsetAsync(e->s1.p, 0, sizeof(double) * span, e->stream));
-    PMC_CUDA(e, cudaMemsetAsync(e->s2.p, 0, sizeof(double) * span, e->stream));
+    rc = begin_maps(e, n_cols);
     PMC_CUDA(e, cudaMemsetAsync(e->d_total_q, 0, sizeof(unsigned long long), e->stream));
+    const size_t row = sizeof(int64_t) * (size_t)n_vox, pitch = sizeof(int64_t) * (size_t)e->col_stride;
     for (int b = 0; b < n_batches && !rc; ++b) {
-        PMC_CUDA(e, cudaMemcpyAsync(e->edep.p, quanta + (size_t)b * span, sizeof(int64_t) * span,
-                                    cudaMemcpyHostToDevice, e->stream));
-        rc = launch_fold(e, n_vox, n_cols, (const double*)e->col_nhist.p);
+        // The host map is dense: every sector of it counts as deposited.
+        PMC_CUDA(e, cudaMemcpy2DAsync(e->edep.p, pitch, quanta + (size_t)b * n_cols * n_vox, row, row,
+                                      (size_t)n_cols, cudaMemcpyHostToDevice, e->stream));
+        rc = fill_bitmap(e, e->dirty, n_cols, 0xffffffffu);
+        if (!rc) rc = launch_fold(e, n_vox, n_cols, (const double*)e->col_nhist.p);
     }
     if (!rc) rc = launch_finalize(e, n_vox, n_cols, n_batches);
     unsigned long long tq = 0;
     if (!rc) {
-        cudaMemcpyAsync(mean, e->s1.p, sizeof(double) * span, cudaMemcpyDeviceToHost, e->stream);
-        cudaMemcpyAsync(sigma, e->s2.p, sizeof(double) * span, cudaMemcpyDeviceToHost, e->stream);
+        cudaMemcpy2DAsync(mean, row, e->s1.p, pitch, row, (size_t)n_cols, cudaMemcpyDeviceToHost, e->stream);
+        cudaMemcpy2DAsync(sigma, row, e->s2.p, pitch, row, (size_t)n_cols, cudaMemcpyDeviceToHost, e->stream);
         cudaMemcpyAsync(&tq, e->d_total_q, sizeof tq, cudaMemcpyDeviceToHost, e->stream);
-        cudaStreamSynchronize(e->stream);
+        if (cudaStreamSynchronize(e->stream) == cudaSuccess) e->edep_clean = true;
     }
     e->d_mass = saved_mass;
     cudaFree(mass);
@@ -1200,20 +1428,21 @@ int pmc_truncate_dense(pmc_engine* e, const double* mean, const double* sigma, i
     if (n_cols < 1 || n_vox < 1) return fail(e, PMC_ERR_INVALID, "empty truncation");
     if (truncation < 0.0) return fail(e, PMC_ERR_INVALID, "negative truncation %g", truncation);
     PMC_CUDA(e, cudaSetDevice(e->device));
-    const long long span = (long long)n_cols * n_vox;
-    int rc = ensure_dense(e, span);
+    int rc = ensure_maps(e, n_cols, n_vox);
     if (rc) return rc;
-    PMC_CUDA(e, cudaMemcpy(e->s1.p, mean, sizeof(double) * span, cudaMemcpyHostToDevice));
-    e->h2d_bytes += (unsigned long long)(sizeof(double) * span);
-    PMC_CUDA(e, cudaMemcpy(e->s2.p, sigma, sizeof(double) * span, cudaMemcpyHostToDevice));
-    e->h2d_bytes += (unsigned long long)(sizeof(double) * span);
+    const size_t row = sizeof(double) * (size_t)n_vox, pitch = sizeof(double) * (size_t)e->col_stride;
+    PMC_CUDA(e, cudaMemcpy2DAsync(e->s1.p, pitch, mean, row, row, (size_t)n_cols, cudaMemcpyHostToDevice, e->stream));
+    PMC_CUDA(e, cudaMemcpy2DAsync(e->s2.p, pitch, sigma, row, row, (size_t)n_cols, cudaMemcpyHostToDevice, e->stream));
+    e->h2d_bytes += (unsigned long long)(2 * row * n_cols);
+    rc = fill_bitmap(e, e->touched, n_cols, 0xffffffffu);  // a dense map: every sector counts
+    if (rc) return rc;
     rc = ensure_colmax(e, n_cols);
     if (rc) return rc;
     PMC_CUDA(e, cudaMemsetAsync(e->d_colmax, 0, sizeof(unsigned long long) * n_cols, e->stream));
     {
-        const int n_tiles = (int)((n_vox + kTileVoxels - 1) / kTileVoxels);
+        const int n_tiles = (int)(e->col_stride / kTileVoxels);
         colmax_kernel<<<dim3(n_tiles, n_cols), kReduceThreads, 0, e->stream>>>(
-            (const double*)e->s1.p, n_vox, e->d_colmax);
+            (const double*)e->s1.p, n_vox, e->col_stride, e->d_colmax);
         PMC_CUDA(e, cudaGetLastError());
     }
     e->dij_indptr.assign(1, 0);
@@ -1236,13 +1465,13 @@ int pmc_truncate_dense(pmc_engine* e, const double* mean, const double* sigma, i
 // Allocation-free truncation + CSC compaction (pmc_dij_compact_static)
 // ============================================================================
 // Some callers cannot call cudaMalloc: an application that owns all device
-// memory through its own pool or allocator, a process that forbids allocation
-// after start-up so its footprint stays fixed, or a caller recording work into
-// a CUDA graph, where an allocation would break the capture.  For them the
+// memory through its own pool or allocator, or a process that forbids
+// allocation after start-up so its footprint stays fixed.  For them the
 // truncation + compaction scratch (column maxima, per-tile counts and offsets,
 // per-column counts, the entry total) lives in this file-scope device array
 // instead of engine-owned buffers.  Every GPU that loads the library holds it
-// until the process exits.
+// until the process exits.  The call reads the entry total back to the host
+// and synchronizes its stream, so it cannot be recorded into a CUDA graph.
 namespace {
 
 constexpr int kStaticMaxCols = 4096;
@@ -1265,7 +1494,8 @@ std::mutex g_scratch_mutex;
 
 // Host code cannot use g_static_scratch's address directly (on the host the
 // name is only a stand-in for the device symbol), so the device address is
-// looked up once per device, with that device current.
+// looked up once per device, with that device current, and kept for the life
+// of the process (a cudaDeviceReset of the device would invalidate it).
 cudaError_t static_scratch(int device, StaticScratch** out) {
     std::lock_guard<std::mutex> lock(g_scratch_mutex);
     if (device < 0 || device >= kStaticMaxDevices) return cudaErrorInvalidDevice;
@@ -1291,9 +1521,9 @@ int pmc_dij_compact_static(const double* mean, const double* sigma, int32_t n_co
         return PMC_ERR_INVALID;
     if (!(truncation >= 0.0)) return PMC_ERR_INVALID;
     const long long n_tiles = (n_vox + kTileVoxels - 1) / kTileVoxels;
-    if (n_cols > kStaticMaxCols || n_tiles * n_cols > kStaticMaxTiles || n_tiles > 65535)
+    if (n_cols > kStaticMaxCols || n_tiles * n_cols > kStaticMaxTiles)
         return PMC_ERR_INVALID;  // beyond the static scratch: at most 4096 columns and
-                                 // 262144 tiles of 4096 voxels, 65535 tiles per column
+                                 // 262144 tiles of 4096 voxels
     int device = 0;
     if (cudaGetDevice(&device) != cudaSuccess) return PMC_ERR_CUDA;
     StaticScratch* scratch = nullptr;
@@ -1303,7 +1533,7 @@ int pmc_dij_compact_static(const double* mean, const double* sigma, int32_t n_co
     if (cudaMemsetAsync(scratch->col_max, 0, sizeof(unsigned long long) * n_cols, st) != cudaSuccess)
         return PMC_ERR_CUDA;
     const dim3 grid((unsigned)n_tiles, (unsigned)n_cols);
-    colmax_kernel<<<grid, kReduceThreads, 0, st>>>(mean, n_vox, scratch->col_max);
+    colmax_kernel<<<grid, kReduceThreads, 0, st>>>(mean, n_vox, n_vox, scratch->col_max);
     count_kept_kernel<<<grid, kReduceThreads, 0, st>>>(mean, n_vox, (int)n_tiles, truncation,
                                                         scratch->col_max, scratch->tile_counts);
     scan_tiles_kernel<<<1, 1024, 0, st>>>(scratch->tile_counts, n_tiles * n_cols,
@@ -1315,7 +1545,8 @@ int pmc_dij_compact_static(const double* mean, const double* sigma, int32_t n_co
         cudaStreamSynchronize(st) != cudaSuccess)
         return PMC_ERR_CUDA;
     *nnz = (int64_t)total;
-    if ((long long)total > out_capacity) return PMC_ERR_INVALID;  // *nnz tells the size needed
+    // Too small: report the size needed; neither out_* nor col_counts is written.
+    if ((long long)total > out_capacity) return PMC_ERR_CAPACITY;
     if (total > 0) {
         if (!out_indices || !out_dose || !out_sigma) return PMC_ERR_INVALID;
         compact_kernel<<<grid, kReduceThreads, 0, st>>>(

@@ -21,6 +21,7 @@
 
 #include "pmc_common.cuh"
 #include "pmc_physics.cuh"
+#include "pmc_reduce.cuh"
 
 namespace pmc {
 
@@ -50,9 +51,22 @@ struct Sched {
     unsigned long long cond_handle; // CUDA graph conditional handle (0: host loop)
 };
 
+// One beamlet (or one mixture component of a beamlet) of the record
+// generator, 64 bytes:
+//   lattice: a = (x_lo, x_extent, y_lo, y_extent), b = (z0, energy, -, -)
+//   fan:     a = (focal, width_u), b = (aperture centre, width_v),
+//            c = (u axis, first spectrum entry), d = (v axis, -)
+// d.w holds the kind (0 lattice, 1 fan) in bit 0 and the fan's spectrum bin
+// count above it, as integer bits.  Spectra are concatenated in segments of
+// n_bins + 1 entries that start at the same index in the edge and the
+// cumulative arrays (the cumulative segment's last entry is unused).
+struct __align__(16) BeamletRec {
+    float4 a, b, c, d;
+};
+
 // Primary generator of the current group (device-resident).
 struct GenDesc {
-    int type;           // 0 pencil, 1 parallel/lattice, 2 spectral fan, 3 upload
+    int type;           // 0 pencil, 1 parallel/lattice, 2 spectral fan, 3 upload, 4 records
     int kind;           // particle kind of analytic primaries
     int forward;        // 1: open-field run (history = batch * per_batch + t)
     int correlated;
@@ -83,6 +97,9 @@ struct GenDesc {
     const float* up_dir;
     const float* up_weight;
     int book_emitted;                    // spectral/upload: book emitted energy per primary
+    const BeamletRec* recs;              // records: [group][n_comp]
+    const float* comp_cdf;               // records: [n_comp] mixture selection
+    int n_comp;
 };
 
 struct Counters {
@@ -99,7 +116,9 @@ struct TransportParams {
     unsigned int capacity;
     Sched* sched;
     const GenDesc* gen;
-    unsigned long long* edep;  // [group][n_scoring_voxels] int64 quanta
+    unsigned long long* edep;  // [group][col_stride] int64 quanta
+    unsigned int* dirty;       // sector bitmap of edep (pmc_reduce.cuh)
+    long long col_stride;      // entries per column: scoring voxels rounded up to a tile
     Counters* counters;
     uint32_t seed_lo, seed_hi;
     float pcut, ecut;
@@ -109,7 +128,8 @@ struct TransportParams {
     int msc_gs;
     int dose_to_water;
     int split_n;
-    long long max_steps;
+    int max_steps;
+    int tail_steps;       // steps a lane may still take once its round's input ran dry
 };
 
 // ---- per-block books ------------------------------------------------------------
@@ -141,11 +161,14 @@ __device__ __forceinline__ float spr_factor(const TransportParams& P, float e, i
 // next deposit into it when it lands in the same entry — an electron's two
 // half-substep deposits and its next substep's usually do — so a run of
 // deposits into one voxel costs one atomic.  Integer sums: merging is exact.
+// Every atomic also marks its entry's sector in the dirty bitmap, the only
+// sectors the batch fold visits.
 struct DirectSink {
-    unsigned long long n = 0;  // atomics issued
+    unsigned int n = 0;  // atomics issued
     __device__ __forceinline__ void add(const TransportParams& P, long long flat,
                                         unsigned long long q) {
         atomicAdd(P.edep + flat, q);
+        mark_dirty(P.dirty, flat);
         ++n;
     }
 };
@@ -153,7 +176,7 @@ struct DirectSink {
 struct HeldSink {
     long long idx = -1;
     unsigned long long q = 0;
-    unsigned long long n = 0;
+    unsigned int n = 0;
     __device__ __forceinline__ void add(const TransportParams& P, long long flat,
                                         unsigned long long quanta) {
         if (flat == idx) {
@@ -167,6 +190,7 @@ struct HeldSink {
     __device__ __forceinline__ void release(const TransportParams& P) {
         if (q != 0ull) {
             atomicAdd(P.edep + idx, q);
+            mark_dirty(P.dirty, idx);
             ++n;
         }
         idx = -1;
@@ -225,7 +249,7 @@ __device__ inline void deposit_spread(const TransportParams& P, BlockBooks& B, l
 __device__ __forceinline__ void queue_push(const TransportParams& P, int qi, int kind, int beamlet,
                                            float e, float w, float x, float y, float z, float ux,
                                            float uy, float uz, const StreamId& sid,
-                                           unsigned long long& n_push) {
+                                           unsigned int& n_push) {
     cg::coalesced_group g = cg::coalesced_threads();
     unsigned int base = 0;
     if (g.thread_rank() == 0) base = atomicAdd(&P.sched->count[qi], (unsigned int)g.size());
@@ -242,6 +266,13 @@ __device__ __forceinline__ void queue_push(const TransportParams& P, int qi, int
     s->c = make_uint4(sid.id_lo, sid.id_hi, sid.tag, sid.ctr);
     s->d = make_uint4(pack_meta(kind, 0, beamlet), 0u, 0u, 0u);
 }
+
+// Park an unfinished particle in queue qi for the next round: its whole state
+// (phase space, kind, primary flag, beamlet, stream position, steps taken)
+// goes into the slot, so the next round continues it exactly where it stopped.
+struct Particle;
+__device__ __forceinline__ void queue_suspend(const TransportParams& P, int qi, const Particle& p,
+                                              unsigned int& n_push);
 
 __device__ __forceinline__ unsigned long long fetch_one(unsigned long long* ctr) {
     cg::coalesced_group g = cg::coalesced_threads();
@@ -262,7 +293,7 @@ __device__ __forceinline__ unsigned int fetch_one(unsigned int* ctr) {
 struct Particle {
     float e, w, x, y, z, ux, uy, uz;
     int kind, primary, beamlet;
-    long long steps;
+    int steps;  // the host caps max_steps below 2^31
     Rng rng;
 };
 
@@ -276,8 +307,34 @@ __device__ __forceinline__ void load_slot(const TransportParams& P, const Slot* 
     p.kind = (int)(d.x & 3u);
     p.primary = (int)((d.x >> 2) & 1u);
     p.beamlet = (int)(d.x >> 3);
-    p.steps = 0;
+    p.steps = (int)d.y;
     p.rng.load(P.seed_lo, P.seed_hi, StreamId{c.x, c.y, c.z, c.w});
+}
+
+__device__ __forceinline__ void queue_suspend(const TransportParams& P, int qi, const Particle& p,
+                                              unsigned int& n_push) {
+    cg::coalesced_group g = cg::coalesced_threads();
+    unsigned int base = 0;
+    if (g.thread_rank() == 0) base = atomicAdd(&P.sched->count[qi], (unsigned int)g.size());
+    base = g.shfl(base, 0);
+    const unsigned int idx = base + g.thread_rank();
+    ++n_push;
+    if (idx >= P.capacity) {
+        atomicOr(&P.sched->flags, kFlagOverflow);
+        return;
+    }
+    Slot* s = P.q[qi] + idx;
+    const StreamId sid = p.rng.state();
+    s->a = make_float4(p.e, p.w, p.x, p.y);
+    s->b = make_float4(p.z, p.ux, p.uy, p.uz);
+    s->c = make_uint4(sid.id_lo, sid.id_hi, sid.tag, sid.ctr);
+    s->d = make_uint4(pack_meta(p.kind, p.primary, p.beamlet), (uint32_t)p.steps, 0u, 0u);
+}
+
+// Copy `n` table entries into the block's shared memory (strided over the block).
+template <typename T>
+__device__ __forceinline__ void stage(T* dst, const T* src, int n) {
+    for (int i = threadIdx.x; i < n; i += blockDim.x) dst[i] = __ldg(src + i);
 }
 
 // Vacuum flight to the grid for a particle born outside (photon.py:137-148);
@@ -369,16 +426,63 @@ __device__ inline int generate_primary(const TransportParams& P, const GenDesc& 
         const float inv = 1.0f / sqrtf(dx * dx + dy * dy + dz * dz);
         p.x = G.fx; p.y = G.fy; p.z = G.fz;
         p.ux = dx * inv; p.uy = dy * inv; p.uz = dz * inv;
-    } else {  // host-sampled record
-        p.kind = __ldg(G.up_kind + record);
-        p.e = __ldg(G.up_energy + record);
-        p.w = __ldg(G.up_weight + record);
-        p.x = __ldg(G.up_pos + 3 * record);
-        p.y = __ldg(G.up_pos + 3 * record + 1);
-        p.z = __ldg(G.up_pos + 3 * record + 2);
-        p.ux = __ldg(G.up_dir + 3 * record);
-        p.uy = __ldg(G.up_dir + 3 * record + 1);
-        p.uz = __ldg(G.up_dir + 3 * record + 2);
+    } else if (G.type == 4) {  // per-beamlet record (CompositeBeamletSource.emit for mixtures)
+        const BeamletRec* r = G.recs + (long long)local * G.n_comp;
+        if (G.n_comp > 1) {  // one uniform: the first component whose cdf reaches it
+            const float u = p.rng.uniform();
+            int lo = 0, hi = G.n_comp;
+            while (lo < hi) {
+                const int mid = (lo + hi) >> 1;
+                if (__ldg(G.comp_cdf + mid) < u) lo = mid + 1;
+                else hi = mid;
+            }
+            r += min(lo, G.n_comp - 1);
+        }
+        const float4 a = __ldg(&r->a), b = __ldg(&r->b);
+        const float4 d = __ldg(&r->d);
+        const int bits = __float_as_int(d.w);
+        p.kind = kPhoton;
+        if ((bits & 1) == 0) {  // lattice rectangle: two uniforms
+            p.e = b.y;
+            p.x = a.x + a.y * p.rng.uniform();
+            p.y = a.z + a.w * p.rng.uniform();
+            p.z = b.x;
+            p.ux = 0.0f; p.uy = 0.0f; p.uz = 1.0f;
+        } else {  // divergent fan through the aperture: four uniforms
+            const float4 c = __ldg(&r->c);
+            const int first = __float_as_int(c.w);
+            const int n_bins = bits >> 1;
+            const float u_bin = p.rng.uniform();
+            const float u_within = p.rng.uniform();
+            const float du = (p.rng.uniform() - 0.5f) * a.w;
+            const float dv = (p.rng.uniform() - 0.5f) * b.w;
+            int lo = 0, hi = n_bins;
+            while (lo < hi) {
+                const int mid = (lo + hi) >> 1;
+                if (__ldg(G.cdf + first + mid) < u_bin) lo = mid + 1;
+                else hi = mid;
+            }
+            const int k = first + min(lo, n_bins - 1);
+            const float e_lo = __ldg(G.edges + k);
+            p.e = e_lo + (__ldg(G.edges + k + 1) - e_lo) * u_within;
+            const float dx = b.x + du * c.x + dv * d.x - a.x;
+            const float dy = b.y + du * c.y + dv * d.y - a.y;
+            const float dz = b.z + du * c.z + dv * d.z - a.z;
+            const float inv = 1.0f / sqrtf(dx * dx + dy * dy + dz * dz);
+            p.x = a.x; p.y = a.y; p.z = a.z;
+            p.ux = dx * inv; p.uy = dy * inv; p.uz = dz * inv;
+        }
+    } else {  // host-sampled record: the run's history, or the batch block's slot t (Dij)
+        const long long ri = G.forward ? record : (long long)t;
+        p.kind = G.up_kind ? __ldg(G.up_kind + ri) : kPhoton;
+        p.e = __ldg(G.up_energy + ri);
+        p.w = __ldg(G.up_weight + ri);
+        p.x = __ldg(G.up_pos + 3 * ri);
+        p.y = __ldg(G.up_pos + 3 * ri + 1);
+        p.z = __ldg(G.up_pos + 3 * ri + 2);
+        p.ux = __ldg(G.up_dir + 3 * ri);
+        p.uy = __ldg(G.up_dir + 3 * ri + 1);
+        p.uz = __ldg(G.up_dir + 3 * ri + 2);
     }
     if (G.book_emitted) {
         const float latent = p.kind == kPositron ? 2.0f * kElectronMass : 0.0f;
@@ -391,7 +495,7 @@ __device__ inline int generate_primary(const TransportParams& P, const GenDesc& 
 template <class Sink>
 __device__ inline void annihilate_at_rest(const TransportParams& P, BlockBooks& B, Particle& p,
                                           long long base, int q_photon, float factor, Sink& sink,
-                                          unsigned long long& n_push) {
+                                          unsigned int& n_push) {
     if (P.pcut >= kElectronMass) {
         deposit(P, B, base, p.x, p.y, p.z, p.w * 2.0f * kElectronMass, factor, sink);
         return;
@@ -454,23 +558,39 @@ __device__ __forceinline__ void block_sum_add(unsigned long long* dst, unsigned 
 // ---- the photon kernel ---------------------------------------------------------------
 // One lane transports one photon to termination (Woodcock tracking), then takes
 // the next: queued photons first, then fresh primaries of the batch block.
-__global__ void __launch_bounds__(256, 3) photon_kernel(TransportParams P) {
+// kSmem: the channel rows of every material and the majorant row are staged in
+// the block's shared memory (dynamic, n_materials * n_points * 16 + n_points * 4
+// bytes) instead of being read through L1.
+// kMinBlocks: resident blocks of 256 per SM the register allocation targets
+// (3: 80 registers, no spill; 4: 64 registers, a few bytes spilled).
+template <bool kSmem, int kMinBlocks = 3>
+__global__ void __launch_bounds__(256, kMinBlocks) photon_kernel(TransportParams P) {
     __shared__ BlockBooks B;
-    init_books(B);
+    extern __shared__ __align__(16) unsigned char pmc_smem[];
+    const float4* tab_ch = P.tab.ch;
+    const float* tab_maj = P.tab.maj;
+    if constexpr (kSmem) {
+        const int n = P.tab.n_materials * P.tab.n_points;
+        float4* sch = reinterpret_cast<float4*>(pmc_smem);
+        float* smaj = reinterpret_cast<float*>(sch + n);
+        stage(sch, P.tab.ch, n);
+        stage(smaj, P.tab.maj, P.tab.n_points);
+        tab_ch = sch;
+        tab_maj = smaj;
+    }
+    init_books(B);  // its barrier also publishes the staged tables
     Sched* S = P.sched;
     const int pin = S->p_in, ein = S->e_in;
     const int q_in = pin, q_out = pin ^ 1, q_el = 2 + ein;
     const unsigned int n_in = min(S->count[q_in], P.capacity);
-    const unsigned long long limit = S->limit;
-    const int batch = S->batch;
-    const GenDesc& G = *P.gen;
     const Tables& T = P.tab;
     const float pcut = P.pcut, ecut = P.ecut;
 
-    unsigned long long n_flight = 0, n_inter = 0, n_push = 0, n_prim = 0;
+    unsigned int n_flight = 0, n_inter = 0, n_push = 0;  // per lane and launch
     DirectSink dep;
     Particle p;
-    bool active = false, exhausted = false;
+    bool active = false, exhausted = false, dry = false;
+    int tail = 0;  // steps of the current photon since its warp found the round dry
     float e_tab = -1.0f, maj = 0.0f;
     LogIdx li{0, 0.0f};
     int mat_tab = -1;
@@ -482,35 +602,29 @@ __global__ void __launch_bounds__(256, 3) photon_kernel(TransportParams P) {
             if (__any_sync(0xffffffffu, (*(volatile int*)&S->flags) & (kFlagOverflow | kFlagStepCap)))
                 break;
         }
-        if (!active && !exhausted) {
+        if (!active && !exhausted) {  // the round's photons: secondaries, parked, then primaries
             const unsigned int i = fetch_one(&S->head[q_in]);
-            bool got = false;
             if (i < n_in) {
                 load_slot(P, P.q[q_in], i, p);
-                got = true;
-            } else {
-                const unsigned long long t = fetch_one(&S->cursor);
-                if (t < limit) {
-                    ++n_prim;
-                    const int kind = generate_primary(P, G, batch, t, p, B);
-                    if (kind == kPhoton) {
-                        got = true;
-                    } else {  // charged primary: hand to the electron queue unchanged
-                        queue_push(P, q_el, kind, p.beamlet, p.e, p.w, p.x, p.y, p.z, p.ux, p.uy,
-                                   p.uz, p.rng.state(), n_push);
-                    }
-                } else {
-                    exhausted = true;
-                }
-            }
-            if (got) {
                 active = enter_grid(P, B, p, 0.0f);
-                base = (long long)p.beamlet * P.si.n_voxels;
+                base = (long long)p.beamlet * P.col_stride;
                 e_tab = -1.0f;
+                tail = 0;
+            } else {
+                exhausted = true;
             }
         }
         if (!__any_sync(0xffffffffu, active || !exhausted)) break;
+        if (!dry) dry = __any_sync(0xffffffffu, exhausted);
         if (!active) continue;
+        // Once the round's input has run dry, a photon that still needs more than
+        // tail_steps flights is parked for the next round instead of holding its
+        // warp (and its block's barrier) while every other lane idles.
+        if (dry && ++tail > P.tail_steps) {
+            queue_suspend(P, q_out, p, n_push);
+            active = false;
+            continue;
+        }
 
         // ---- one Woodcock flight (photon.py:150-181) ----
         if (++p.steps > P.max_steps) {
@@ -521,7 +635,7 @@ __global__ void __launch_bounds__(256, 3) photon_kernel(TransportParams P) {
         }
         if (p.e != e_tab) {
             li = log_index(p.e, T.p_log_min, T.p_inv_dlog, T.n_points);
-            maj = lerp1(T.maj, li);
+            maj = lerp1<kSmem>(tab_maj, li);
             e_tab = p.e;
             mat_tab = -1;
         }
@@ -539,7 +653,7 @@ __global__ void __launch_bounds__(256, 3) photon_kernel(TransportParams P) {
         const float rho = vx.x;
         const int mat = __float_as_int(vx.y);
         if (mat != mat_tab) {
-            ch = lerp4(T.ch + (long long)mat * T.n_points, li);
+            ch = lerp4<kSmem>(tab_ch + (long long)mat * T.n_points, li);
             mat_tab = mat;
         }
         const float mc = rho * ch.x, mp = rho * ch.y, mpa = rho * ch.z, mr = rho * ch.w;
@@ -678,27 +792,90 @@ __global__ void __launch_bounds__(256, 3) photon_kernel(TransportParams P) {
     block_sum_add(&B.interactions, n_inter);
     block_sum_add(&B.deposits, dep.n);
     block_sum_add(&B.pushes, n_push);
-    block_sum_add(&B.primaries, n_prim);
     flush_books(P, B);
 
-    // The last block retires the consumed photon queue and clamps the cursor.
+    // The last block retires the consumed photon queue; the round's admission
+    // window has been generated.
     if (last_block_arrives(S) && threadIdx.x == 0) {
         S->count[q_in] = 0u;
         S->head[q_in] = 0u;
         S->p_in = q_out;
-        if (S->cursor > S->limit) S->cursor = S->limit;
+        S->cursor = S->limit;
         S->blocks_done = 0u;
         __threadfence();
     }
+}
+
+// ---- the primary generator ---------------------------------------------------------
+// The round's admission window [cursor, limit) of the batch block, one thread
+// per primary (kernels.py:1888-2401): sampled at full warp width, flown
+// through vacuum to the grid, then queued with its stream position — photons
+// into the round's photon input queue behind the secondaries already there,
+// charged primaries into its electron queue.  The photon kernel then loads
+// every particle the same way, and no lane of it idles behind another's
+// primary sampling.
+__global__ void __launch_bounds__(256) generate_kernel(TransportParams P) {
+    __shared__ BlockBooks B;
+    init_books(B);
+    Sched* S = P.sched;
+    const unsigned long long cursor = S->cursor, limit = S->limit;
+    const int q_ph = S->p_in, q_el = 2 + S->e_in;
+    const int batch = S->batch;
+    const GenDesc& G = *P.gen;
+    unsigned int n_push = 0, n_prim = 0;
+    const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
+    for (unsigned long long t = cursor + (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
+         t < limit; t += stride) {
+        Particle p;
+        ++n_prim;
+        const int kind = generate_primary(P, G, batch, t, p, B);
+        if (kind == kPhoton) {
+            if (enter_grid(P, B, p, 0.0f)) queue_suspend(P, q_ph, p, n_push);
+        } else {  // charged primary: to the electron queue unchanged (it enters there)
+            queue_push(P, q_el, kind, p.beamlet, p.e, p.w, p.x, p.y, p.z, p.ux, p.uy, p.uz,
+                       p.rng.state(), n_push);
+        }
+    }
+    block_sum_add(&B.pushes, n_push);
+    block_sum_add(&B.primaries, n_prim);
+    flush_books(P, B);
+}
+
+__device__ __forceinline__ long long col_base(const TransportParams& P, const Particle& p) {
+    return (long long)p.beamlet * P.col_stride;
+}
+
+// Annihilation energy a positron still carries (2 m c^2), booked with it on escape.
+__device__ __forceinline__ float rest_energy(const Particle& p) {
+    return p.kind == kPositron ? 2.0f * kElectronMass : 0.0f;
 }
 
 // ---- the electron kernel -------------------------------------------------------------
 // One lane runs one electron or positron to ECUT (Class II condensed history,
 // electron.py:345-481); delta rays go to the next round's electron queue,
 // bremsstrahlung and annihilation photons to the next photon round.
-__global__ void __launch_bounds__(256, 4) electron_kernel(TransportParams P) {
+// kSmem: the (csda range, moller, restricted range, radiative stopping) and
+// (scattering power, log eta) rows of every material are staged in the block's
+// shared memory (n_materials * n_points * 24 bytes); the inverse-range row
+// (one read per substep) stays on the L1 path.
+// kMinBlocks: as for the photon kernel (4: 64 registers, a few bytes spilled;
+// 3: 85 registers, none).
+template <bool kSmem, int kMinBlocks = 4>
+__global__ void __launch_bounds__(256, kMinBlocks) electron_kernel(TransportParams P) {
     __shared__ BlockBooks B;
-    init_books(B);
+    extern __shared__ __align__(16) unsigned char pmc_smem[];
+    const float4* tab_ea = P.tab.ea;
+    const float2* tab_eb = P.tab.eb;
+    if constexpr (kSmem) {
+        const int n = P.tab.n_materials * P.tab.n_points;
+        float4* sea = reinterpret_cast<float4*>(pmc_smem);
+        float2* seb = reinterpret_cast<float2*>(sea + n);
+        stage(sea, P.tab.ea, n);
+        stage(seb, P.tab.eb, n);
+        tab_ea = sea;
+        tab_eb = seb;
+    }
+    init_books(B);  // its barrier also publishes the staged tables
     Sched* S = P.sched;
     const int pin = S->p_in, ein = S->e_in;
     const int q_in = 2 + ein, q_out = 2 + (ein ^ 1), q_ph = pin;
@@ -706,12 +883,13 @@ __global__ void __launch_bounds__(256, 4) electron_kernel(TransportParams P) {
     const Tables& T = P.tab;
     const float pcut = P.pcut, ecut = P.ecut;
 
-    unsigned long long n_sub = 0, n_push = 0;
+    unsigned int n_sub = 0, n_push = 0;  // per lane and launch
     HeldSink dep;
+    // The particle's column offset (col_base) is recomputed at each deposit
+    // instead of being held in two registers for the particle's whole life.
     Particle p;
-    bool active = false, exhausted = false;
-    float latent = 0.0f;
-    long long base = 0;
+    bool active = false, exhausted = false, dry = false;
+    int tail = 0;  // substeps of the current particle since its warp found the round dry
 
     for (unsigned int it = 0;; ++it) {
         if ((it & 255u) == 0u) {
@@ -723,27 +901,34 @@ __global__ void __launch_bounds__(256, 4) electron_kernel(TransportParams P) {
             const unsigned int i = fetch_one(&S->head[q_in]);
             if (i < n_in) {
                 load_slot(P, P.q[q_in], i, p);
-                latent = p.kind == kPositron ? 2.0f * kElectronMass : 0.0f;
-                base = (long long)p.beamlet * P.si.n_voxels;
-                active = enter_grid(P, B, p, latent);
+                active = enter_grid(P, B, p, rest_energy(p));
+                tail = 0;
             } else {
                 exhausted = true;
             }
         }
         if (!__any_sync(0xffffffffu, active || !exhausted)) break;
+        if (!dry) dry = __any_sync(0xffffffffu, exhausted);
         if (!active) continue;
+        // Park a particle that outlives the round's input by tail_steps substeps
+        // (its held deposit is released at the top of the next iteration).
+        if (dry && ++tail > P.tail_steps) {
+            queue_suspend(P, q_out, p, n_push);
+            active = false;
+            continue;
+        }
 
         if (++p.steps > P.max_steps) {
             atomicOr(&S->flags, kFlagStepCap);
-            escape(B, p.w * (p.e + latent));
+            escape(B, p.w * (p.e + rest_energy(p)));
             active = false;
             continue;
         }
         if (p.e <= ecut) {  // terminal: local deposit (electron.py:347-365)
             const int tm = __float_as_int(__ldg(P.vox + flat_index(p.x, p.y, p.z, P.gi)).y);
-            deposit(P, B, base, p.x, p.y, p.z, p.w * p.e, spr_factor(P, p.e, tm), dep);
+            deposit(P, B, col_base(P, p), p.x, p.y, p.z, p.w * p.e, spr_factor(P, p.e, tm), dep);
             if (p.kind == kPositron)
-                annihilate_at_rest(P, B, p, base, q_ph, spr_factor(P, kElectronMass, tm), dep,
+                annihilate_at_rest(P, B, p, col_base(P, p), q_ph, spr_factor(P, kElectronMass, tm), dep,
                                    n_push);
             active = false;
             continue;
@@ -756,11 +941,11 @@ __global__ void __launch_bounds__(256, 4) electron_kernel(TransportParams P) {
 
         // --- substep length ---
         const LogIdx le = log_index(p.e, T.e_log_min, T.e_inv_dlog, T.n_points);
-        const float4 A = lerp4(T.ea + row, le);  // csda, moller, restricted range, radiative
+        const float4 A = lerp4<kSmem>(tab_ea + row, le);  // csda, moller, restricted range, radiative
         const float range_cm = A.x / rho;
         float s_max = P.step_fraction * range_cm;
         if (!P.msc_gs) {
-            const float tp = lerp2(T.eb + row, le).x;
+            const float tp = lerp2<kSmem>(tab_eb + row, le).x;
             s_max = fminf(s_max, kHingeTheta2Max / (tp * rho));
         }
         const float s_boundary =
@@ -802,18 +987,18 @@ __global__ void __launch_bounds__(256, 4) electron_kernel(TransportParams P) {
         if (s > 0.0f) d1 = continuous * (s1 / s);
         const float d2 = continuous - d1;
 
-        deposit_spread(P, B, base, p.x, p.y, p.z, p.ux, p.uy, p.uz, s1, p.w * d1, factor, dep);
+        deposit_spread(P, B, col_base(P, p), p.x, p.y, p.z, p.ux, p.uy, p.uz, s1, p.w * d1, factor, dep);
         p.e -= d1;
         p.x += p.ux * s1;
         p.y += p.uy * s1;
         p.z += p.uz * s1;
         if (!point_inside(p.x, p.y, p.z, P.gi)) {
-            escape(B, p.w * (p.e + latent));
+            escape(B, p.w * (p.e + rest_energy(p)));
             active = false;
             continue;
         }
         const LogIdx lh = log_index(p.e, T.e_log_min, T.e_inv_dlog, T.n_points);
-        const float2 Bh = lerp2(T.eb + row, lh);  // scattering power, log eta
+        const float2 Bh = lerp2<kSmem>(tab_eb + row, lh);  // scattering power, log eta
         const float ms = Bh.x * rho * s;
         float cos_hinge;
         if (P.msc_gs) {
@@ -841,18 +1026,18 @@ __global__ void __launch_bounds__(256, 4) electron_kernel(TransportParams P) {
                                sid, n_push);
                 }
             } else {
-                deposit_or_escape(P, B, base, p.x, p.y, p.z, p.w * k, spr_factor(P, k, mat), dep);
+                deposit_or_escape(P, B, col_base(P, p), p.x, p.y, p.z, p.w * k, spr_factor(P, k, mat), dep);
             }
             p.e -= k;
         }
 
-        deposit_spread(P, B, base, p.x, p.y, p.z, p.ux, p.uy, p.uz, s2, p.w * d2, factor, dep);
+        deposit_spread(P, B, col_base(P, p), p.x, p.y, p.z, p.ux, p.uy, p.uz, s2, p.w * d2, factor, dep);
         p.e -= d2;
         p.x += p.ux * s2;
         p.y += p.uy * s2;
         p.z += p.uz * s2;
         if (!point_inside(p.x, p.y, p.z, P.gi)) {
-            escape(B, p.w * (p.e + latent));
+            escape(B, p.w * (p.e + rest_energy(p)));
             active = false;
             continue;
         }

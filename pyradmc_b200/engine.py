@@ -235,6 +235,175 @@ def merge_shards(parts):
         provenance=first.provenance)
 
 
+# ---- beamlet sources beyond the two built-in generators ------------------------------
+_IN_KERNEL_BEAMLETS = ("BeamletGridSource", "SpectralBeamletSource")
+
+
+def _simple_records(src, spectra: list) -> list | None:
+    """Per-beamlet record tuples of a built-in beamlet source (None otherwise);
+    `spectra` collects the distinct spectra the fans draw from."""
+    name = _type_name(src)
+    if name == "BeamletGridSource":
+        out = []
+        for j in range(int(src.n_beamlets)):
+            x0, x1, y0, y1 = src.beamlet_bounds(j)
+            out.append(("lattice", float(src.energy), float(src.z), x0, x1 - x0, y0, y1 - y0))
+        return out
+    if name == "SpectralBeamletSource":
+        k = next((i for i, sp in enumerate(spectra) if sp is src.spectrum), None)
+        if k is None:
+            spectra.append(src.spectrum)
+            k = len(spectra) - 1
+        return [("fan", k, tuple(src.focal_point), tuple(c), tuple(src.u_axis), tuple(src.v_axis),
+                 float(src.width_u), float(src.width_v)) for c in src.centers]
+    return None
+
+
+def _records_plan(source, spectra: list | None = None):
+    """(rows, component cdf or None, spectra) when every beamlet of `source`
+    is a built-in lattice rectangle or fan, or a fixed mixture of them
+    (CompositeBeamletSource); a ConcatenatedBeamletSource joins such parts when
+    they share one mixture.  None when the source needs host pre-sampling."""
+    spectra = [] if spectra is None else spectra
+    name = _type_name(source)
+    if name in _IN_KERNEL_BEAMLETS:
+        return [[r] for r in _simple_records(source, spectra)], None, spectra
+    if name == "CompositeBeamletSource":
+        comps = [_simple_records(c, spectra) for c in source._sources]
+        if any(c is None for c in comps):
+            return None
+        n = int(source.n_beamlets)
+        return [[c[j] for c in comps] for j in range(n)], np.asarray(source._cdf, float), spectra
+    if name == "ConcatenatedBeamletSource":
+        rows, cdf = [], None
+        for part in source.sources:
+            plan = _records_plan(part, spectra)
+            if plan is None:
+                return None
+            part_rows, part_cdf, _ = plan
+            if rows and (len(part_rows[0]) != len(rows[0]) or
+                         (part_cdf is None) != (cdf is None) or
+                         (cdf is not None and not np.array_equal(cdf, part_cdf))):
+                return None  # differently mixed parts: pre-sampled instead
+            rows += part_rows
+            cdf = part_cdf
+        return rows, cdf, spectra
+    return None
+
+
+def _fill_general_desc(desc, source, records, sl: slice, seed: int, keep: list) -> None:
+    """PMC_BEAMLET_RECORDS for `records`, else PMC_BEAMLET_UPLOAD through the
+    source's ``sample_beamlet_batch`` (the Warp engine's pre-sampling route,
+    engine.py:3224-3335), for the columns `sl` of the call."""
+    if records is not None:
+        rows, cdf, spectra = records
+        rows = rows[sl]
+        nc = len(rows[0])
+        arr = (_lib.BeamletRec * (len(rows) * nc))()
+        for i, row in enumerate(rows):
+            for c, r in enumerate(row):
+                rec = arr[i * nc + c]
+                if r[0] == "lattice":
+                    rec.type = _lib.PMC_BEAMLET_LATTICE
+                    rec.energy, rec.z0, rec.x_lo, rec.x_extent, rec.y_lo, rec.y_extent = r[1:]
+                else:
+                    rec.type = _lib.PMC_BEAMLET_SPECTRAL
+                    rec.spectrum = r[1]
+                    rec.focal[:], rec.center[:], rec.u_axis[:], rec.v_axis[:] = r[2:6]
+                    rec.width_u, rec.width_v = r[6], r[7]
+        bins = np.array([int(np.asarray(sp.cdf).size) for sp in spectra] or [0], dtype=np.int32)
+        edges = np.ascontiguousarray(np.concatenate([np.asarray(sp.edges, float) for sp in spectra])
+                                     if spectra else np.zeros(1))
+        cdfs = np.ascontiguousarray(np.concatenate([np.asarray(sp.cdf, float) for sp in spectra])
+                                    if spectra else np.zeros(1))
+        comp = np.ascontiguousarray(cdf if cdf is not None else np.ones(1))
+        keep += [arr, bins, edges, cdfs, comp]
+        desc.type = _lib.PMC_BEAMLET_RECORDS
+        desc.n_components = nc
+        desc.records = C.cast(arr, C.POINTER(_lib.BeamletRec))
+        desc.component_cdf = _lib.ptr(comp, C.c_double)
+        desc.n_spectra = len(spectra)
+        desc.spectrum_bins = _lib.ptr(bins, C.c_int32)
+        desc.spectrum_edges = _lib.ptr(edges, C.c_double)
+        desc.spectrum_cdf = _lib.ptr(cdfs, C.c_double)
+        return
+    first = sl.start or 0
+    errors: list = []
+
+    def sample(_user, beamlet, key_offset, n, energy, position, direction, weight):
+        try:
+            cols = source.sample_beamlet_batch(seed, int(key_offset), int(n), first + int(beamlet))
+            np.ctypeslib.as_array(energy, (n,))[:] = cols["energy"]
+            np.ctypeslib.as_array(weight, (n,))[:] = cols["weight"]
+            pos = np.ctypeslib.as_array(position, (n, 3))
+            dirs = np.ctypeslib.as_array(direction, (n, 3))
+            for k, (a, b) in enumerate((("x", "ux"), ("y", "uy"), ("z", "uz"))):
+                pos[:, k] = cols[a]
+                dirs[:, k] = cols[b]
+            return 0
+        except Exception as exc:  # reported after the call returns
+            errors.append(exc)
+            return 1
+
+    callback = _lib.SAMPLE_FN(sample)
+    keep += [callback, errors]
+    desc.type = _lib.PMC_BEAMLET_UPLOAD
+    desc.sample = callback
+
+
+def beamlet_arrays(source):
+    """(per-beamlet arrays of a built-in generator or None, records plan or None):
+    the host-side flattening of a beamlet source for ``pmc_run_dij``."""
+    name = _type_name(source)
+    n = int(source.n_beamlets)
+    if name == "BeamletGridSource":
+        bounds = np.array([source.beamlet_bounds(j) for j in range(n)], dtype=np.float64)
+        return dict(x_lo=bounds[:, 0], x_extent=bounds[:, 1] - bounds[:, 0],
+                    y_lo=bounds[:, 2], y_extent=bounds[:, 3] - bounds[:, 2]), None
+    if name == "SpectralBeamletSource":
+        return dict(centers=np.asarray(source.centers, dtype=np.float64).reshape(n, 3)), None
+    records = _records_plan(source)
+    if records is None and not hasattr(source, "sample_beamlet_batch"):
+        raise ValueError(f"unsupported beamlet source type {name}")
+    return None, records
+
+
+def beamlet_descriptor(source, sl: slice, seed: int, keep: list, per=None, records=None):
+    """The ``pmc_beamlet_desc`` of columns `sl` of `source` (the arrays it
+    points to are appended to `keep`, which must outlive the call)."""
+    if per is None and records is None:
+        per, records = beamlet_arrays(source)
+    desc = _lib.BeamletDesc(n_beamlets=sl.stop - sl.start)
+    name = _type_name(source)
+    if per is None:
+        _fill_general_desc(desc, source, records, sl, seed, keep)
+    elif name == "BeamletGridSource":
+        desc.type = _lib.PMC_BEAMLET_LATTICE
+        desc.energy = float(source.energy)
+        desc.z0 = float(source.z)
+        for key in ("x_lo", "x_extent", "y_lo", "y_extent"):
+            arr = np.ascontiguousarray(per[key][sl])
+            keep.append(arr)
+            setattr(desc, key, _lib.ptr(arr, C.c_double))
+    else:
+        spectrum = source.spectrum
+        edges = np.ascontiguousarray(spectrum.edges, dtype=np.float64)
+        cdf = np.ascontiguousarray(spectrum.cdf, dtype=np.float64)
+        centers = np.ascontiguousarray(per["centers"][sl])
+        keep += [edges, cdf, centers]
+        desc.type = _lib.PMC_BEAMLET_SPECTRAL
+        desc.n_bins = int(cdf.size)
+        desc.edges = _lib.ptr(edges, C.c_double)
+        desc.cdf = _lib.ptr(cdf, C.c_double)
+        desc.focal[:] = [float(v) for v in source.focal_point]
+        desc.u_axis[:] = [float(v) for v in source.u_axis]
+        desc.v_axis[:] = [float(v) for v in source.v_axis]
+        desc.width_u = float(source.width_u)
+        desc.width_v = float(source.width_v)
+        desc.centers = _lib.ptr(centers, C.c_double)
+    return desc
+
+
 def _device_dij(native: "_Native", n_cols: int, nnz: int, books) -> DeviceDij:
     indptr = np.zeros(n_cols + 1, dtype=np.int64)
     ptrs = [C.c_void_p() for _ in range(3)]
@@ -268,6 +437,14 @@ class B200Engine:
         Launch shape of the persistent transport kernels and whether each batch
         drains inside one CUDA graph (a conditional WHILE node) or under a host
         loop.  All bit-inert.
+    tail_steps
+        Steps a particle may still take once its transport round has no input
+        left before it is parked, state and all, for the next round (``None``:
+        the library default; a negative value never parks).  Bit-inert.
+    smem_tables
+        Stage the photon and electron table rows in each block's shared memory
+        (True), read them through L1 (False) or let the library decide (None).
+        Bit-inert: the same values either way.
     """
 
     grid: object
@@ -279,6 +456,8 @@ class B200Engine:
     blocks_per_sm: int | None = None
     use_graph: bool = True
     max_steps: int | None = None
+    tail_steps: int | None = None
+    smem_tables: bool | None = None
     _natives: dict = field(default_factory=dict, init=False, repr=False, compare=False)
     _table_cache: dict = field(default_factory=dict, init=False, repr=False, compare=False)
     _table_cache_lock: threading.Lock = field(
@@ -421,6 +600,8 @@ class B200Engine:
             blocks_per_sm=int(self.blocks_per_sm or 0),
             use_graph=1 if self.use_graph else 0,
             max_steps=int(self.max_steps or 0),
+            tail_steps=int(self.tail_steps or 0),
+            smem_tables=0 if self.smem_tables is None else (1 if self.smem_tables else -1),
         )
 
     def _provenance(self, seed, pcut, ecut, msc_model, step_energy_fraction,
@@ -744,16 +925,9 @@ class B200Engine:
             raise ValueError(f"column range {columns} outside 0..{n_beamlets}")
         if columns is not None and len(device_list) > 1:
             raise ValueError("a column range runs on one device")
-        if name == "BeamletGridSource":
-            bounds = np.array([source.beamlet_bounds(j) for j in range(n_beamlets)], dtype=np.float64)
-            per = dict(x_lo=bounds[:, 0], x_extent=bounds[:, 1] - bounds[:, 0],
-                       y_lo=bounds[:, 2], y_extent=bounds[:, 3] - bounds[:, 2])
-            energy_emitted = float(np.sum(counts[col_lo:col_hi])) * source.max_energy
-        elif name == "SpectralBeamletSource":
-            per = dict(centers=np.asarray(source.centers, dtype=np.float64).reshape(n_beamlets, 3))
-            energy_emitted = None
-        else:
-            raise ValueError(f"unsupported beamlet source type {name}")
+        per, records = beamlet_arrays(source)
+        energy_emitted = (float(np.sum(counts[col_lo:col_hi])) * source.max_energy
+                          if name == "BeamletGridSource" else None)
 
         params = self._params(
             n_batches=n_batches, seed=seed, pcut=pcut, ecut=ecut,
@@ -784,32 +958,8 @@ class B200Engine:
             while (g0 := next_group()) is not None:
                 g1 = min(g0 + span, col_hi)
                 sl = slice(g0, g1)
-                desc = _lib.BeamletDesc(n_beamlets=g1 - g0)
                 keep = []
-                if name == "BeamletGridSource":
-                    desc.type = _lib.PMC_BEAMLET_LATTICE
-                    desc.energy = float(source.energy)
-                    desc.z0 = float(source.z)
-                    for key in ("x_lo", "x_extent", "y_lo", "y_extent"):
-                        arr = np.ascontiguousarray(per[key][sl])
-                        keep.append(arr)
-                        setattr(desc, key, _lib.ptr(arr, C.c_double))
-                else:
-                    spectrum = source.spectrum
-                    edges = np.ascontiguousarray(spectrum.edges, dtype=np.float64)
-                    cdf = np.ascontiguousarray(spectrum.cdf, dtype=np.float64)
-                    centers = np.ascontiguousarray(per["centers"][sl])
-                    keep += [edges, cdf, centers]
-                    desc.type = _lib.PMC_BEAMLET_SPECTRAL
-                    desc.n_bins = int(cdf.size)
-                    desc.edges = _lib.ptr(edges, C.c_double)
-                    desc.cdf = _lib.ptr(cdf, C.c_double)
-                    desc.focal[:] = [float(v) for v in source.focal_point]
-                    desc.u_axis[:] = [float(v) for v in source.u_axis]
-                    desc.v_axis[:] = [float(v) for v in source.v_axis]
-                    desc.width_u = float(source.width_u)
-                    desc.width_v = float(source.width_v)
-                    desc.centers = _lib.ptr(centers, C.c_double)
+                desc = beamlet_descriptor(source, sl, seed, keep, per=per, records=records)
                 sub_counts = np.ascontiguousarray(counts[sl])
                 sub_offsets = np.ascontiguousarray(offsets[sl])
                 keep += [sub_counts, sub_offsets]
@@ -825,6 +975,9 @@ class B200Engine:
                                                C.byref(nnz), C.byref(books))
                     finally:
                         lib.pmc_set_progress(native.handle, None, None)
+                    for item in keep:  # an exception the host sampler raised inside the call
+                        if isinstance(item, list) and item and isinstance(item[0], Exception):
+                            raise item[0]
                     native.check(code)
                     if device_view:
                         return _device_dij(native, g1 - g0, nnz.value, books), None

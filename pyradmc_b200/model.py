@@ -13,6 +13,7 @@ same names, fields and semantics, so the same calls work:
 * :class:`Spectrum`             geometry/spectrum.py:34
 * :class:`SpectralBeamSource`   geometry/source.py:560
 * :class:`SpectralBeamletSource` geometry/source.py:637
+* :class:`CompositeBeamletSource` geometry/source.py:239
 * :class:`ScoringGrid`          scoring/grid.py:67 (``for_grid`` only)
 * :class:`RunProvenance`, :class:`TransportResult`  backends/results.py:19, :77
 * :class:`DijResult`            scoring/dij.py:195
@@ -38,6 +39,8 @@ import numpy as np
 __all__ = [
     "AnalyticWaterTables",
     "BeamletGridSource",
+    "CompositeBeamletSource",
+    "ConcatenatedBeamletSource",
     "DijResult",
     "ParallelBeamSource",
     "PencilBeamSource",
@@ -57,6 +60,7 @@ logger = logging.getLogger("pyradmc_b200.progress")
 
 DATA = Path(__file__).resolve().parent / "data"
 ELECTRON_MASS_MEV = 0.51099895069
+MAJORANT_HEADROOM = 1.0 + 1.0e-6  # data/tables.py:73
 GY_PER_MEV_PER_G = 1.602176634e-10
 WATER = 0
 
@@ -330,6 +334,84 @@ class SpectralBeamletSource:
     v_axis = property(lambda self: self._fan.v_axis)
 
 
+def _selection_cdf(weights) -> np.ndarray:
+    """Normalized cumulative mixture weights (geometry/source.py:192-202)."""
+    w = np.asarray(weights, dtype=np.float64)
+    if w.size == 0:
+        raise ValueError("a composite source needs at least one component")
+    if np.any(w < 0.0):
+        raise ValueError("component weights must be non-negative")
+    total = float(w.sum())
+    if total <= 0.0:
+        raise ValueError("component weights must sum to a positive value")
+    return np.cumsum(w) / total
+
+
+class CompositeBeamletSource:
+    """A per-beamlet mixture of beamlet sources (geometry/source.py:239-277):
+    every component describes the same beamlets, and beamlet ``j``'s primary
+    comes from the first component whose cumulative weight reaches one uniform
+    draw, then from that component's beamlet ``j``."""
+
+    def __init__(self, components) -> None:
+        if not components:
+            raise ValueError("a composite beamlet source needs at least one component")
+        self._sources = tuple(source for source, _ in components)
+        counts = {source.n_beamlets for source in self._sources}
+        if len(counts) != 1:
+            raise ValueError(f"all components must share n_beamlets, got {sorted(counts)}")
+        self._n_beamlets = counts.pop()
+        self._cdf = _selection_cdf([weight for _, weight in components])
+        self._max_energy = max(source.max_energy for source in self._sources)
+
+    max_energy = property(lambda self: self._max_energy)
+    n_beamlets = property(lambda self: self._n_beamlets)
+
+    def emit(self, beamlet: int, rng_state):
+        """One uniform picks the component, then it emits (only when the
+        components are pyRadMC objects with ``emit``)."""
+        from pyradmc.rng import uniform
+
+        index = min(int(np.searchsorted(self._cdf, uniform(rng_state))), len(self._sources) - 1)
+        return self._sources[index].emit(beamlet, rng_state)
+
+
+class ConcatenatedBeamletSource:
+    """Several beamlet sources as one Dij: the columns of ``sources[0]``, then
+    those of ``sources[1]``, ...  A treatment plan of several beams (each its
+    own focal spot and aperture axes) is one call, one set of persistent
+    launches and one CSC, where pyRadMC would run one ``run_dij`` per beam and
+    stack the matrices.  Beamlet ``j`` of the concatenation is beamlet
+    ``j - first(part)`` of its part, with the history and stream mapping of the
+    concatenated column index, so it also runs on pyRadMC's ReferenceEngine
+    when the parts are pyRadMC sources (``emit`` dispatches)."""
+
+    def __init__(self, sources) -> None:
+        self._sources = tuple(sources)
+        if not self._sources:
+            raise ValueError("a concatenation needs at least one beamlet source")
+        self._first = np.concatenate([[0], np.cumsum([int(s.n_beamlets) for s in self._sources])])
+
+    sources = property(lambda self: self._sources)
+    n_beamlets = property(lambda self: int(self._first[-1]))
+    max_energy = property(lambda self: max(float(s.max_energy) for s in self._sources))
+
+    def part_of(self, beamlet: int) -> tuple[int, int]:
+        """(part index, beamlet index within the part) of a concatenated column."""
+        if not 0 <= beamlet < self.n_beamlets:
+            raise IndexError(f"beamlet {beamlet} outside a concatenation of {self.n_beamlets}")
+        k = int(np.searchsorted(self._first, beamlet, side="right")) - 1
+        return k, beamlet - int(self._first[k])
+
+    def emit(self, beamlet: int, rng_state):
+        k, j = self.part_of(beamlet)
+        return self._sources[k].emit(j, rng_state)
+
+    def sample_beamlet_batch(self, seed: int, history_offset: int, n: int, beamlet: int):
+        k, j = self.part_of(beamlet)
+        return self._sources[k].sample_beamlet_batch(seed, history_offset, n, j)
+
+
 # ---- results ----------------------------------------------------------------------
 @dataclass(frozen=True)
 class RunProvenance:
@@ -539,7 +621,11 @@ class AnalyticWaterTables:
         for k in ("ecut", "pcut", "e_max", "photon_log_e_min", "photon_inv_dlog",
                   "electron_log_e_min", "electron_inv_dlog", "range_log_r_min", "range_inv_dlog"):
             fields[k] = float(fields[k])
-        fields["majorant"] = np.asarray(z["majorant"]) * self._rho_max
+        # AnalyticCrossSections.majorant (data/analytic.py:198-206) times the
+        # node headroom (data/tables.py:73, :272), in the reference's operation
+        # order: rho * ((compton + photoelectric) + pair), then * headroom.
+        mu_total = (np.asarray(z["mu_compton"][0]) + np.asarray(z["mu_photo"][0])) + np.asarray(z["mu_pair"][0])
+        fields["majorant"] = (self._rho_max * mu_total) * MAJORANT_HEADROOM
         return SimpleNamespace(**fields)
 
     def gs_grid_for(self, tables, materials: Sequence[int]):

@@ -19,7 +19,23 @@ for p in (str(ROOT), str(GOLDEN)):
     if p not in sys.path:
         sys.path.insert(0, p)
 
-from cases import CASES, SEED, layered_density  # noqa: E402
+from cases import CASES, CT_CASE, SEED, layered_density, make_source  # noqa: E402
+
+
+def pytest_sessionfinish(session, exitstatus):
+    """Write every named chi-squared comparison of the session ({case,
+    chi2_per_dof, p, n_voxels}) to $PMC_PARITY_REPORT, default
+    .parity/chi2.json at the repository root."""
+    import json
+    import os
+
+    from oracle import stats
+
+    if not stats.RECORDS:
+        return
+    path = Path(os.environ.get("PMC_PARITY_REPORT", ROOT / ".parity" / "chi2.json"))
+    path.parent.mkdir(parents=True, exist_ok=True)
+    path.write_text(json.dumps(stats.RECORDS, indent=1))
 
 
 def pytest_configure(config):
@@ -54,22 +70,28 @@ def build_case(name: str):
         grid = P.VoxelGrid(shape=g["shape"], spacing=g["spacing"],
                            density=layered_density(g["shape"], g["spacing"], (0, 0, 0), g["layers"]),
                            material=grid.material)
-    s = case["source"]
-    kind = s["kind"]
-    if kind == "parallel":
-        src = P.ParallelBeamSource(s["energy"], s["z"], s["x_range"], s["y_range"])
-    elif kind == "pencil":
-        src = P.PencilBeamSource(s["energy"], s["position"], s["direction"])
-    elif kind == "spectral":
-        src = P.SpectralBeamSource(P.ali_rogers_varian_6mv(), s["focal_point"], s["center"],
-                                   s["width_u"], s["width_v"])
-    elif kind == "lattice":
-        src = P.BeamletGridSource(s["energy"], s["z"], s["x_range"], s["y_range"], s["n_x"], s["n_y"])
-    else:
-        src = P.SpectralBeamletSource(P.ali_rogers_varian_6mv(), s["focal_point"], s["centers"],
-                                      s["width_u"], s["width_v"])
+    from types import SimpleNamespace
+
+    ns = SimpleNamespace(**{name: getattr(P, name) for name in (
+        "PencilBeamSource", "ParallelBeamSource", "SpectralBeamSource", "BeamletGridSource",
+        "SpectralBeamletSource", "CompositeBeamletSource")}, spectrum=P.ali_rogers_varian_6mv)
+    src = make_source(case["source"], ns)
     xs = P.AnalyticWaterTables(geometry_densities=grid.max_density_by_material())
     return grid, xs, src, dict(case["run"])
+
+
+def build_ct_case():
+    """(grid, cross_sections, source) of the scaled-down CT-like Dij case."""
+    import pyradmc_b200 as P
+    from pyradmc_b200 import phantoms
+
+    g = CT_CASE["grid"]
+    grid = phantoms.ellipsoid_phantom(shape=g["shape"], spacing=g["spacing"], seed=g["ellipsoid_seed"])
+    f = CT_CASE["fan"]
+    src = phantoms.beamlet_fan(grid, n_x=f["n_x"], n_y=f["n_y"], pitch=f["pitch"], width=f["width"],
+                               sad=f["sad"])
+    xs = P.AnalyticWaterTables(geometry_densities=grid.max_density_by_material())
+    return grid, xs, src
 
 
 def load_ref(name: str) -> dict:
@@ -77,4 +99,5 @@ def load_ref(name: str) -> dict:
         return {k: z[k] for k in z.files}
 
 
-__all__ = ["CASES", "GOLDEN", "ROOT", "SEED", "build_case", "cuda_available", "load_ref"]
+__all__ = ["CASES", "CT_CASE", "GOLDEN", "ROOT", "SEED", "build_case", "build_ct_case",
+           "cuda_available", "load_ref"]

@@ -47,11 +47,15 @@ CASES: dict[str, dict] = {
         source=dict(kind="pencil", energy=6.0, position=(8.0, 8.0, -1.0), direction=(0.0, 0.0, 1.0)),
         run=dict(n_histories=80000, n_batches=10, seed=20260726),
     ),
+    # 160,000 histories: enough that a 2 % bias in the lung or bone layer fails
+    # the batched chi-squared.  Generated as 16 one-batch shards (see
+    # make_golden.py), since the reference engine is single-threaded.
     "slab_spectral": dict(
         grid=dict(shape=(64, 64, 64), spacing=(0.2, 0.2, 0.2), layers=SLAB_LAYERS),
         source=dict(kind="spectral", focal_point=(6.4, 6.4, -100.0), center=(6.4, 6.4, 0.0),
                     width_u=10.0, width_v=10.0),
-        run=dict(n_histories=8000, n_batches=16, seed=SEED),
+        run=dict(n_histories=160_000, n_batches=16, seed=SEED),
+        shards=16,
     ),
     "dij_lattice": dict(
         grid=dict(shape=(8, 8, 16), spacing=(2.0, 2.0, 0.5)),
@@ -66,7 +70,67 @@ CASES: dict[str, dict] = {
                     width_u=1.5, width_v=1.5),
         run=dict(n_histories_per_beamlet=480, n_batches=8, seed=SEED, truncation=0.0),
     ),
+    # A fan entering through the -x face (its aperture axes y and z): the
+    # geometry of a beam of a coplanar plan at gantry angle 90 degrees.
+    "dij_oblique": dict(
+        grid=dict(shape=(16, 16, 16), spacing=(0.5, 0.5, 0.5)),
+        source=dict(kind="spectral_beamlets", focal_point=(-100.0, 4.0, 4.0),
+                    centers=((4.0, 3.0, 3.0), (4.0, 5.0, 3.0), (4.0, 3.0, 5.0), (4.0, 5.0, 5.0)),
+                    width_u=1.5, width_v=1.5, u_axis=(0.0, 1.0, 0.0), v_axis=(0.0, 0.0, 1.0)),
+        run=dict(n_histories_per_beamlet=8000, n_batches=8, seed=SEED, truncation=0.0),
+    ),
+    # A per-beamlet mixture (CompositeBeamletSource): beamlet j is 60 % the
+    # lattice rectangle j, 40 % the spectral fan j.
+    "dij_composite": dict(
+        grid=dict(shape=(8, 8, 16), spacing=(2.0, 2.0, 0.5)),
+        source=dict(kind="composite", components=(
+            (dict(kind="lattice", energy=6.0, z=-1.0, x_range=(2.0, 14.0), y_range=(2.0, 14.0),
+                  n_x=2, n_y=2), 0.6),
+            (dict(kind="spectral_beamlets", focal_point=(8.0, 8.0, -100.0),
+                  centers=((5.0, 5.0, 0.0), (5.0, 11.0, 0.0), (11.0, 5.0, 0.0), (11.0, 11.0, 0.0)),
+                  width_u=3.0, width_v=3.0), 0.4))),
+        run=dict(n_histories_per_beamlet=6400, n_batches=8, seed=SEED, truncation=0.0),
+    ),
 }
+
+
+def make_source(s: dict, ns):
+    """A case's source built from the classes of `ns` (pyRadMC's modules or this
+    package): PencilBeamSource, ParallelBeamSource, SpectralBeamSource,
+    BeamletGridSource, SpectralBeamletSource, CompositeBeamletSource and a
+    6 MV spectrum factory ``spectrum()``."""
+    kind = s["kind"]
+    if kind == "parallel":
+        return ns.ParallelBeamSource(s["energy"], s["z"], s["x_range"], s["y_range"])
+    if kind == "pencil":
+        return ns.PencilBeamSource(s["energy"], s["position"], s["direction"])
+    if kind == "spectral":
+        return ns.SpectralBeamSource(ns.spectrum(), s["focal_point"], s["center"], s["width_u"],
+                                     s["width_v"])
+    if kind == "lattice":
+        return ns.BeamletGridSource(s["energy"], s["z"], s["x_range"], s["y_range"], s["n_x"], s["n_y"])
+    if kind == "spectral_beamlets":
+        axes = {k: s[k] for k in ("u_axis", "v_axis") if k in s}
+        return ns.SpectralBeamletSource(ns.spectrum(), s["focal_point"], s["centers"], s["width_u"],
+                                        s["width_v"], **axes)
+    if kind == "composite":
+        return ns.CompositeBeamletSource([(make_source(c, ns), w) for c, w in s["components"]])
+    raise ValueError(kind)
+
+
+# Scaled-down batched-Dij case: the benchmark's CT-like phantom family (water
+# plus seeded ellipsoids of density U(0.2, 1.9), pyradmc_b200.phantoms) at
+# 40^3 x 2.5 mm, a 2x2 fan of 5 mm Varian 6 MV spectral beamlets at SAD 100 cm
+# through the phantom centre, GS multiple scattering.  The reference's run_dij
+# takes one count for every column, so it runs once per count of CT_COUNTS;
+# the B200 run gives the columns uneven counts and each column is compared
+# with the reference run at its own count (ref_ct_beamlets_<count>.npz).
+CT_CASE = dict(
+    grid=dict(shape=(40, 40, 40), spacing=(0.25, 0.25, 0.25), ellipsoid_seed=20260805),
+    fan=dict(n_x=2, n_y=2, pitch=0.5, width=0.5, sad=100.0),
+    run=dict(n_batches=10, seed=SEED, truncation=0.0),
+    counts=(40_000, 120_000),
+)
 
 
 def layered_density(shape, spacing, origin, layers):

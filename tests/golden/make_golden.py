@@ -14,9 +14,20 @@ It writes, next to this file:
     on them — ``BatchedBeamletScorer.end_batch``/``finalize`` (scoring/dij.py:
     155-191) and ``DijAssembler.add_block``/``finalize`` (:351-434) — the
     bit-exact pin of the device fold, finalize, truncation and compaction.
+``ref_ct_beamlets_<count>.npz``
+    ``ReferenceEngine.run_dij`` on the scaled-down CT-like Dij (``CT_CASE``),
+    once per per-beamlet count of ``CT_CASE["counts"]``.
 ``philox_kat.npz``
     Nothing from pyRadMC: the Philox4x32-10 known-answer vectors are checked in
     ``tests/test_oracle.py`` directly.
+
+Cases with ``shards`` (and the CT case) run as one process per statistical
+batch: shard ``k`` is a one-batch ``ReferenceEngine`` run with seed
+``seed * 100 + k``, and the shards' batch means are combined with the
+reference scorer's own formulas (``scoring/dose.py:169-207``: mean of the batch
+means, sigma from their sample variance).  That is exactly the estimate a
+single multi-batch run would give if its batch ``k`` drew those streams; it
+only spreads the single-threaded reference over the host's cores.
 
 pyRadMC's GS table cache lives under ``$HOME/.cache/pyradmc``; point ``HOME`` at
 a scratch directory.
@@ -33,20 +44,28 @@ import numpy as np
 HERE = Path(__file__).resolve().parent
 sys.path.insert(0, str(HERE))
 
-from cases import CASES, layered_density  # noqa: E402
+from cases import CASES, CT_CASE, layered_density, make_source  # noqa: E402
+
+REFERENCE: str | None = None  # path of the pyRadMC checkout, set by __main__ and the workers
+
+
+def _reference_sources():
+    from types import SimpleNamespace
+
+    import pyradmc.geometry.source as S
+    from pyradmc.geometry.spectrum import ali_rogers_mv
+
+    return SimpleNamespace(
+        PencilBeamSource=S.PencilBeamSource, ParallelBeamSource=S.ParallelBeamSource,
+        SpectralBeamSource=S.SpectralBeamSource, BeamletGridSource=S.BeamletGridSource,
+        SpectralBeamletSource=S.SpectralBeamletSource,
+        CompositeBeamletSource=S.CompositeBeamletSource,
+        spectrum=lambda: ali_rogers_mv("varian-6mv", e_min=0.1))
 
 
 def build_case(name: str):
     from pyradmc.data.analytic import AnalyticCrossSections
     from pyradmc.geometry.grid import VoxelGrid
-    from pyradmc.geometry.source import (
-        BeamletGridSource,
-        ParallelBeamSource,
-        PencilBeamSource,
-        SpectralBeamletSource,
-        SpectralBeamSource,
-    )
-    from pyradmc.geometry.spectrum import ali_rogers_mv
 
     case = CASES[name]
     g = case["grid"]
@@ -55,28 +74,151 @@ def build_case(name: str):
         density = layered_density(g["shape"], g["spacing"], (0.0, 0.0, 0.0), g["layers"])
         grid = VoxelGrid(shape=g["shape"], spacing=g["spacing"], density=density,
                          material=grid.material)
-    s = case["source"]
-    kind = s["kind"]
-    if kind == "parallel":
-        source = ParallelBeamSource(s["energy"], s["z"], s["x_range"], s["y_range"])
-    elif kind == "pencil":
-        source = PencilBeamSource(s["energy"], s["position"], s["direction"])
-    elif kind == "spectral":
-        source = SpectralBeamSource(ali_rogers_mv("varian-6mv", e_min=0.1), s["focal_point"],
-                                    s["center"], s["width_u"], s["width_v"])
-    elif kind == "lattice":
-        source = BeamletGridSource(s["energy"], s["z"], s["x_range"], s["y_range"], s["n_x"],
-                                   s["n_y"])
-    elif kind == "spectral_beamlets":
-        source = SpectralBeamletSource(ali_rogers_mv("varian-6mv", e_min=0.1), s["focal_point"],
-                                       s["centers"], s["width_u"], s["width_v"])
-    else:
-        raise ValueError(kind)
+    source = make_source(case["source"], _reference_sources())
     xs = AnalyticCrossSections(geometry_densities=grid.max_density_by_material())
     return grid, xs, source, case["run"]
 
 
+def _combine_batches(batch_means: np.ndarray):
+    """Mean and sigma of equal-weight batch means (scoring/dose.py:188-207)."""
+    n = batch_means.shape[0]
+    s1 = batch_means.sum(axis=0)
+    s2 = (batch_means**2).sum(axis=0)
+    mean = s1 / n
+    variance = np.maximum(0.0, s2 / n - mean**2) * n / (n - 1)
+    return mean, np.sqrt(variance / n)
+
+
+def _init_worker(reference: str) -> None:
+    global REFERENCE
+    REFERENCE = reference
+    sys.path.insert(0, reference)
+
+
+def _forward_shard(task):
+    name, k = task
+    from pyradmc.backends.ref.engine import ReferenceEngine
+    from pyradmc.rng.host import HostRNG
+
+    grid, xs, source, run = build_case(name)
+    shards = CASES[name]["shards"]
+    run = dict(run)
+    run["n_histories"] //= shards
+    run["n_batches"] = 1
+    run["seed"] = run["seed"] * 100 + k
+    res = ReferenceEngine(grid=grid, cross_sections=xs, rng=HostRNG()).run(source, **run)
+    books = (res.energy_emitted, res.energy_deposited, res.energy_escaped, res.energy_unscored)
+    return res.dose.reshape(-1), books
+
+
+def _ct_build():
+    from pyradmc.data.analytic import AnalyticCrossSections
+    from pyradmc.geometry.grid import VoxelGrid
+    from pyradmc.geometry.source import SpectralBeamletSource
+    from pyradmc.geometry.spectrum import ali_rogers_mv
+
+    sys.path.insert(0, str(HERE.parents[1]))
+    from pyradmc_b200 import phantoms
+
+    g = CT_CASE["grid"]
+    mirror = phantoms.ellipsoid_phantom(shape=g["shape"], spacing=g["spacing"], seed=g["ellipsoid_seed"])
+    grid = VoxelGrid(shape=g["shape"], spacing=g["spacing"], density=mirror.density,
+                     material=np.zeros(g["shape"], dtype=np.int32))
+    f = CT_CASE["fan"]
+    fan = phantoms.beamlet_fan(mirror, n_x=f["n_x"], n_y=f["n_y"], pitch=f["pitch"], width=f["width"],
+                               sad=f["sad"])
+    source = SpectralBeamletSource(ali_rogers_mv("varian-6mv", e_min=0.1), fan.focal_point,
+                                   fan.centers, fan.width_u, fan.width_v)
+    xs = AnalyticCrossSections(geometry_densities=grid.max_density_by_material())
+    return grid, xs, source
+
+
+def _ct_shard(task):
+    count, k = task
+    from pyradmc.backends.ref.engine import ReferenceEngine
+    from pyradmc.rng.host import HostRNG
+
+    grid, xs, source = _ct_build()
+    run = dict(CT_CASE["run"])
+    n_batches = run.pop("n_batches")
+    seed = run.pop("seed") * 100 + k
+    res = ReferenceEngine(grid=grid, cross_sections=xs, rng=HostRNG()).run_dij(
+        source, n_histories_per_beamlet=count // n_batches, n_batches=1, seed=seed, **run)
+    dense = np.stack([res.column_dense(j).reshape(-1) for j in range(res.n_beamlets)])
+    books = (res.energy_emitted, res.energy_deposited, res.energy_escaped, res.energy_unscored)
+    return dense, books
+
+
+def _pool(n_tasks: int):
+    import multiprocessing
+    import os
+    from concurrent.futures import ProcessPoolExecutor
+
+    for var in ("OMP_NUM_THREADS", "OPENBLAS_NUM_THREADS", "MKL_NUM_THREADS"):
+        os.environ[var] = "1"  # one core per shard
+    return ProcessPoolExecutor(max_workers=min(n_tasks, os.cpu_count() or 1),
+                               mp_context=multiprocessing.get_context("spawn"),
+                               initializer=_init_worker, initargs=(REFERENCE,))
+
+
+def _warm_gs_cache(name: str) -> None:
+    """Build the eager GS node window once before the workers start: the
+    reference otherwise extends its on-disk grid lazily, node by node, in every
+    worker at once."""
+    from pyradmc.data.goudsmit_saunderson import build_gs_grid, gs_window_from_tables
+
+    _, xs, source, _ = build_case(name)
+    for e_max in (source.max_energy, 6.0):
+        tables = xs.build_tables(ecut=0.2, pcut=0.05, e_max=e_max * (1 + 1e-6))
+        build_gs_grid(*gs_window_from_tables(tables, [0]))
+
+
+def run_sharded(name: str) -> None:
+    shards = CASES[name]["shards"]
+    _warm_gs_cache(name)
+    t0 = time.perf_counter()
+    with _pool(shards) as pool:
+        parts = list(pool.map(_forward_shard, [(name, k) for k in range(shards)]))
+    elapsed = time.perf_counter() - t0
+    grid_shape = CASES[name]["grid"]["shape"]
+    mean, sigma = _combine_batches(np.stack([p[0] for p in parts]))
+    books = np.sum([p[1] for p in parts], axis=0)
+    run = CASES[name]["run"]
+    np.savez_compressed(
+        HERE / f"ref_{name}.npz",
+        energy_emitted=books[0], energy_deposited=books[1], energy_escaped=books[2],
+        energy_unscored=books[3], seconds=elapsed,
+        dose=mean.reshape(grid_shape), dose_sigma=sigma.reshape(grid_shape),
+        n_batches=shards, n_histories=run["n_histories"], shard_seeds=run["seed"] * 100 + np.arange(shards),
+    )
+    print(f"{name}: {elapsed:.1f} s over {shards} shards", flush=True)
+
+
+def run_ct() -> None:
+    n_batches = CT_CASE["run"]["n_batches"]
+    _warm_gs_cache("dij_spectral")
+    for count in CT_CASE["counts"]:
+        t0 = time.perf_counter()
+        with _pool(n_batches) as pool:
+            parts = list(pool.map(_ct_shard, [(count, k) for k in range(n_batches)]))
+        elapsed = time.perf_counter() - t0
+        batch = np.stack([p[0] for p in parts])  # [batch][column][voxel]
+        mean, sigma = _combine_batches(batch)
+        books = np.sum([p[1] for p in parts], axis=0)
+        np.savez_compressed(
+            HERE / f"ref_ct_beamlets_{count}.npz",
+            energy_emitted=books[0], energy_deposited=books[1], energy_escaped=books[2],
+            energy_unscored=books[3], seconds=elapsed, dose=mean, dose_sigma=sigma,
+            n_batches=n_batches, n_histories_per_beamlet=count,
+            shard_seeds=CT_CASE["run"]["seed"] * 100 + np.arange(n_batches),
+        )
+        print(f"ct_beamlets {count}: {elapsed:.1f} s over {n_batches} shards", flush=True)
+
+
 def run_case(name: str) -> None:
+    if "shards" in CASES[name]:
+        run_sharded(name)
+        return
     from pyradmc.backends.ref.engine import ReferenceEngine
     from pyradmc.rng.host import HostRNG
 
@@ -155,10 +297,13 @@ def make_reduction() -> None:
 if __name__ == "__main__":
     if len(sys.argv) < 2:
         raise SystemExit("usage: python tests/golden/make_golden.py /path/to/pyRadMC [case ...]")
-    sys.path.insert(0, sys.argv[1])
-    names = sys.argv[2:] or ["reduction", *CASES]
+    REFERENCE = sys.argv[1]
+    sys.path.insert(0, REFERENCE)
+    names = sys.argv[2:] or ["reduction", *CASES, "ct_beamlets"]
     for name in names:
         if name == "reduction":
             make_reduction()
+        elif name == "ct_beamlets":
+            run_ct()
         else:
             run_case(name)

@@ -39,7 +39,7 @@ def test_library_exports_every_declared_symbol():
 
 
 def test_abi_version():
-    assert _lib.load().pmc_abi_version() == 1
+    assert _lib.load().pmc_abi_version() == 2
 
 
 def test_ctypes_structs_match_the_c_layout(tmp_path):
@@ -48,6 +48,7 @@ def test_ctypes_structs_match_the_c_layout(tmp_path):
         "pmc_scoring_desc": _lib.ScoringDesc,
         "pmc_source_desc": _lib.SourceDesc,
         "pmc_beamlet_desc": _lib.BeamletDesc,
+        "pmc_beamlet_rec": _lib.BeamletRec,
         "pmc_run_params": _lib.RunParams,
         "pmc_books": _lib.Books,
         "pmc_counters": _lib.Counters,

@@ -20,6 +20,8 @@ class FakeEngine:
     chunk_size: int | None = None
     block_size: int | None = None
     blocks_per_sm: int | None = None
+    tail_steps: int | None = None
+    smem_tables: bool | None = None
 
     def drop_uploads(self):
         pass
@@ -38,6 +40,8 @@ def _fake_timer(calls):
         chunk = engine.chunk_size or 16 * 148 * 3 * bs
         t = abs(bs - 192) + (0 if engine.blocks_per_sm is None else 5)
         t += abs(chunk - 16 * 148 * 3 * bs) / 1e6
+        t += 0.0 if engine.tail_steps == 256 else 0.5   # the second stage's favourite
+        t += 0.0 if engine.smem_tables is None else 0.25
         return 1.0 + t, _dij()
     return timer
 
@@ -64,7 +68,11 @@ def test_tuner_picks_the_fastest_shape_and_caches_it(tmp_path):
                            timer=_fake_timer(calls), sm_count=148, device_name="B200")
     assert (tuned.block_size, tuned.blocks_per_sm) == (192, None)
     assert tuned.chunk_size == 16 * 148 * 3 * 192
-    assert not report["cached"] and len(report["timings"]) == len(T.candidates(148))
+    assert (tuned.tail_steps, tuned.smem_tables) == (256, None)  # refined on the best geometry
+    stage2 = T.refinements(T.LaunchShape(192, None, 16 * 148 * 3 * 192))
+    assert len(stage2) == len(T.TAIL_STEPS) * len(T.SMEM_TABLES)  # the best itself is among them
+    assert not report["cached"]
+    assert len(report["timings"]) == len(T.candidates(148)) + len(stage2) - 1
     assert report["timings"][0]["block_size"] is None  # the default was timed
     assert all(c[3] == 100 * 20_000 for c in calls)  # probes run a tenth of the histories
     again, report2 = T.tune(engine, source, np.full(100, 200_000), 10, 1, cache=cache,

@@ -1,0 +1,138 @@
+"""Beamlet sources beyond the two built-in generators, through the C-ABI (CUDA
+device needed).
+
+* A concatenation of beamlet sources (a multi-beam plan as one Dij) gives, for
+  correlated sampling, exactly the columns of the separate runs: the stream key
+  of a history is its within-beamlet index, whatever column it lands in.
+* A per-beamlet mixture (CompositeBeamletSource, geometry/source.py:239-277)
+  is pinned against pyRadMC's ReferenceEngine in test_gpu_transport.py
+  (``dij_composite``); here its mean is checked against the weighted sum of its
+  components' Dijs.
+* The host pre-sampling route (BeamletSource.sample_beamlet_batch, the Warp
+  engine's ``_generate_group_presampled``, engine.py:3224-3335) transports the
+  same primaries as the in-kernel fan, statistically.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import pyradmc_b200 as P
+from oracle import stats
+from tests.conftest import SEED, build_case
+
+pytestmark = pytest.mark.gpu
+
+
+def _water(shape=(16, 16, 16), spacing=(0.5, 0.5, 0.5)):
+    grid = P.VoxelGrid.uniform_water(shape, spacing)
+    return grid, P.AnalyticWaterTables(geometry_densities=grid.max_density_by_material())
+
+
+def _fan(focal, centers, u=(1.0, 0.0, 0.0), v=(0.0, 1.0, 0.0), width=1.5):
+    return P.SpectralBeamletSource(P.ali_rogers_varian_6mv(), focal, centers, width, width, u, v)
+
+
+class PresampledFan:
+    """A beamlet source the engine cannot generate in-kernel: it only offers
+    vectorized host sampling (the fan of _DivergentFan.sample_through_batch,
+    geometry/source.py:508-549, with its own PCG64 stream)."""
+
+    def __init__(self, fan):
+        self.fan = fan
+        self.n_beamlets = fan.n_beamlets
+        self.max_energy = fan.max_energy
+
+    def sample_beamlet_batch(self, seed, history_offset, n, beamlet):
+        bitgen = np.random.PCG64(seed)
+        bitgen.advance(4 * history_offset)
+        u = np.random.Generator(bitgen).random((n, 4))
+        sp = self.fan.spectrum
+        k = np.minimum(np.searchsorted(sp.cdf, u[:, 0], side="left"), sp.cdf.size - 1)
+        energy = sp.edges[k] + (sp.edges[k + 1] - sp.edges[k]) * u[:, 1]
+        du = (u[:, 2] - 0.5) * self.fan.width_u
+        dv = (u[:, 3] - 0.5) * self.fan.width_v
+        focal = np.asarray(self.fan.focal_point)
+        target = (np.asarray(self.fan.centers[beamlet]) + du[:, None] * np.asarray(self.fan.u_axis)
+                  + dv[:, None] * np.asarray(self.fan.v_axis))
+        d = target - focal
+        d /= np.linalg.norm(d, axis=1, keepdims=True)
+        f32 = np.float32
+        return {"particle_type": np.ones(n, np.int32), "energy": energy.astype(f32),
+                "x": np.full(n, focal[0], f32), "y": np.full(n, focal[1], f32),
+                "z": np.full(n, focal[2], f32), "ux": d[:, 0].astype(f32),
+                "uy": d[:, 1].astype(f32), "uz": d[:, 2].astype(f32),
+                "weight": np.ones(n, f32)}
+
+
+def test_concatenated_beams_are_the_separate_dijs_bit_for_bit(gpu):
+    grid, xs = _water()
+    beam_z = _fan((4.0, 4.0, -100.0), [(3.0, 3.0, 0.0), (5.0, 5.0, 0.0)])
+    beam_x = _fan((-100.0, 4.0, 4.0), [(4.0, 3.0, 3.0), (4.0, 5.0, 5.0), (4.0, 4.0, 4.0)],
+                  u=(0.0, 1.0, 0.0), v=(0.0, 0.0, 1.0))
+    lattice = P.BeamletGridSource(6.0, -1.0, (1.0, 7.0), (1.0, 7.0), 2, 1)
+    plan = P.ConcatenatedBeamletSource([beam_z, beam_x, lattice])
+    kw = dict(n_batches=4, seed=SEED, truncation=1e-3)
+    engine = P.B200Engine(grid, xs)
+    whole = engine.run_dij(plan, n_histories_per_beamlet=[4000, 8000, 4000, 4000, 8000, 4000, 4000], **kw)
+    parts = [engine.run_dij(beam_z, n_histories_per_beamlet=[4000, 8000], **kw),
+             engine.run_dij(beam_x, n_histories_per_beamlet=[4000, 4000, 8000], **kw),
+             engine.run_dij(lattice, n_histories_per_beamlet=4000, **kw)]
+    j = 0
+    for part in parts:
+        for k in range(part.n_beamlets):
+            np.testing.assert_array_equal(whole.column_dense(j), part.column_dense(k))
+            np.testing.assert_array_equal(whole.sigma_dense(j), part.sigma_dense(k))
+            j += 1
+    assert j == whole.n_beamlets == 7
+
+
+def test_composite_mean_is_the_weighted_sum_of_its_components(gpu):
+    grid, xs, src, run = build_case("dij_composite")
+    engine = P.B200Engine(grid, xs)
+    run["n_histories_per_beamlet"] = 16_000
+    mix = engine.run_dij(src, correlated=False, **run)
+    comps = [engine.run_dij(c, correlated=False, seed=run["seed"] + 1 + i,
+                            **{k: v for k, v in run.items() if k != "seed"})
+             for i, c in enumerate(src._sources)]
+    w = np.diff(np.concatenate([[0.0], src._cdf]))
+    for j in range(mix.n_beamlets):
+        a = mix.column_dense(j).reshape(-1)
+        sa = mix.sigma_dense(j).reshape(-1)
+        b = sum(wk * c.column_dense(j).reshape(-1) for wk, c in zip(w, comps, strict=True))
+        sb = np.sqrt(sum((wk * c.sigma_dense(j).reshape(-1)) ** 2 for wk, c in zip(w, comps, strict=True)))
+        mask = stats.high_dose_mask(a, sa, sb, minimum=50)
+        stats.assert_chi2_consistent_batched(a, sa, mix.n_batches, b, sb, mix.n_batches, mask=mask,
+                                             case=f"composite = weighted components, column {j}")
+
+
+def test_presampled_route_matches_the_in_kernel_fan(gpu):
+    grid, xs = _water()
+    fan = _fan((4.0, 4.0, -100.0), [(3.0, 3.0, 0.0), (5.0, 4.0, 0.0)])
+    engine = P.B200Engine(grid, xs)
+    kw = dict(n_histories_per_beamlet=[40_000, 80_000], n_batches=8, truncation=0.0)
+    inner = engine.run_dij(fan, seed=SEED, **kw)
+    host = engine.run_dij(PresampledFan(fan), seed=SEED + 5, **kw)
+    for j in range(2):
+        a, sa = inner.column_dense(j).reshape(-1), inner.sigma_dense(j).reshape(-1)
+        b, sb = host.column_dense(j).reshape(-1), host.sigma_dense(j).reshape(-1)
+        mask = stats.high_dose_mask(a, sa, sb, minimum=50)
+        stats.assert_chi2_consistent_batched(a, sa, 8, b, sb, 8, mask=mask,
+                                             case=f"presampled fan column {j}")
+    # emitted energy is booked per uploaded primary; the ledger closes
+    assert host.energy_emitted == pytest.approx(inner.energy_emitted, rel=0.01)
+    balance = host.energy_deposited + host.energy_escaped + host.energy_unscored
+    assert balance == pytest.approx(host.energy_emitted, rel=1e-4)
+
+
+def test_a_failing_host_sampler_raises_its_own_exception(gpu):
+    grid, xs = _water((8, 8, 8))
+
+    class Broken(PresampledFan):
+        def sample_beamlet_batch(self, *args):
+            raise KeyError("no such beamlet file")
+
+    with pytest.raises(KeyError, match="no such beamlet file"):
+        P.B200Engine(grid, xs).run_dij(Broken(_fan((2.0, 2.0, -100.0), [(2.0, 2.0, 0.0)])),
+                                       n_histories_per_beamlet=100, n_batches=2, seed=SEED)

@@ -24,7 +24,7 @@ import pytest
 import pyradmc_b200 as P
 from oracle import stats
 from pyradmc_b200 import _lib
-from tests.conftest import CASES, GOLDEN, SEED, build_case, load_ref
+from tests.conftest import CASES, CT_CASE, GOLDEN, SEED, build_case, build_ct_case, load_ref
 
 pytestmark = pytest.mark.gpu
 
@@ -48,7 +48,8 @@ def test_dose_matches_reference_engine(gpu, name):
     ref = load_ref(name)
     mask = stats.high_dose_mask(ref["dose"], ref["dose_sigma"], result.dose_sigma, minimum=50)
     stats.assert_chi2_consistent_batched(ref["dose"], ref["dose_sigma"], int(ref["n_batches"]),
-                                         result.dose, result.dose_sigma, result.n_batches, mask=mask)
+                                         result.dose, result.dose_sigma, result.n_batches, mask=mask,
+                                         case=name)
 
 
 @pytest.mark.parametrize("name", DIJ)
@@ -62,7 +63,31 @@ def test_dij_columns_match_reference_engine(gpu, name):
         b, sb = dij.column_dense(j).reshape(-1), dij.sigma_dense(j).reshape(-1)
         mask = stats.high_dose_mask(a, sa, sb, minimum=50)
         stats.assert_chi2_consistent_batched(a, sa, int(ref["n_batches"]), b, sb, dij.n_batches,
-                                             mask=mask)
+                                             mask=mask, case=f"{name} column {j}")
+
+
+def test_ct_phantom_with_uneven_counts_matches_reference_engine(gpu):
+    """The benchmark's Dij at reduced size: a 40^3 CT-like phantom (seeded
+    ellipsoids of density 0.2-1.9 g/cc), 5 mm 6 MV spectral beamlets, uneven
+    per-column counts.  pyRadMC's run_dij takes one count for all columns, so
+    each column is compared with the reference run at its own count."""
+    grid, xs, src = build_ct_case()
+    lo, hi = CT_CASE["counts"]
+    counts = [lo, hi, lo, hi]
+    n_batches = CT_CASE["run"]["n_batches"]
+    engine = P.B200Engine(grid, xs)
+    dij = engine.run_dij(src, n_histories_per_beamlet=[4 * c for c in counts], n_batches=n_batches,
+                         seed=SEED + 1, truncation=0.0)
+    refs = {c: load_ref(f"ct_beamlets_{c}") for c in (lo, hi)}
+    for j, c in enumerate(counts):
+        ref = refs[c]
+        a, sa = ref["dose"][j], ref["dose_sigma"][j]
+        b, sb = dij.column_dense(j).reshape(-1), dij.sigma_dense(j).reshape(-1)
+        for fraction in (0.1, 0.01):  # the beamlet core, then the penumbra and low-dose tail
+            mask = stats.high_dose_mask(a, sa, sb, fraction=fraction, minimum=50)
+            stats.assert_chi2_consistent_batched(
+                a, sa, int(ref["n_batches"]), b, sb, dij.n_batches, mask=mask,
+                case=f"ct_beamlets column {j} ({c} histories, >= {fraction:g} of max)")
 
 
 def _same(a, b):
@@ -84,6 +109,10 @@ def test_bit_reproducible_within_device(gpu):
     dict(chunk_size=5000, block_size=128),
     dict(blocks_per_sm=1, block_size=64),
     dict(queue_factor=64, chunk_size=1000),
+    dict(tail_steps=1),  # every particle parked after one step once its round runs dry
+    dict(tail_steps=-1),  # never parked
+    dict(smem_tables=False),
+    dict(smem_tables=True, tail_steps=7, use_graph=False),
 ])
 def test_scheduling_knobs_are_bit_inert(gpu, knobs):
     base, src, run = _engine("full_slab")
@@ -94,8 +123,19 @@ def test_scheduling_knobs_are_bit_inert(gpu, knobs):
 def test_spectral_and_electron_routes_are_bit_inert(gpu):
     for name in ("slab_spectral", "electron_beam"):
         a, src, run = _engine(name)
-        b, _, _ = _engine(name, chunk_size=777, use_graph=False)
+        b, _, _ = _engine(name, chunk_size=777, use_graph=False, tail_steps=3, smem_tables=False)
         _same(a.run(src, **run), b.run(src, **run))
+
+
+def test_ct_dij_is_bit_inert_to_parking_and_table_placement(gpu):
+    grid, xs, src = build_ct_case()
+    kw = dict(n_histories_per_beamlet=[20_000, 60_000, 20_000, 60_000], n_batches=10, seed=SEED,
+              truncation=1e-3)
+    a = P.B200Engine(grid, xs).run_dij(src, **kw)
+    b = P.B200Engine(grid, xs, tail_steps=2, smem_tables=False, chunk_size=4096).run_dij(src, **kw)
+    for f in ("indptr", "indices", "dose", "sigma"):
+        np.testing.assert_array_equal(getattr(a, f), getattr(b, f))
+    assert a.energy_deposited == b.energy_deposited and a.energy_escaped == b.energy_escaped
 
 
 @pytest.mark.parametrize("transport_electrons", [False, True])

@@ -69,7 +69,12 @@ def _oracle_case(name, mult, seed_offset=1, n_threads=None):
     return grid, src, run, counts, mean, sigma, books
 
 
-@pytest.mark.parametrize("name", list(CASES))
+# The C oracle restates the built-in generators only; mixtures are pinned on
+# the GPU against the reference fixtures directly.
+ORACLE_CASES = [n for n, c in CASES.items() if c["source"]["kind"] != "composite"]
+
+
+@pytest.mark.parametrize("name", ORACLE_CASES)
 def test_oracle_transport_matches_reference_engine(name):
     mult = 1 if name == "readme_pencil" else 4
     _, _, run, counts, mean, sigma, _ = _oracle_case(name, mult)
