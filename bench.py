@@ -381,6 +381,98 @@ def denoiser_leg(args, engine, source, counts, stream, device, plain_s_at_2pct):
     }
 
 
+# ---- the full-plan workload ----------------------------------------------------------
+PLAN_SHAPE = (256, 256, 128)
+PLAN_SPACING = 0.3
+PLAN_HELD_OUT = 50
+PLAN_REF_HISTORIES = 8_000_000  # per held-out beamlet
+
+
+def plan_workload():
+    """A 256 x 256 x 128 phantom at 3 mm (water plus seeded ellipsoids of
+    density U(0.2, 1.9), semi-axes scaled with the box from the 128^3 case's
+    1-4 cm), 7 coplanar equi-spaced beams x 20 x 20 beamlets of 5 mm of the
+    6 MV spectrum at SAD 100 cm = 2,800 columns, and 50 held-out columns
+    spread evenly over the plan."""
+    from pyradmc_b200 import model, phantoms
+    from pyradmc_b200.model import AnalyticWaterTables
+
+    scale = PLAN_SHAPE[0] * PLAN_SPACING / (128 * 0.25)
+    grid = phantoms.ellipsoid_phantom(shape=PLAN_SHAPE, spacing=(PLAN_SPACING,) * 3, seed=SEED,
+                                      semi_axis_range=(1.0 * scale, 4.0 * scale))
+    plan, angles = phantoms.coplanar_plan(grid)
+    held = np.linspace(0, plan.n_beamlets - 1, PLAN_HELD_OUT).round().astype(int)
+    parts = []
+    for j in held:
+        k, i = plan.part_of(int(j))
+        beam = plan.sources[k]
+        parts.append(model.SpectralBeamletSource(beam.spectrum, beam.focal_point, [beam.centers[i]],
+                                                 beam.width_u, beam.width_v, beam.u_axis, beam.v_axis))
+    held_source = model.ConcatenatedBeamletSource(parts)
+    xs = AnalyticWaterTables(geometry_densities=grid.max_density_by_material())
+    return grid, xs, plan, angles, held, held_source
+
+
+def plan_leg(args, device, stream):
+    """s per plan at 2 % sigma-equivalent error, plain Monte Carlo.
+
+    Untimed: a PLAN_REF_HISTORIES-per-beamlet reference of the 50 held-out
+    columns (independent streams), then a pilot at 1e5 histories per beamlet
+    that sets the count N at which the held-out columns reach 2 % (1/sqrt(N)).
+    Timed (CUDA events, device-resident like ``value``): the whole 2,800-column
+    Dij at N, transport to CSC in HBM through grouped dense maps.  The held-out
+    columns at N (bit-identical to the plan's own: correlated keys) confirm the
+    error reached."""
+    import torch
+
+    from pyradmc_b200 import B200Engine
+    from pyradmc_b200 import denoise_dij as D
+
+    grid, xs, plan, angles, held, held_source = plan_workload()
+    engine = B200Engine(grid, xs, device=device)
+    engine.use_stream(stream.cuda_stream)
+    ref = engine.run_dij_device(held_source, PLAN_REF_HISTORIES, N_BATCHES, SEED + 977, truncation=0.0)
+    ref_dose, _, ref_sigma = D.dense_columns(ref, device, with_sigma=True)
+
+    def held_error(n_per):
+        view = engine.run_dij_device(held_source, n_per, N_BATCHES, SEED, truncation=0.0)
+        dose, _, _ = D.dense_columns(view, device)
+        err = D.sigma_equivalent_error(dose, ref_dose, ref_sigma)
+        del dose
+        return float(np.nanmean(err))
+
+    pilot_n = 100_000
+    pilot = held_error(pilot_n)
+    n_2pct = int(np.ceil(pilot_n * (pilot / 0.02) ** 2 / N_BATCHES)) * N_BATCHES
+    engine.run_dij_device(plan, pilot_n, N_BATCHES, SEED, truncation=1e-3)  # warm-up
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    view = engine.run_dij_device(plan, n_2pct, N_BATCHES, SEED, truncation=1e-3)
+    e1.record(stream)
+    e1.synchronize()
+    seconds = e0.elapsed_time(e1) / 1e3
+    c = engine.last_counters()
+    nnz = int(view.nnz)
+    reached = held_error(n_2pct)
+    del ref_dose, ref_sigma
+    torch.cuda.empty_cache()
+    return {
+        "workload": "plan_256x256x128_3mm_7beams_2800beamlets_6MV",
+        "beams_deg": [round(a, 2) for a in angles],
+        "columns": int(plan.n_beamlets),
+        "held_out_columns": int(len(held)),
+        "reference_histories_per_beamlet": PLAN_REF_HISTORIES,
+        "pilot_histories_per_beamlet": pilot_n,
+        "pilot_sigma_eq": pilot,
+        "plain": {"histories_per_beamlet": n_2pct, "histories": int(n_2pct * plan.n_beamlets),
+                  "s_per_plan": seconds, "histories_per_s": n_2pct * plan.n_beamlets / seconds,
+                  "sigma_eq_held_out": reached, "nnz": nnz,
+                  "transport_ms": c["transport_ms"], "reduce_ms": c["reduce_ms"],
+                  "measured": "timed at the 2 % count (not extrapolated)"},
+    }
+
+
 def conv_arm(args, local):
     """``--workload conv``: the denoiser's dominant convolution (decoder level 0,
     48 -> 16 channels, one inference chunk of 16 windows of 64 x 64 x 128) on
@@ -522,6 +614,11 @@ def b200_arm(args, world, rank, local):
     s_at_2pct_pre = total_ms / args.steps / 1e3 * (sigma_pre / 0.02) ** 2
     den = None if args.no_denoiser else denoiser_leg(args, engine, source, counts, stream, device,
                                                      s_at_2pct_pre)
+    plan = None
+    if not args.no_plan:
+        engine.drop_uploads()
+        torch.cuda.empty_cache()
+        plan = plan_leg(args, device, stream)
     transport_s = c["transport_ms"] / 1e3
     achieved = algorithmic_bytes(c) / transport_s / 1e9
     sigma = phantoms.per_beamlet_sigma(dij)
@@ -561,6 +658,7 @@ def b200_arm(args, world, rank, local):
         "s_per_dij_at_2pct_sigma": s_at_2pct,
         "plain_2pct": "extrapolated: measured s per Dij x (per-beamlet sigma / 2 %)^2 (1/sqrt(N) scaling)",
         "denoiser": den,
+        "plan": plan,
         "e2e": {"value": e2e_value, "unit": "histories/s",
                 "h2d_bytes_per_step": int(np.median(h2d)), "d2h_bytes_per_step": int(np.median(d2h)),
                 "ms_per_step": e2e_total / args.steps},
@@ -604,6 +702,8 @@ def main() -> int:
                     help="skip the CPU baseline leg (profiling runs)")
     ap.add_argument("--no-denoiser", action="store_true",
                     help="skip the MC + denoiser leg (profiling runs)")
+    ap.add_argument("--no-plan", action="store_true",
+                    help="skip the full-plan leg (2,800 columns on a 256 x 256 x 128 phantom)")
     ap.add_argument("--no-autotune", action="store_true",
                     help="default launch shape instead of the autotuned one")
     args = ap.parse_args()

@@ -57,6 +57,10 @@ extern "C" {
 #define PMC_SRC_PARALLEL 1
 #define PMC_SRC_SPECTRAL 2
 #define PMC_SRC_UPLOAD 3
+/* A phase space kept resident on the device: history h draws record
+ * floor(r * n_records), r a 64-bit draw of its own stream, the per-history
+ * sampling of PhaseSpaceSource.emit (geometry/phasespace.py:546). */
+#define PMC_SRC_PHASESPACE 4
 
 /* Beamlet generators: generate_beamlet_lattice (kernels.py:2248),
  * generate_spectral_beamlets (kernels.py:2322), per-beamlet records (fans and
@@ -99,13 +103,21 @@ typedef struct pmc_tables_desc {
     const double* coherent_cumulative; /* [n_materials][n_coherent] */
 } pmc_tables_desc;
 
-/* Scoring geometry: a rectilinear grid (pyradmc/scoring/grid.py:67).  A
- * deposit outside it is booked to the unscored ledger (kernels.py:536-585). */
+/* Scoring geometry: a rectilinear grid (pyradmc/scoring/grid.py:67) or, with
+ * mode 1, depth bins by radial shells about an axis parallel to z
+ * (CylindricalScoringGrid, pyradmc/scoring/cylinder.py:172; device side
+ * _scoring_index, kernels.py:492-533).  A deposit outside it is booked to the
+ * unscored ledger (kernels.py:536-585). */
 typedef struct pmc_scoring_desc {
     int32_t nx, ny, nz;
     double origin[3];
     double spacing[3];
-    const double* voxel_mass; /* [nx*ny*nz] grams, C order */
+    const double* voxel_mass; /* [nx*ny*nz] grams, C order; mode 1: [n_depth][n_shells] */
+    int32_t mode;             /* 0 rectilinear, 1 cylindrical */
+    double axis[2];           /* mode 1: (x, y) of the axis */
+    int32_t n_depth, n_shells;
+    const double* depth_edges;  /* mode 1: [n_depth + 1], increasing */
+    const double* radial_edges; /* mode 1: [n_shells + 1], increasing, >= 0 */
 } pmc_scoring_desc;
 
 /* Open-field primary source (WarpEngine.run, engine.py:454). */
@@ -128,6 +140,7 @@ typedef struct pmc_source_desc {
     const float* up_pos;    /* [n][3] */
     const float* up_dir;    /* [n][3] */
     const float* up_weight;
+    int64_t n_records; /* PMC_SRC_PHASESPACE: records in the up_* arrays */
 } pmc_source_desc;
 
 /* One beamlet of a PMC_BEAMLET_RECORDS source: a lattice rectangle

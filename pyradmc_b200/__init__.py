@@ -12,7 +12,9 @@ from pyradmc_b200.model import (
     BeamletGridSource,
     CompositeBeamletSource,
     ConcatenatedBeamletSource,
+    CylindricalScoringGrid,
     DijResult,
+    PackedCrossSections,
     ParallelBeamSource,
     PencilBeamSource,
     ScoringGrid,
@@ -22,6 +24,9 @@ from pyradmc_b200.model import (
     TransportResult,
     VoxelGrid,
     ali_rogers_varian_6mv,
+    geometric_edges,
+    save_pack,
+    uniform_edges,
 )
 
 __all__ = [
@@ -30,7 +35,9 @@ __all__ = [
     "BeamletGridSource",
     "CompositeBeamletSource",
     "ConcatenatedBeamletSource",
+    "CylindricalScoringGrid",
     "DijResult",
+    "PackedCrossSections",
     "ParallelBeamSource",
     "PencilBeamSource",
     "ScoringGrid",
@@ -40,4 +47,7 @@ __all__ = [
     "TransportResult",
     "VoxelGrid",
     "ali_rogers_varian_6mv",
+    "geometric_edges",
+    "save_pack",
+    "uniform_edges",
 ]

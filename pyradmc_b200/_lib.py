@@ -24,7 +24,7 @@ PMC_ERR_STATE = -7
 PMC_ERR_CAPACITY = -8
 
 PMC_PHOTON, PMC_ELECTRON, PMC_POSITRON = 0, 1, 2
-PMC_SRC_PENCIL, PMC_SRC_PARALLEL, PMC_SRC_SPECTRAL, PMC_SRC_UPLOAD = 0, 1, 2, 3
+PMC_SRC_PENCIL, PMC_SRC_PARALLEL, PMC_SRC_SPECTRAL, PMC_SRC_UPLOAD, PMC_SRC_PHASESPACE = 0, 1, 2, 3, 4
 PMC_BEAMLET_LATTICE, PMC_BEAMLET_SPECTRAL, PMC_BEAMLET_RECORDS, PMC_BEAMLET_UPLOAD = 0, 1, 2, 3
 
 _dp = C.POINTER(C.c_double)
@@ -72,6 +72,12 @@ class ScoringDesc(C.Structure):
         ("origin", _d3),
         ("spacing", _d3),
         ("voxel_mass", _dp),
+        ("mode", C.c_int32),
+        ("axis", C.c_double * 2),
+        ("n_depth", C.c_int32),
+        ("n_shells", C.c_int32),
+        ("depth_edges", _dp),
+        ("radial_edges", _dp),
     ]
 
 
@@ -101,6 +107,7 @@ class SourceDesc(C.Structure):
         ("up_pos", _fp),
         ("up_dir", _fp),
         ("up_weight", _fp),
+        ("n_records", C.c_int64),
     ]
 
 

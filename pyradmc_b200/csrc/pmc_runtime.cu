@@ -62,8 +62,12 @@ struct pmc_engine {
     float2* d_vox = nullptr;
     std::vector<double> default_mass;  // density * volume for the default scoring grid
 
-    // scoring grid
+    // scoring geometry
     GridInfo si{};
+    int score_mode = 0;           // 0 rectilinear (si), 1 cylindrical (cyl)
+    CylInfo cyl{};
+    float* d_cyl_z = nullptr;
+    float* d_cyl_r2 = nullptr;
     bool custom_scoring = false;
     double* d_mass = nullptr;
     long long mass_len = 0;
@@ -372,6 +376,8 @@ TransportParams make_params(pmc_engine* e, const pmc_run_params* p, const RunPla
     TransportParams P{};
     P.gi = e->gi;
     P.si = e->si;
+    P.score_mode = e->score_mode;
+    P.cyl = e->cyl;
     P.vox = e->d_vox;
     P.tab = e->tab;
     for (int i = 0; i < 4; ++i) P.q[i] = (Slot*)e->q[i].p;
@@ -797,6 +803,8 @@ void pmc_destroy(pmc_engine* e) {
     if (e->d_gs4) cudaFree(e->d_gs4);
     if (e->d_vox) cudaFree(e->d_vox);
     if (e->d_mass) cudaFree(e->d_mass);
+    if (e->d_cyl_z) cudaFree(e->d_cyl_z);
+    if (e->d_cyl_r2) cudaFree(e->d_cyl_r2);
     for (DevBuf* b : {&e->q[0], &e->q[1], &e->q[2], &e->q[3], &e->edep, &e->s1, &e->s2,
                       &e->tile_counts, &e->tile_offsets, &e->col_counts, &e->out_idx,
                       &e->out_dose, &e->out_sigma, &e->col_nhist})
@@ -842,6 +850,7 @@ int pmc_upload_grid(pmc_engine* e, int32_t nx, int32_t ny, int32_t nz, const dou
     e->has_grid = true;
     e->max_material = max_mat;
     if (!e->custom_scoring) {
+        e->score_mode = 0;
         e->si = e->gi;
         if (e->d_mass) cudaFree(e->d_mass);
         e->d_mass = nullptr;
@@ -859,6 +868,7 @@ int pmc_set_scoring(pmc_engine* e, const pmc_scoring_desc* s) {
     PMC_CUDA(e, cudaSetDevice(e->device));
     if (!s) {
         e->custom_scoring = false;
+        e->score_mode = 0;
         e->si = e->gi;
         const long long n = e->gi.n_voxels;
         if (e->d_mass) cudaFree(e->d_mass);
@@ -869,16 +879,56 @@ int pmc_set_scoring(pmc_engine* e, const pmc_scoring_desc* s) {
         e->mass_len = n;
         return PMC_OK;
     }
-    if (s->nx < 1 || s->ny < 1 || s->nz < 1 || !s->voxel_mass)
-        return fail(e, PMC_ERR_INVALID, "invalid scoring grid");
-    const long long n = (long long)s->nx * s->ny * s->nz;
+    if (!s->voxel_mass) return fail(e, PMC_ERR_INVALID, "invalid scoring grid");
+    long long n = 0;
+    if (s->mode == 1) {
+        const int nd = s->n_depth, ns = s->n_shells;
+        if (nd < 1 || ns < 1 || !s->depth_edges || !s->radial_edges)
+            return fail(e, PMC_ERR_INVALID, "a cylindrical scoring grid needs depth and radial edges");
+        for (int k = 0; k < nd; ++k)
+            if (!(s->depth_edges[k + 1] > s->depth_edges[k]))
+                return fail(e, PMC_ERR_INVALID, "depth_edges must be strictly increasing");
+        for (int k = 0; k < ns; ++k)
+            if (!(s->radial_edges[k + 1] > s->radial_edges[k]) || s->radial_edges[k] < 0.0)
+                return fail(e, PMC_ERR_INVALID, "radial_edges must be non-negative and strictly increasing");
+        n = (long long)nd * ns;
+        std::vector<float> ze(nd + 1), re2(ns + 1);
+        for (int k = 0; k <= nd; ++k) ze[k] = (float)s->depth_edges[k];
+        for (int k = 0; k <= ns; ++k) re2[k] = (float)(s->radial_edges[k] * s->radial_edges[k]);
+        for (float** dst : {&e->d_cyl_z, &e->d_cyl_r2})
+            if (*dst) cudaFree(*dst), *dst = nullptr;
+        PMC_CUDA(e, cudaMalloc(&e->d_cyl_z, sizeof(float) * ze.size()));
+        PMC_CUDA(e, cudaMalloc(&e->d_cyl_r2, sizeof(float) * re2.size()));
+        PMC_CUDA(e, cudaMemcpy(e->d_cyl_z, ze.data(), sizeof(float) * ze.size(), cudaMemcpyHostToDevice));
+        PMC_CUDA(e, cudaMemcpy(e->d_cyl_r2, re2.data(), sizeof(float) * re2.size(), cudaMemcpyHostToDevice));
+        e->h2d_bytes += sizeof(float) * (ze.size() + re2.size());
+        CylInfo c{};
+        c.ax = (float)s->axis[0];
+        c.ay = (float)s->axis[1];
+        c.z_lo = ze.front();
+        c.z_hi = ze.back();
+        c.r_in_sq = re2.front();
+        c.r_out_sq = re2.back();
+        c.n_depth = nd;
+        c.n_shells = ns;
+        c.z_edges = e->d_cyl_z;
+        c.r_edges_sq = e->d_cyl_r2;
+        e->cyl = c;
+        e->score_mode = 1;
+        e->si = GridInfo{};
+        e->si.n_voxels = n;
+    } else {
+        if (s->nx < 1 || s->ny < 1 || s->nz < 1) return fail(e, PMC_ERR_INVALID, "invalid scoring grid");
+        n = (long long)s->nx * s->ny * s->nz;
+        e->si = make_grid(s->nx, s->ny, s->nz, s->origin, s->spacing);
+        e->score_mode = 0;
+    }
     if (e->d_mass) cudaFree(e->d_mass);
     e->d_mass = nullptr;
     PMC_CUDA(e, cudaMalloc(&e->d_mass, sizeof(double) * n));
     PMC_CUDA(e, cudaMemcpy(e->d_mass, s->voxel_mass, sizeof(double) * n, cudaMemcpyHostToDevice));
     e->h2d_bytes += (unsigned long long)(sizeof(double) * n);
     e->mass_len = n;
-    e->si = make_grid(s->nx, s->ny, s->nz, s->origin, s->spacing);
     e->custom_scoring = true;
     return PMC_OK;
 }
@@ -1050,6 +1100,26 @@ int pmc_run_forward(pmc_engine* e, const pmc_source_desc* src, const pmc_run_par
             if (!rc) rc = fill_gen_spectrum(e, G, src->n_bins, src->edges, src->cdf);
             break;
         }
+        case PMC_SRC_PHASESPACE: {
+            G.type = 5;
+            G.book_emitted = 1;
+            const long long n = src->n_records;
+            if (n < 1 || !src->up_kind || !src->up_energy || !src->up_pos || !src->up_dir || !src->up_weight)
+                return fail(e, PMC_ERR_INVALID, "phase-space source without records");
+            for (long long i = 0; i < n; ++i)
+                if (src->up_kind[i] < 0 || src->up_kind[i] > 2)
+                    return fail(e, PMC_ERR_INVALID, "bad particle kind in the phase space");
+            G.n_records = n;
+            std::vector<int> k(src->up_kind, src->up_kind + n);
+            std::vector<float> en(src->up_energy, src->up_energy + n), ps(src->up_pos, src->up_pos + 3 * n),
+                dr(src->up_dir, src->up_dir + 3 * n), w(src->up_weight, src->up_weight + n);
+            rc = upload_vec(e, k, &G.up_kind);
+            if (!rc) rc = upload_f32(e, en, &G.up_energy);
+            if (!rc) rc = upload_f32(e, ps, &G.up_pos);
+            if (!rc) rc = upload_f32(e, dr, &G.up_dir);
+            if (!rc) rc = upload_f32(e, w, &G.up_weight);
+            break;
+        }
         case PMC_SRC_UPLOAD: {
             G.type = 3;
             G.book_emitted = 1;
@@ -1072,7 +1142,7 @@ int pmc_run_forward(pmc_engine* e, const pmc_source_desc* src, const pmc_run_par
             return fail(e, PMC_ERR_INVALID, "unknown source type %d", src->type);
     }
     if (rc) return rc;
-    if (G.kind != PMC_PHOTON && G.kind != PMC_ELECTRON && G.type != 3)
+    if (G.kind != PMC_PHOTON && G.kind != PMC_ELECTRON && G.type != 3 && G.type != 5)
         return fail(e, PMC_ERR_INVALID, "unknown primary kind %d", G.kind);
     PMC_CUDA(e, cudaMemcpy(e->d_gen, &G, sizeof G, cudaMemcpyHostToDevice));
     e->h2d_bytes += (unsigned long long)(sizeof G);

@@ -66,7 +66,8 @@ struct __align__(16) BeamletRec {
 
 // Primary generator of the current group (device-resident).
 struct GenDesc {
-    int type;           // 0 pencil, 1 parallel/lattice, 2 spectral fan, 3 upload, 4 records
+    int type;           // 0 pencil, 1 parallel/lattice, 2 spectral fan, 3 upload, 4 records,
+                        // 5 resident phase space
     int kind;           // particle kind of analytic primaries
     int forward;        // 1: open-field run (history = batch * per_batch + t)
     int correlated;
@@ -97,6 +98,7 @@ struct GenDesc {
     const float* up_dir;
     const float* up_weight;
     int book_emitted;                    // spectral/upload: book emitted energy per primary
+    long long n_records;                 // resident phase space: records in up_*
     const BeamletRec* recs;              // records: [group][n_comp]
     const float* comp_cdf;               // records: [n_comp] mixture selection
     int n_comp;
@@ -107,9 +109,23 @@ struct Counters {
     long long escaped, unscored, deposited, emitted, violations;
 };
 
+// Cylindrical scoring bins (geometry/cylinder.py): depth along z by radial
+// shell about an axis parallel to z, edges in float32 as the Warp kernels hold
+// them, radial edges squared.
+struct CylInfo {
+    float ax, ay;             // axis
+    float z_lo, z_hi;         // first and last depth edge
+    float r_in_sq, r_out_sq;  // first and last squared radial edge
+    int n_depth, n_shells;
+    const float* z_edges;     // [n_depth + 1]
+    const float* r_edges_sq;  // [n_shells + 1]
+};
+
 struct TransportParams {
     GridInfo gi;          // transport grid
-    GridInfo si;          // scoring grid
+    GridInfo si;          // scoring grid (score_mode 0)
+    int score_mode;       // 0 rectilinear, 1 cylindrical
+    CylInfo cyl;          // scoring bins (score_mode 1)
     const float2* vox;    // (density, material bits) per transport voxel
     Tables tab;
     Slot* q[4];           // P0, P1, E0, E1
@@ -198,14 +214,41 @@ struct HeldSink {
     }
 };
 
+// edge_bin_index (geometry/cylinder.py): the bin k with edges[k] <= v <
+// edges[k + 1], clamped into [0, n - 1]; the caller has checked containment.
+__device__ __forceinline__ int edge_bin_index(float v, const float* edges, int n) {
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (v >= __ldg(edges + mid)) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+// kernels.py:492 _scoring_index: the flat scoring bin of a position, or -1
+// when the scoring geometry excludes it (half-open on every axis and shell).
+__device__ __forceinline__ long long scoring_index(const TransportParams& P, float x, float y,
+                                                   float z) {
+    if (P.score_mode == 0) return point_inside(x, y, z, P.si) ? flat_index(x, y, z, P.si) : -1;
+    const CylInfo& c = P.cyl;
+    if (z < c.z_lo || z >= c.z_hi) return -1;
+    const float dx = x - c.ax, dy = y - c.ay;
+    const float r2 = dx * dx + dy * dy;
+    if (r2 < c.r_in_sq || r2 >= c.r_out_sq) return -1;
+    const int depth = edge_bin_index(z, c.z_edges, c.n_depth);
+    const int shell = edge_bin_index(r2, c.r_edges_sq, c.n_shells);
+    return (long long)depth * c.n_shells + shell;
+}
+
 // kernels.py:536 _deposit: quantize once, route by position into the scoring
 // grid of this particle's column, or into the unscored book.
 template <class Sink>
 __device__ __forceinline__ void deposit(const TransportParams& P, BlockBooks& B, long long base,
                                        float x, float y, float z, float amount, float factor,
                                        Sink& sink) {
-    if (point_inside(x, y, z, P.si)) {
-        const long long idx = flat_index(x, y, z, P.si);
+    const long long idx = scoring_index(P, x, y, z);
+    if (idx >= 0) {
         const long long q =
             (long long)((double)amount * (double)factor * kInvQuantum + 0.5);
         if (q != 0) sink.add(P, base + idx, (unsigned long long)q);
@@ -472,8 +515,14 @@ __device__ inline int generate_primary(const TransportParams& P, const GenDesc& 
             p.x = a.x; p.y = a.y; p.z = a.z;
             p.ux = dx * inv; p.uy = dy * inv; p.uz = dz * inv;
         }
-    } else {  // host-sampled record: the run's history, or the batch block's slot t (Dij)
-        const long long ri = G.forward ? record : (long long)t;
+    } else {  // host-sampled record: the run's history, or the batch block's slot t (Dij);
+              // resident phase space: a record drawn by the history's own stream
+        long long ri = G.forward ? record : (long long)t;
+        if (G.type == 5) {
+            const unsigned long long r =
+                ((unsigned long long)p.rng.next_u32() << 32) | (unsigned long long)p.rng.next_u32();
+            ri = (long long)__umul64hi(r, (unsigned long long)G.n_records);
+        }
         p.kind = G.up_kind ? __ldg(G.up_kind + ri) : kPhoton;
         p.e = __ldg(G.up_energy + ri);
         p.w = __ldg(G.up_weight + ri);

@@ -565,13 +565,20 @@ class B200Engine:
         if native.scoring_key != skey:
             if scoring is None:
                 scoring = model.ScoringGrid.for_grid(grid)
-            if _type_name(scoring) == "CylindricalScoringGrid":
-                raise ValueError("cylindrical scoring grids are not supported by the B200 backend")
             mass = np.ascontiguousarray(np.asarray(scoring.voxel_mass).reshape(-1), dtype=np.float64)
-            sdesc = _lib.ScoringDesc(nx=int(scoring.shape[0]), ny=int(scoring.shape[1]),
-                                     nz=int(scoring.shape[2]))
-            sdesc.origin[:] = [float(v) for v in scoring.origin]
-            sdesc.spacing[:] = [float(v) for v in scoring.spacing]
+            if _type_name(scoring) == "CylindricalScoringGrid":  # scoring/cylinder.py:172
+                depth = np.ascontiguousarray(scoring.depth_edges, dtype=np.float64)
+                radial = np.ascontiguousarray(scoring.radial_edges, dtype=np.float64)
+                native._keep = [mass, depth, radial]
+                sdesc = _lib.ScoringDesc(mode=1, n_depth=depth.size - 1, n_shells=radial.size - 1)
+                sdesc.axis[:] = [float(v) for v in scoring.axis]
+                sdesc.depth_edges = _lib.ptr(depth, C.c_double)
+                sdesc.radial_edges = _lib.ptr(radial, C.c_double)
+            else:
+                sdesc = _lib.ScoringDesc(nx=int(scoring.shape[0]), ny=int(scoring.shape[1]),
+                                         nz=int(scoring.shape[2]))
+                sdesc.origin[:] = [float(v) for v in scoring.origin]
+                sdesc.spacing[:] = [float(v) for v in scoring.spacing]
             sdesc.voxel_mass = _lib.ptr(mass, C.c_double)
             native.check(lib.pmc_set_scoring(native.handle, C.byref(sdesc)))
             native.scoring_key = skey
@@ -726,6 +733,24 @@ class B200Engine:
             src.v_axis[:] = [float(v) for v in source.v_axis]
             src.width_u = float(source.width_u)
             src.width_v = float(source.width_v)
+        elif name in ("PhaseSpaceSource", "InMemoryPhaseSpaceSource") and hasattr(source, "columns"):
+            # The whole phase space resident on the device, one record drawn per
+            # history from its own stream (PhaseSpaceSource.emit, geometry/phasespace.py:546).
+            cols = source.columns()
+            iaea_to_kind = np.array([-1, 0, 1, 2], dtype=np.int32)
+            kind = np.ascontiguousarray(iaea_to_kind[np.asarray(cols["particle_type"], dtype=np.int32)])
+            energy = np.ascontiguousarray(cols["energy"], dtype=np.float32)
+            pos = np.ascontiguousarray(np.stack([cols["x"], cols["y"], cols["z"]], axis=1), dtype=np.float32)
+            dirs = np.ascontiguousarray(np.stack([cols["ux"], cols["uy"], cols["uz"]], axis=1), dtype=np.float32)
+            weight = np.ascontiguousarray(cols["weight"], dtype=np.float32)
+            keep += [kind, energy, pos, dirs, weight]
+            src.type = _lib.PMC_SRC_PHASESPACE
+            src.n_records = int(energy.size)
+            src.up_kind = _lib.ptr(kind, C.c_int32)
+            src.up_energy = _lib.ptr(energy, C.c_float)
+            src.up_pos = _lib.ptr(pos, C.c_float)
+            src.up_dir = _lib.ptr(dirs, C.c_float)
+            src.up_weight = _lib.ptr(weight, C.c_float)
         elif hasattr(source, "sample_batch"):
             # Host pre-sampling route (Source.sample_batch): records in history order.
             cols = source.sample_batch(seed, 0, n_histories)

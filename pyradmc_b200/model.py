@@ -15,12 +15,17 @@ same names, fields and semantics, so the same calls work:
 * :class:`SpectralBeamletSource` geometry/source.py:637
 * :class:`CompositeBeamletSource` geometry/source.py:239
 * :class:`ScoringGrid`          scoring/grid.py:67 (``for_grid`` only)
+* :class:`CylindricalScoringGrid` scoring/cylinder.py:172, with
+  :func:`uniform_edges` and :func:`geometric_edges` (:62, :76)
 * :class:`RunProvenance`, :class:`TransportResult`  backends/results.py:19, :77
 * :class:`DijResult`            scoring/dij.py:195
 * :class:`ProgressEvent`, :class:`ProgressEmitter`  progress.py:30, :50
 * :class:`AnalyticWaterTables`  the analytic water source's flattened tables
   (data/analytic.py:117 + data/tables.py:222), served from the packs that
   ``pyradmc_b200/data/make_packs.py`` generated with pyRadMC's own builders.
+* :class:`PackedCrossSections`  any ``CrossSectionSource``'s flattened tables
+  and GS node grid (multi-material, analytic or tabulated EPICS,
+  data/tabulated/source.py:58), written by :func:`save_pack` where pyRadMC runs.
 """
 
 from __future__ import annotations
@@ -41,7 +46,9 @@ __all__ = [
     "BeamletGridSource",
     "CompositeBeamletSource",
     "ConcatenatedBeamletSource",
+    "CylindricalScoringGrid",
     "DijResult",
+    "PackedCrossSections",
     "ParallelBeamSource",
     "PencilBeamSource",
     "ProgressEmitter",
@@ -54,6 +61,9 @@ __all__ = [
     "TransportResult",
     "VoxelGrid",
     "ali_rogers_varian_6mv",
+    "geometric_edges",
+    "save_pack",
+    "uniform_edges",
 ]
 
 logger = logging.getLogger("pyradmc_b200.progress")
@@ -136,6 +146,139 @@ class ScoringGrid:
     @property
     def n_voxels(self) -> int:
         return int(self.shape[0] * self.shape[1] * self.shape[2])
+
+
+def uniform_edges(r_max: float, n_shells: int) -> np.ndarray:
+    """Equal-thickness shell edges 0 .. r_max (scoring/cylinder.py:62)."""
+    if n_shells < 1:
+        raise ValueError(f"a cylindrical scorer needs at least one shell, got {n_shells}")
+    if r_max <= 0.0:
+        raise ValueError(f"r_max must be positive, got {r_max}")
+    return np.linspace(0.0, r_max, n_shells + 1, dtype=np.float64)
+
+
+def geometric_edges(r_max: float, n_shells: int, r_min: float) -> np.ndarray:
+    """A central disc [0, r_min), then n_shells - 1 equal-ratio shells to r_max
+    (scoring/cylinder.py:76)."""
+    if n_shells < 2:
+        raise ValueError(
+            f"geometric edges need at least two shells (a central disc plus one "
+            f"geometric shell), got {n_shells}"
+        )
+    if r_max <= 0.0:
+        raise ValueError(f"r_max must be positive, got {r_max}")
+    if not 0.0 < r_min < r_max:
+        raise ValueError(f"need 0 < r_min < r_max, got r_min={r_min}, r_max={r_max}")
+    return np.concatenate(([0.0], np.geomspace(r_min, r_max, n_shells, dtype=np.float64)))
+
+
+def _check_edges(depth, radial) -> tuple[np.ndarray, np.ndarray]:
+    depth = np.asarray(depth, dtype=np.float64)
+    radial = np.asarray(radial, dtype=np.float64)
+    if depth.ndim != 1 or depth.size < 2:
+        raise ValueError("depth_edges needs at least one depth bin, i.e. two depths")
+    if np.any(np.diff(depth) <= 0.0):
+        raise ValueError("depth_edges must be strictly increasing")
+    if radial.ndim != 1 or radial.size < 2:
+        raise ValueError("radial_edges needs at least one shell, i.e. two radii")
+    if np.any(radial < 0.0):
+        raise ValueError("negative radial edge")
+    if np.any(np.diff(radial) <= 0.0):
+        raise ValueError("radial_edges must be strictly increasing")
+    return depth, radial
+
+
+@dataclass(frozen=True)
+class CylindricalScoringGrid:
+    """Depth bins by radial shells about an axis parallel to z, the pencil-beam
+    kernel geometry (scoring/cylinder.py:172): a scoring geometry only, the
+    transport stays on the voxel grid.  Bins are half-open on both axes; the
+    shell mass is analytic, ``rho * pi * (r_out^2 - r_in^2) * dz``, which is
+    why :meth:`for_grid` refuses a medium that is not uniform over the bins."""
+
+    axis: tuple[float, float]
+    depth_edges: np.ndarray
+    radial_edges: np.ndarray
+    voxel_mass: np.ndarray
+
+    def __post_init__(self) -> None:
+        depth, radial = _check_edges(self.depth_edges, self.radial_edges)
+        mass = np.asarray(self.voxel_mass, dtype=np.float64)
+        if mass.shape != (depth.size - 1, radial.size - 1):
+            raise ValueError(
+                f"voxel_mass shape {mass.shape} != {(depth.size - 1, radial.size - 1)} "
+                "(n_depth, n_shells)")
+        if np.any(mass < 0.0):
+            raise ValueError("negative shell mass")
+        object.__setattr__(self, "depth_edges", depth)
+        object.__setattr__(self, "radial_edges", radial)
+        object.__setattr__(self, "voxel_mass", mass)
+
+    @classmethod
+    def uniform(cls, density: float, axis, depth_edges, radial_edges) -> CylindricalScoringGrid:
+        """Bins in a medium of the stated uniform density (scoring/cylinder.py:274)."""
+        if density <= 0.0:
+            raise ValueError(f"non-positive density {density}")
+        depth, radial = _check_edges(depth_edges, radial_edges)
+        shell_area = math.pi * (radial[1:] ** 2 - radial[:-1] ** 2)
+        mass = density * np.outer(np.diff(depth), shell_area)
+        return cls(axis=tuple(axis), depth_edges=depth, radial_edges=radial, voxel_mass=mass)
+
+    @classmethod
+    def for_grid(cls, grid, radial_edges, axis=None, depth_edges=None) -> CylindricalScoringGrid:
+        """Bins spanning a transport phantom, density read from it and checked
+        uniform over every voxel the cylinder meets (scoring/cylinder.py:311)."""
+        edges = np.asarray(radial_edges, dtype=np.float64)
+        if edges.ndim != 1 or edges.size < 2:
+            raise ValueError("radial_edges needs at least one shell, i.e. two radii")
+        lo = np.asarray(grid.origin, dtype=np.float64)
+        hi = lo + np.asarray(grid.shape) * np.asarray(grid.spacing, dtype=np.float64)
+        if axis is None:
+            axis = (0.5 * (lo[0] + hi[0]), 0.5 * (lo[1] + hi[1]))
+        if depth_edges is None:
+            n_depth = max(1, math.floor((hi[2] - lo[2]) / grid.spacing[2]))
+            depth_edges = lo[2] + grid.spacing[2] * np.arange(n_depth + 1, dtype=np.float64)
+        depth = np.asarray(depth_edges, dtype=np.float64)
+        r_max = float(edges[-1])
+        if (axis[0] - r_max < lo[0] or axis[0] + r_max > hi[0] or axis[1] - r_max < lo[1]
+                or axis[1] + r_max > hi[1] or depth[0] < lo[2] or depth[-1] > hi[2]):
+            raise ValueError(
+                f"the scoring cylinder (axis {tuple(axis)}, r_max {r_max} cm, depth "
+                f"[{depth[0]}, {depth[-1]}) cm) reaches outside the transport grid "
+                f"{tuple(lo)} to {tuple(hi)}; its shells would claim mass the phantom does not have")
+        nx, ny, nz = grid.shape
+        sx, sy, sz = grid.spacing
+        x0 = lo[0] + sx * np.arange(nx)
+        y0 = lo[1] + sy * np.arange(ny)
+        z0 = lo[2] + sz * np.arange(nz)
+        dx = np.maximum(0.0, np.maximum(x0 - axis[0], axis[0] - (x0 + sx)))
+        dy = np.maximum(0.0, np.maximum(y0 - axis[1], axis[1] - (y0 + sy)))
+        lateral = (dx[:, None] ** 2 + dy[None, :] ** 2) < r_max**2
+        deep = (z0 + sz > depth[0]) & (z0 < depth[-1])
+        overlaps = lateral[:, :, None] & deep[None, None, :]
+        densities = np.unique(np.asarray(grid.density)[overlaps])
+        materials = np.unique(np.asarray(grid.material)[overlaps])
+        if densities.size != 1 or materials.size != 1:
+            raise ValueError(
+                "cylindrical scoring needs a uniform medium over the binned region "
+                f"(found {densities.size} densities and {materials.size} materials there)")
+        return cls.uniform(float(densities[0]), axis, depth, edges)
+
+    @property
+    def n_depth(self) -> int:
+        return self.depth_edges.size - 1
+
+    @property
+    def n_shells(self) -> int:
+        return self.radial_edges.size - 1
+
+    @property
+    def shape(self) -> tuple[int, int]:
+        return (self.n_depth, self.n_shells)
+
+    @property
+    def n_voxels(self) -> int:
+        return self.n_depth * self.n_shells
 
 
 # ---- sources ----------------------------------------------------------------------
@@ -670,3 +813,82 @@ def gs_grid_from_pack(tables, materials):
         raise ValueError("the packed Goudsmit-Saunderson grid does not cover this run's window; "
                          "use pyRadMC's build_gs_grid")
     return g
+
+
+# ---- any cross-section source, packed ---------------------------------------------
+PACK_TABLE_FIELDS = ("mu_compton", "mu_photo", "mu_pair", "mu_rayleigh", "majorant",
+                     "stopping_restricted", "stopping_radiative", "moller", "csda_range",
+                     "scattering_power", "log_eta", "restricted_range",
+                     "energy_of_restricted_range", "coherent_x", "coherent_cumulative")
+PACK_TABLE_SCALARS = ("n_points", "ecut", "pcut", "e_max", "photon_log_e_min", "photon_inv_dlog",
+                      "electron_log_e_min", "electron_inv_dlog", "range_log_r_min",
+                      "range_inv_dlog", "n_coherent")
+
+
+def save_pack(cross_sections, path, *, ecut: float, pcut: float, e_max: float,
+              materials: Sequence[int]) -> None:
+    """Write one ``CrossSectionSource``'s flattened tables
+    (``build_tables(ecut, pcut, e_max)``, data/interface.py:413) and the
+    Goudsmit-Saunderson node grid of the window its `materials` reach
+    (``build_gs_grid(*gs_window_from_tables(tables, materials))``,
+    data/goudsmit_saunderson.py:1108, :1222) to `path`, for
+    :class:`PackedCrossSections`.  Needs pyRadMC; `e_max` is the table edge
+    (the primary energy times the engine's 1 + 1e-6 margin)."""
+    from pyradmc.data.goudsmit_saunderson import build_gs_grid, gs_window_from_tables
+
+    tab = cross_sections.build_tables(ecut=ecut, pcut=pcut, e_max=e_max)
+    gs = build_gs_grid(*gs_window_from_tables(tab, list(materials)))
+    payload = {name: np.asarray(getattr(tab, name), dtype=np.float64) for name in PACK_TABLE_FIELDS}
+    payload.update({name: np.asarray(getattr(tab, name)) for name in PACK_TABLE_SCALARS})
+    payload.update(gs_values=np.asarray(gs.values, dtype=np.float32), gs_ix0=np.int64(gs.ix0),
+                   gs_iy0=np.int64(gs.iy0), gs_n_u=np.int64(gs.n_u),
+                   gs_bins_per_log=np.float64(gs.bins_per_log),
+                   gs_materials=np.asarray(sorted({int(m) for m in materials}), dtype=np.int64),
+                   n_materials=np.int64(cross_sections.n_materials),
+                   provenance=np.asarray(str(getattr(cross_sections, "provenance",
+                                                     type(cross_sections).__name__))))
+    np.savez_compressed(path, **payload)
+
+
+class PackedCrossSections:
+    """A ``CrossSectionSource`` for the B200 engine from a :func:`save_pack`
+    file: the flattened tables of any number of materials and the GS node grid
+    they need, built where pyRadMC (and its data, such as the EPICS libraries
+    of ``TabulatedCrossSections``) is available and used where it is not.
+
+    ``build_tables`` serves the packed tables for exactly the packed
+    (ecut, pcut, e_max); ``gs_grid_for`` serves the packed grid when it covers
+    the requested materials' window, and raises otherwise."""
+
+    def __init__(self, path) -> None:
+        with np.load(path) as z:
+            data = {k: z[k] for k in z.files}
+        self._fields = {k: data[k] for k in PACK_TABLE_FIELDS}
+        for k in ("n_points", "n_coherent"):
+            self._fields[k] = int(data[k])
+        for k in PACK_TABLE_SCALARS:
+            if k not in ("n_points", "n_coherent"):
+                self._fields[k] = float(data[k])
+        self._gs = SimpleNamespace(values=np.ascontiguousarray(data["gs_values"], dtype=np.float32),
+                                   ix0=int(data["gs_ix0"]), iy0=int(data["gs_iy0"]),
+                                   n_u=int(data["gs_n_u"]), bins_per_log=float(data["gs_bins_per_log"]))
+        self._gs_materials = {int(m) for m in data["gs_materials"]}
+        self.n_materials = int(data["n_materials"])
+        self.provenance = str(data["provenance"])
+
+    def build_tables(self, ecut: float, pcut: float, e_max: float, n_points=None):
+        f = self._fields
+        if not (math.isclose(f["e_max"], e_max, rel_tol=0, abs_tol=1e-12)
+                and f["ecut"] == ecut and f["pcut"] == pcut
+                and (n_points is None or n_points == f["n_points"])):
+            raise ValueError(
+                f"this pack holds tables at ecut={f['ecut']}, pcut={f['pcut']}, e_max={f['e_max']}; "
+                f"requested ecut={ecut}, pcut={pcut}, e_max={e_max}")
+        return SimpleNamespace(**f)
+
+    def gs_grid_for(self, tables, materials: Sequence[int]):
+        wanted = {int(m) for m in materials}
+        if not wanted <= self._gs_materials:
+            raise ValueError(f"the packed GS grid covers materials {sorted(self._gs_materials)}, "
+                             f"not {sorted(wanted)}")
+        return self._gs

@@ -19,7 +19,15 @@ for p in (str(ROOT), str(GOLDEN)):
     if p not in sys.path:
         sys.path.insert(0, p)
 
-from cases import CASES, CT_CASE, SEED, layered_density, make_source  # noqa: E402
+from cases import (  # noqa: E402
+    CASES,
+    CT_CASE,
+    SEED,
+    layered_density,
+    layered_material,
+    make_scoring,
+    make_source,
+)
 
 
 def pytest_sessionfinish(session, exitstatus):
@@ -67,17 +75,29 @@ def build_case(name: str):
     g = case["grid"]
     grid = P.VoxelGrid.uniform_water(g["shape"], g["spacing"])
     if "layers" in g:
+        material = grid.material
+        if "material_layers" in g:
+            material = layered_material(g["shape"], g["spacing"], (0, 0, 0), g["material_layers"])
         grid = P.VoxelGrid(shape=g["shape"], spacing=g["spacing"],
                            density=layered_density(g["shape"], g["spacing"], (0, 0, 0), g["layers"]),
-                           material=grid.material)
+                           material=material)
     from types import SimpleNamespace
+
+    from pyradmc_b200.phasespace import PhaseSpaceSource
 
     ns = SimpleNamespace(**{name: getattr(P, name) for name in (
         "PencilBeamSource", "ParallelBeamSource", "SpectralBeamSource", "BeamletGridSource",
-        "SpectralBeamletSource", "CompositeBeamletSource")}, spectrum=P.ali_rogers_varian_6mv)
+        "SpectralBeamletSource", "CompositeBeamletSource")}, spectrum=P.ali_rogers_varian_6mv,
+        PhaseSpaceSource=PhaseSpaceSource)
     src = make_source(case["source"], ns)
-    xs = P.AnalyticWaterTables(geometry_densities=grid.max_density_by_material())
-    return grid, xs, src, dict(case["run"])
+    if case.get("cross_sections") == "water_bone":
+        xs = P.PackedCrossSections(GOLDEN / "pack_water_bone.npz")
+    else:
+        xs = P.AnalyticWaterTables(geometry_densities=grid.max_density_by_material())
+    run = dict(case["run"])
+    if "scoring" in case:
+        run["scoring_grid"] = make_scoring(case, grid, P)
+    return grid, xs, src, run
 
 
 def build_ct_case():

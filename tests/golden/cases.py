@@ -19,6 +19,8 @@ SEED = 20260711  # the reference test suite's fixed seed (tests/conftest.py:25)
 # Water slab with a density step, for the heterogeneous spectral case: water,
 # lung 0.26, bone 1.85, water, by voxel-centre depth in cm.
 SLAB_LAYERS = ((0.0, 3.0, 1.0), (3.0, 7.0, 0.26), (7.0, 9.0, 1.85), (9.0, 1.0e9, 1.0))
+BONE_LAYERS = ((0.0, 2.0, 1.0), (2.0, 4.0, 1.85), (4.0, 1.0e9, 1.0))
+BONE_MATERIAL = 4  # cortical_bone in pyRadMC's registry (data/materials.py:295)
 
 CASES: dict[str, dict] = {
     "kerma_slab": dict(
@@ -70,6 +72,45 @@ CASES: dict[str, dict] = {
                     width_u=1.5, width_v=1.5),
         run=dict(n_histories_per_beamlet=480, n_batches=8, seed=SEED, truncation=0.0),
     ),
+    # An IAEA phase space (tests/golden/phsp_beam.*, written by make_golden.py):
+    # a divergent 6 x 6 cm field of 6 MV photons with electron and positron
+    # contamination at non-unit weights, sampled with replacement.
+    "phasespace": dict(
+        grid=dict(shape=(16, 16, 16), spacing=(0.5, 0.5, 0.5)),
+        source=dict(kind="phasespace", file="phsp_beam"),
+        run=dict(n_histories=80_000, n_batches=10, seed=SEED),
+        shards=10,
+    ),
+    # A 6 MeV pencil-beam kernel scored in depth bins by radial shells
+    # (CylindricalScoringGrid.for_grid, scoring/cylinder.py:311): a central
+    # 1 mm disc and 11 geometric shells out to 6 cm, depth bins on the grid's
+    # z planes.
+    "pencil_cylinder": dict(
+        grid=dict(shape=(16, 16, 16), spacing=(1.0, 1.0, 1.0)),
+        source=dict(kind="pencil", energy=6.0, position=(8.0, 8.0, -1.0), direction=(0.0, 0.0, 1.0)),
+        run=dict(n_histories=200_000, n_batches=10, seed=SEED),
+        scoring=dict(kind="cylinder", r_max=6.0, n_shells=12, r_min=0.1),
+        shards=10,
+    ),
+    # Dose to water and dose to medium behind a cortical-bone layer (material 4
+    # of pyRadMC's registry at 1.85 g/cc) in water: the stopping-power ratio
+    # water/bone weights every bone deposit (scoring/dose_to_water.py:67-84).
+    # The cross sections are the analytic source with the registry's first
+    # five materials addressable, packed in pack_water_bone.npz.
+    "dtw_bone": dict(
+        grid=dict(shape=(16, 16, 30), spacing=(0.5, 0.5, 0.2), layers=BONE_LAYERS,
+                  material_layers=((2.0, 4.0, 4),)),
+        source=dict(kind="parallel", energy=6.0, z=-1.0, x_range=(0.0, 8.0), y_range=(0.0, 8.0)),
+        run=dict(n_histories=80_000, n_batches=10, seed=SEED, scoring_mode="dose_to_water"),
+        cross_sections="water_bone", shards=10,
+    ),
+    "dtm_bone": dict(
+        grid=dict(shape=(16, 16, 30), spacing=(0.5, 0.5, 0.2), layers=BONE_LAYERS,
+                  material_layers=((2.0, 4.0, 4),)),
+        source=dict(kind="parallel", energy=6.0, z=-1.0, x_range=(0.0, 8.0), y_range=(0.0, 8.0)),
+        run=dict(n_histories=80_000, n_batches=10, seed=SEED, scoring_mode="dose_to_medium"),
+        cross_sections="water_bone", shards=10,
+    ),
     # A fan entering through the -x face (its aperture axes y and z): the
     # geometry of a beam of a coplanar plan at gantry angle 90 degrees.
     "dij_oblique": dict(
@@ -97,8 +138,8 @@ CASES: dict[str, dict] = {
 def make_source(s: dict, ns):
     """A case's source built from the classes of `ns` (pyRadMC's modules or this
     package): PencilBeamSource, ParallelBeamSource, SpectralBeamSource,
-    BeamletGridSource, SpectralBeamletSource, CompositeBeamletSource and a
-    6 MV spectrum factory ``spectrum()``."""
+    BeamletGridSource, SpectralBeamletSource, CompositeBeamletSource,
+    PhaseSpaceSource and a 6 MV spectrum factory ``spectrum()``."""
     kind = s["kind"]
     if kind == "parallel":
         return ns.ParallelBeamSource(s["energy"], s["z"], s["x_range"], s["y_range"])
@@ -115,6 +156,10 @@ def make_source(s: dict, ns):
                                         s["width_v"], **axes)
     if kind == "composite":
         return ns.CompositeBeamletSource([(make_source(c, ns), w) for c, w in s["components"]])
+    if kind == "phasespace":
+        from pathlib import Path
+
+        return ns.PhaseSpaceSource(Path(__file__).resolve().parent / s["file"])
     raise ValueError(kind)
 
 
@@ -131,6 +176,28 @@ CT_CASE = dict(
     run=dict(n_batches=10, seed=SEED, truncation=0.0),
     counts=(40_000, 120_000),
 )
+
+
+def make_scoring(case: dict, grid, ns):
+    """The case's scoring geometry built with `ns` (CylindricalScoringGrid and
+    geometric_edges), or None for the transport grid."""
+    sc = case.get("scoring")
+    if sc is None:
+        return None
+    return ns.CylindricalScoringGrid.for_grid(grid, ns.geometric_edges(sc["r_max"], sc["n_shells"],
+                                                                       sc["r_min"]))
+
+
+def layered_material(shape, spacing, origin, layers):
+    """Material index by voxel-centre depth: (z_lo, z_hi, material) slabs along z."""
+    import numpy as np
+
+    nz = shape[2]
+    z = origin[2] + (np.arange(nz) + 0.5) * spacing[2]
+    column = np.zeros(nz, dtype=np.int32)
+    for lo, hi, m in layers:
+        column[(z >= lo) & (z < hi)] = m
+    return np.broadcast_to(column, shape).copy()
 
 
 def layered_density(shape, spacing, origin, layers):

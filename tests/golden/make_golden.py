@@ -44,7 +44,14 @@ import numpy as np
 HERE = Path(__file__).resolve().parent
 sys.path.insert(0, str(HERE))
 
-from cases import CASES, CT_CASE, layered_density, make_source  # noqa: E402
+from cases import (  # noqa: E402
+    CASES,
+    CT_CASE,
+    layered_density,
+    layered_material,
+    make_scoring,
+    make_source,
+)
 
 REFERENCE: str | None = None  # path of the pyRadMC checkout, set by __main__ and the workers
 
@@ -60,7 +67,44 @@ def _reference_sources():
         SpectralBeamSource=S.SpectralBeamSource, BeamletGridSource=S.BeamletGridSource,
         SpectralBeamletSource=S.SpectralBeamletSource,
         CompositeBeamletSource=S.CompositeBeamletSource,
+        PhaseSpaceSource=_reference_phsp,
         spectrum=lambda: ali_rogers_mv("varian-6mv", e_min=0.1))
+
+
+def _reference_phsp(path):
+    import warnings
+
+    from pyradmc.geometry.phasespace import PhaseSpaceSource
+
+    warnings.filterwarnings("ignore", message=".*latent variance")  # oversampling is intended
+    return PhaseSpaceSource(path)
+
+
+def make_phsp_file() -> None:
+    """tests/golden/phsp_beam.IAEAheader/.IAEAphsp: 20,000 seeded records, a
+    divergent 6 x 6 cm field at z = -0.5 cm from a focal spot 100 cm above
+    the phantom centre: 90 % photons of the 6 MV spectrum, 8 % electrons and
+    2 % positrons of 0.5-3 MeV, weights U(0.5, 1.5)."""
+    sys.path.insert(0, str(HERE.parents[1]))
+    from pyradmc.geometry.spectrum import ali_rogers_mv
+
+    from pyradmc_b200.phasespace import write_iaea
+
+    rng = np.random.default_rng(20260901)
+    n = 20_000
+    kind = rng.choice([1, 2, 3], size=n, p=[0.90, 0.08, 0.02]).astype(np.int32)
+    spectrum = ali_rogers_mv("varian-6mv", e_min=0.1)
+    u = rng.random((n, 2))
+    energy = spectrum.sample_energies(u[:, 0], u[:, 1])
+    energy = np.where(kind == 1, energy, rng.uniform(0.5, 3.0, size=n))
+    x = rng.uniform(1.0, 7.0, size=n)
+    y = rng.uniform(1.0, 7.0, size=n)
+    z = np.full(n, -0.5)
+    d = np.stack([x - 4.0, y - 4.0, z + 100.0], axis=1)
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    write_iaea(HERE / "phsp_beam", dict(particle_type=kind, energy=energy, x=x, y=y, z=z, ux=d[:, 0],
+                                        uy=d[:, 1], uz=d[:, 2], weight=rng.uniform(0.5, 1.5, size=n)))
+    print("phsp_beam written", flush=True)
 
 
 def build_case(name: str):
@@ -72,11 +116,58 @@ def build_case(name: str):
     grid = VoxelGrid.uniform_water(g["shape"], g["spacing"])
     if "layers" in g:
         density = layered_density(g["shape"], g["spacing"], (0.0, 0.0, 0.0), g["layers"])
-        grid = VoxelGrid(shape=g["shape"], spacing=g["spacing"], density=density,
-                         material=grid.material)
+        material = grid.material
+        if "material_layers" in g:
+            material = layered_material(g["shape"], g["spacing"], (0.0, 0.0, 0.0), g["material_layers"])
+        grid = VoxelGrid(shape=g["shape"], spacing=g["spacing"], density=density, material=material)
     source = make_source(case["source"], _reference_sources())
-    xs = AnalyticCrossSections(geometry_densities=grid.max_density_by_material())
-    return grid, xs, source, case["run"]
+    if case.get("cross_sections") == "water_bone":
+        xs = water_and_bone(grid.max_density_by_material())
+    else:
+        xs = AnalyticCrossSections(geometry_densities=grid.max_density_by_material())
+    run = dict(case["run"])
+    if "scoring" in case:
+        from types import SimpleNamespace
+
+        from pyradmc.scoring.cylinder import CylindricalScoringGrid, geometric_edges
+
+        run["scoring_grid"] = make_scoring(case, grid, SimpleNamespace(
+            CylindricalScoringGrid=CylindricalScoringGrid, geometric_edges=geometric_edges))
+    return grid, xs, source, run
+
+
+def water_and_bone(geometry_densities):
+    """pyRadMC's analytic source with the first five materials of its registry
+    addressable (water ... cortical bone): Compton, stopping powers, Moller and
+    scattering power follow each material's composition; the photoelectric,
+    pair and radiative fits stay water's.  A synthetic multi-material source for
+    the dose-to-water parity case."""
+    from pyradmc.data.analytic import AnalyticCrossSections
+
+    class WaterAndBone(AnalyticCrossSections):
+        @property
+        def n_materials(self) -> int:
+            return 5
+
+        @property
+        def provenance(self) -> str:
+            return "analytic closed-form, registry materials 0-4 (synthetic multi-material test source)"
+
+    return WaterAndBone(geometry_densities=geometry_densities)
+
+
+def make_bone_pack() -> None:
+    """tests/golden/pack_water_bone.npz: the water_and_bone tables at 6 MeV and
+    the GS grid of water + cortical bone."""
+    sys.path.insert(0, str(HERE.parents[1]))
+    from pyradmc_b200.model import save_pack
+
+    from cases import BONE_MATERIAL
+
+    xs = water_and_bone(((0, 1.0), (BONE_MATERIAL, 1.85)))
+    save_pack(xs, HERE / "pack_water_bone.npz", ecut=0.2, pcut=0.05, e_max=6.0 * (1 + 1e-6),
+              materials=[0, BONE_MATERIAL])
+    print("pack_water_bone written", flush=True)
 
 
 def _combine_batches(batch_means: np.ndarray):
@@ -167,10 +258,11 @@ def _warm_gs_cache(name: str) -> None:
     worker at once."""
     from pyradmc.data.goudsmit_saunderson import build_gs_grid, gs_window_from_tables
 
-    _, xs, source, _ = build_case(name)
+    grid, xs, source, _ = build_case(name)
+    materials = sorted({int(m) for m in np.unique(grid.material)})
     for e_max in (source.max_energy, 6.0):
         tables = xs.build_tables(ecut=0.2, pcut=0.05, e_max=e_max * (1 + 1e-6))
-        build_gs_grid(*gs_window_from_tables(tables, [0]))
+        build_gs_grid(*gs_window_from_tables(tables, materials))
 
 
 def run_sharded(name: str) -> None:
@@ -180,7 +272,9 @@ def run_sharded(name: str) -> None:
     with _pool(shards) as pool:
         parts = list(pool.map(_forward_shard, [(name, k) for k in range(shards)]))
     elapsed = time.perf_counter() - t0
-    grid_shape = CASES[name]["grid"]["shape"]
+    grid, _, _, run_kw = build_case(name)
+    scoring = run_kw.get("scoring_grid")
+    grid_shape = tuple(scoring.shape) if scoring is not None else tuple(grid.shape)
     mean, sigma = _combine_batches(np.stack([p[0] for p in parts]))
     books = np.sum([p[1] for p in parts], axis=0)
     run = CASES[name]["run"]
@@ -299,10 +393,14 @@ if __name__ == "__main__":
         raise SystemExit("usage: python tests/golden/make_golden.py /path/to/pyRadMC [case ...]")
     REFERENCE = sys.argv[1]
     sys.path.insert(0, REFERENCE)
-    names = sys.argv[2:] or ["reduction", *CASES, "ct_beamlets"]
+    names = sys.argv[2:] or ["reduction", "bone_pack", "phsp_file", *CASES, "ct_beamlets"]
     for name in names:
         if name == "reduction":
             make_reduction()
+        elif name == "bone_pack":
+            make_bone_pack()
+        elif name == "phsp_file":
+            make_phsp_file()
         elif name == "ct_beamlets":
             run_ct()
         else:

@@ -58,3 +58,29 @@ def test_coarse_and_partial_scoring_grids_book_exactly_the_transport_grid_energy
                                                                           rel=1e-12)
     balance = (part.energy_deposited + part.energy_escaped + part.energy_unscored) / part.energy_emitted
     assert abs(balance - 1.0) < 1e-4, balance
+
+
+def test_cylindrical_scoring_books_the_energy_of_the_voxel_grid_run(gpu):
+    """Depth bins by radial shells (CylindricalScoringGrid, scoring/cylinder.py:
+    172) only decide where a deposit is filed: with the same seed the transport
+    is identical, so scored plus unscored energy is the voxel-grid run's to the
+    quantum, the escaped energy is unchanged, and the shells' dose times their
+    analytic mass adds up to the scored energy."""
+    import pyradmc_b200 as P
+    from tests.conftest import build_case
+
+    grid, xs, src, run = build_case("pencil_cylinder")
+    cyl = run.pop("scoring_grid")
+    run["n_histories"] = 40_000
+    engine = P.B200Engine(grid, xs, device=gpu)
+    shells = engine.run(src, scoring_grid=cyl, **run)
+    voxels = engine.run(src, **run)
+    assert shells.dose.shape == cyl.shape == (16, 12)
+    assert (shells.energy_deposited + shells.energy_unscored
+            == voxels.energy_deposited + voxels.energy_unscored)
+    assert shells.energy_escaped == voxels.energy_escaped
+    assert (shells.dose * cyl.voxel_mass).sum() * run["n_histories"] == pytest.approx(
+        shells.energy_deposited, rel=1e-9)
+    assert 0.0 < shells.energy_unscored < shells.energy_deposited  # the box corners lie outside
+    # the pencil's axis: the central disc carries the highest dose of every depth past build-up
+    assert np.all(np.argmax(shells.dose[4:], axis=1) == 0)

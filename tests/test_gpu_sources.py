@@ -71,8 +71,11 @@ def test_concatenated_beams_are_the_separate_dijs_bit_for_bit(gpu):
     beam_z = _fan((4.0, 4.0, -100.0), [(3.0, 3.0, 0.0), (5.0, 5.0, 0.0)])
     beam_x = _fan((-100.0, 4.0, 4.0), [(4.0, 3.0, 3.0), (4.0, 5.0, 5.0), (4.0, 4.0, 4.0)],
                   u=(0.0, 1.0, 0.0), v=(0.0, 0.0, 1.0))
-    lattice = P.BeamletGridSource(6.0, -1.0, (1.0, 7.0), (1.0, 7.0), 2, 1)
+    # every part at the fans' top energy: the tables' log-energy nodes depend on
+    # the call's maximum energy, so only then are the runs' physics tables equal
+    lattice = P.BeamletGridSource(beam_z.max_energy, -1.0, (1.0, 7.0), (1.0, 7.0), 2, 1)
     plan = P.ConcatenatedBeamletSource([beam_z, beam_x, lattice])
+    assert plan.max_energy == lattice.max_energy == beam_x.max_energy
     kw = dict(n_batches=4, seed=SEED, truncation=1e-3)
     engine = P.B200Engine(grid, xs)
     whole = engine.run_dij(plan, n_histories_per_beamlet=[4000, 8000, 4000, 4000, 8000, 4000, 4000], **kw)
@@ -136,3 +139,40 @@ def test_a_failing_host_sampler_raises_its_own_exception(gpu):
     with pytest.raises(KeyError, match="no such beamlet file"):
         P.B200Engine(grid, xs).run_dij(Broken(_fan((2.0, 2.0, -100.0), [(2.0, 2.0, 0.0)])),
                                        n_histories_per_beamlet=100, n_batches=2, seed=SEED)
+
+
+class _HostSampled:
+    """The phase space seen only through ``sample_batch``: the host
+    pre-sampling route pyRadMC's Warp engine takes (engine.py:2833-2877)."""
+
+    def __init__(self, inner):
+        self.inner = inner
+        self.max_energy = inner.max_energy
+
+    def sample_batch(self, seed, history_offset, n):
+        return self.inner.sample_batch(seed, history_offset, n)
+
+
+def test_resident_phase_space_matches_host_sampling_and_closes_the_ledger(gpu):
+    grid, xs, src, run = build_case("phasespace")
+    engine = P.B200Engine(grid, xs)
+    resident = engine.run(src, **run)
+    host = engine.run(_HostSampled(src), **run)
+    mask = stats.high_dose_mask(resident.dose, resident.dose_sigma, host.dose_sigma, minimum=200)
+    stats.assert_chi2_consistent_batched(resident.dose, resident.dose_sigma, run["n_batches"],
+                                         host.dose, host.dose_sigma, run["n_batches"], mask=mask,
+                                         case="phase space: resident vs host-sampled")
+    for r in (resident, host):  # weights and kinds (positron rest mass) threaded end to end
+        balance = r.energy_deposited + r.energy_escaped + r.energy_unscored
+        assert balance == pytest.approx(r.energy_emitted, rel=1e-4)
+    assert resident.energy_emitted == pytest.approx(host.energy_emitted, rel=0.02)
+
+
+def test_resident_phase_space_is_bit_inert_to_scheduling(gpu):
+    grid, xs, src, run = build_case("phasespace")
+    run["n_histories"] = 20_000
+    a = P.B200Engine(grid, xs).run(src, **run)
+    b = P.B200Engine(grid, xs, chunk_size=999, use_graph=False, tail_steps=5).run(src, **run)
+    np.testing.assert_array_equal(a.dose, b.dose)
+    np.testing.assert_array_equal(a.dose_sigma, b.dose_sigma)
+    assert a.energy_emitted == b.energy_emitted

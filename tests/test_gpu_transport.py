@@ -66,6 +66,33 @@ def test_dij_columns_match_reference_engine(gpu, name):
                                              mask=mask, case=f"{name} column {j}")
 
 
+def test_dose_to_water_weights_the_bone_deposits_by_the_stopping_power_ratio(gpu):
+    """The same histories scored both ways (scoring draws no random numbers):
+    water voxels away from the bone get identical doses, bone voxels get the
+    medium dose times the water/bone restricted stopping-power ratio at the
+    depositing electron's energy (scoring/dose_to_water.py:67-84), a ratio
+    bounded by the table's values from ECUT up."""
+    grid, xs, src, run = build_case("dtw_bone")
+    engine = P.B200Engine(grid, xs)
+    run.pop("scoring_mode")
+    w = engine.run(src, scoring_mode="dose_to_water", **run)
+    m = engine.run(src, scoring_mode="dose_to_medium", **run)
+    bone = np.asarray(grid.material) != 0
+    near = bone.copy()
+    near[:, :, 1:] |= bone[:, :, :-1]
+    near[:, :, :-1] |= bone[:, :, 1:]
+    np.testing.assert_array_equal(w.dose[~near], m.dose[~near])
+    tab = xs.build_tables(0.2, 0.05, 6.0 * (1 + 1e-6))
+    s = np.asarray(tab.stopping_restricted)
+    e = np.exp(tab.electron_log_e_min + np.arange(tab.n_points) / tab.electron_inv_dlog)
+    spr = (s[0] / s[4])[e >= 0.2]
+    hit = bone & (m.dose > 0.05 * m.dose.max())
+    ratio = w.dose[hit] / m.dose[hit]
+    assert spr.min() * (1 - 1e-6) <= ratio.min() and ratio.max() <= spr.max() * (1 + 1e-6)
+    assert ratio.mean() > 1.02  # water stops electrons better than cortical bone per gram
+    assert w.energy_deposited == m.energy_deposited  # the ledger books physical energy
+
+
 def test_ct_phantom_with_uneven_counts_matches_reference_engine(gpu):
     """The benchmark's Dij at reduced size: a 40^3 CT-like phantom (seeded
     ellipsoids of density 0.2-1.9 g/cc), 5 mm 6 MV spectral beamlets, uneven
