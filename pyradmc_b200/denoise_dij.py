@@ -303,10 +303,16 @@ def run_dij_denoised(engine, net: UNet3D | None, source, n_histories_per_beamlet
     """A Dij from low-history Monte Carlo plus the denoiser: the engine runs the
     beamlets (``run_dij_device``), every column's window around its beamlet is
     replaced by the network's estimate, and the dense columns are truncated and
-    compacted to CSC on the device.  The per-entry sigma is the Monte Carlo
-    sigma of the input run.  With ``to_host`` False the CSC entries stay on
-    the device (torch tensors in the result).  With ``net`` None this is plain
-    Monte Carlo (``engine.run_dij``), the method's fallback."""
+    compacted to CSC on the device.  With ``to_host`` False the CSC entries
+    stay on the device (torch tensors in the result).  With ``net`` None this is
+    plain Monte Carlo (``engine.run_dij``), the method's fallback.
+
+    The per-entry ``sigma`` of the result is the batch sigma of the
+    low-history Monte Carlo input, not an uncertainty of the denoised value:
+    the network's estimate is smoother than its input and is judged against
+    high-statistics Monte Carlo instead (:func:`sigma_equivalent_error`,
+    :func:`relative_bias`).  A consumer that weights entries by ``sigma``
+    (a robust optimizer) reads the input's noise level."""
     import torch
 
     from .engine import ENERGY_QUANTUM_MEV, _result_types
@@ -379,4 +385,39 @@ def sigma_equivalent_error(estimate, reference, reference_sigma=None, threshold:
             own = (reference_sigma[c].to(torch.float64)[sel] / r[sel]).median().item()
             rel = float(np.sqrt(max(rel * rel - own * own, 0.0)))
         out[c] = rel
+    return out
+
+
+def relative_bias(estimate, reference, threshold: float = 0.1):
+    """Per-column signed bias of dense columns [C, vox] against a
+    high-statistics reference over the voxels where the reference is at least
+    `threshold` of its column maximum: (mean of (est - ref) / ref, and the
+    integral (sum est - sum ref) / sum ref).  Returns two float64 arrays."""
+    torch = _torch()
+    est = estimate.to(torch.float64)
+    ref = reference.to(torch.float64)
+    mean_rel = np.zeros(ref.shape[0])
+    integral = np.zeros(ref.shape[0])
+    for c in range(ref.shape[0]):
+        r = ref[c]
+        if float(r.max()) <= 0.0:
+            mean_rel[c] = integral[c] = np.nan
+            continue
+        sel = r >= threshold * r.max()
+        d = est[c][sel] - r[sel]
+        mean_rel[c] = (d / r[sel]).mean().item()
+        integral[c] = (d.sum() / r[sel].sum()).item()
+    return mean_rel, integral
+
+
+def error_report(estimate, reference, reference_sigma, thresholds=(0.5, 0.1, 0.01)) -> dict:
+    """Sigma-equivalent error and signed bias (mean over columns) at each
+    threshold of the column maximum: the beamlet core (0.5), the penumbra
+    (0.1) and the low-dose tail the truncation keeps (0.01)."""
+    out = {}
+    for t in thresholds:
+        err = sigma_equivalent_error(estimate, reference, reference_sigma, threshold=t)
+        mean_rel, integral = relative_bias(estimate, reference, threshold=t)
+        out[f"{t:g}"] = {"sigma_eq": float(np.nanmean(err)), "bias_mean": float(np.nanmean(mean_rel)),
+                         "bias_integral": float(np.nanmean(integral))}
     return out

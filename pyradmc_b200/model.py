@@ -730,8 +730,16 @@ class AnalyticWaterTables:
         return out
 
     def _pack(self, e_max: float, ecut: float, pcut: float) -> dict:
+        """The pack built for exactly `e_max`, else the smallest one whose
+        energy range covers it (a source whose top energy is data, such as a
+        phase space, rarely sits on a pack energy; wider tables interpolate the
+        same physics on a log grid that reaches a little further)."""
         e_primary = e_max / (1.0 + 1.0e-6)
         path = DATA / f"water_tables_{_energy_label(e_primary)}.npz"
+        if not path.exists():
+            above = [e for e in self.available_energies() if e * (1.0 + 1.0e-6) >= e_max]
+            if above:
+                path = DATA / f"water_tables_{_energy_label(min(above))}.npz"
         with self._lock:
             cached = self._cache.get(path)
             if cached is None:
@@ -745,7 +753,7 @@ class AnalyticWaterTables:
                     cached = {k: z[k] for k in z.files}
                 self._cache[path] = cached
         if not (
-            math.isclose(float(cached["e_max"]), e_max, rel_tol=0, abs_tol=1e-12)
+            float(cached["e_max"]) >= e_max - 1e-12
             and float(cached["ecut"]) == ecut
             and float(cached["pcut"]) == pcut
         ):

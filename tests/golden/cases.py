@@ -91,6 +91,7 @@ CASES: dict[str, dict] = {
         run=dict(n_histories=200_000, n_batches=10, seed=SEED),
         scoring=dict(kind="cylinder", r_max=6.0, n_shells=12, r_min=0.1),
         shards=10,
+        chi2_fraction=1e-3,  # a pencil kernel spans decades: compare down to 0.1 % of the maximum
     ),
     # Dose to water and dose to medium behind a cortical-bone layer (material 4
     # of pyRadMC's registry at 1.85 g/cc) in water: the stopping-power ratio

@@ -46,7 +46,8 @@ def test_dose_matches_reference_engine(gpu, name):
     run["n_histories"] *= mult
     result = engine.run(src, **run)
     ref = load_ref(name)
-    mask = stats.high_dose_mask(ref["dose"], ref["dose_sigma"], result.dose_sigma, minimum=50)
+    mask = stats.high_dose_mask(ref["dose"], ref["dose_sigma"], result.dose_sigma,
+                                fraction=CASES[name].get("chi2_fraction", 0.1), minimum=50)
     stats.assert_chi2_consistent_batched(ref["dose"], ref["dose_sigma"], int(ref["n_batches"]),
                                          result.dose, result.dose_sigma, result.n_batches, mask=mask,
                                          case=name)
