@@ -38,15 +38,29 @@ extern "C" {
 int pmd_conv3d(const void* x, const void* w, const float* bias, void* y, int n, int d, int h,
                int w_, int cin, int cout, int kpad, int relu, void* stream);
 
-/* Selects the convolution kernels of pmd_conv3d: 0 (default) the tensor-memory
- * kernel (tcgen05.mma, accumulators in TMEM; cout a multiple of 16 up to 192,
+/* Selects the convolution kernels of pmd_conv3d: 0 (default) the warp-specialized
+ * kernel below wherever it applies except cin = 8, then the single-buffered
+ * tensor-memory kernel (tcgen05.mma, accumulators in TMEM; cout a multiple of 16 up to 192,
  * cin 8 or a multiple of 16 up to 96) where its weights are staged in shared
  * memory in at most two passes, and the mma.sync kernel elsewhere; 1 the mma.sync kernel only; 2 the
  * tensor-memory kernel only; 3 its pipelined variant only (two halo buffers
  * and two accumulators, one CTA per SM; measured slower than the default on
- * this network's layers, kept for larger tiles).  Other shapes return -1.  impl < 0 only queries.  Returns the
+ * this network's layers, kept for larger tiles); 4 the warp-specialized kernel only (a TMA producer
+ * warp, one MMA-issuing thread and four epilogue warps over a ring of stage
+ * buffers; cout a multiple of 16 up to 256, cin 8 or any multiple of 16, weights
+ * resident or streamed with the stages).  Other shapes return -1.  impl < 0 only queries.  Returns the
  * previous setting.  Process-wide. */
 int pmd_conv3d_impl(int impl);
+
+/* The kernel pmd_conv3d would launch for this shape under the current
+ * selection (16-byte aligned operands), written to info[8]: info[0] = 4
+ * warp-specialized, 3 pipelined, 2 single-buffered tensor-memory, 1 mma.sync,
+ * -1 none; for the warp-specialized kernel info[1..7] = 8-channel chunks per
+ * stage, stages per tile, stage buffers, weights streamed (1) or resident (0),
+ * output slices per tile, blocks per SM, shared memory bytes per block (the
+ * single-buffered kernel fills info[5..7]).  Returns 0, or -1 for a NULL info or
+ * an invalid shape. */
+int pmd_conv3d_plan(int n, int d, int h, int w_, int cin, int cout, int* info);
 
 /* Number of tensor-memory convolution launches whose wait on the tensor cores
  * ran past its time limit since the last call (their outputs are not valid),

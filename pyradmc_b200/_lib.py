@@ -284,6 +284,7 @@ SIGNATURES.update({
     "pmd_conv3d": (_i, [_v, _v, _v, _v, _i, _i, _i, _i, _i, _i, _i, _i, _v]),
     "pmd_conv3d_wgrad": (_i, [_v, _v, _v, _v, _i, _i, _i, _i, _i, _i, _i, _v]),
     "pmd_conv3d_impl": (_i, [_i]),
+    "pmd_conv3d_plan": (_i, [_i, _i, _i, _i, _i, _i, _ip]),
     "pmd_conv3d_failures": (_i, []),
     "pmd_flip_weights": (_i, [_v, _v, _i, _i, _i, _i, _v]),
     "pmd_relu_mask": (_i, [_v, _v, _l, _v]),

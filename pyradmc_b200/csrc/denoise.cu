@@ -689,6 +689,7 @@ __global__ void csc_to_dense_f64_kernel(const int64_t* indptr, const int64_t* in
 }  // namespace pmd
 
 #include "denoise_umma.cuh"
+#include "denoise_ws.cuh"
 
 using namespace pmd;
 
@@ -725,9 +726,11 @@ int launched() { return cudaGetLastError() == cudaSuccess ? 0 : -2; }
 // The vectorized element-wise kernels index with 32-bit integers.
 bool fits32(long long elements) { return elements < (1LL << 31); }
 
-// Convolution path: 0 = the single-buffered tensor-memory kernel where its
-// weights are staged in at most two passes, else the mma.sync kernel; 1 = mma.sync only;
-// 2 = single-buffered tensor-memory kernel only; 3 = pipelined only.
+// Convolution path: 0 = the warp-specialized kernel (cin != 8), else the
+// single-buffered tensor-memory kernel where its weights are staged in at most
+// two passes, else the mma.sync kernel; 1 = mma.sync only;
+// 2 = single-buffered tensor-memory kernel only; 3 = pipelined only; 4 = warp-specialized
+// (TMA-fed) only.
 int g_conv_impl = 0;
 
 constexpr int kSmemPerSM = 233472;      // bytes of shared memory per SM
@@ -841,6 +844,186 @@ int dispatch_umma_pipe(const __nv_bfloat16* x, const __nv_bfloat16* w, const flo
     }
 }
 
+// ---- warp-specialized tensor-memory kernel ---------------------------------
+
+// Plan of conv3d_ws_kernel; false when the shape is outside it (cout a multiple
+// of 16 up to 256, cin 8 or a multiple of 16) or nothing fits shared memory.
+// Weights stay resident where all 27 taps fit beside at least two halo stages;
+// the halo of a tile is then split into even channel groups only as far as it
+// takes to hold two blocks (two MMA-issuing threads) per SM: one thread issues
+// an MMA every ~50 cycles at best, two keep an SM's tensor cores busier
+// (decoder level 0, 48 -> 16: 0.89 ms in three groups at two blocks per SM,
+// 1.22 ms whole at one).  Otherwise the
+// weights are streamed with the stages, in channel groups as large as three
+// stages allow (two where three never fit).
+bool ws_plan(const ConvShape& s, WsConv& p, int& smem, int& ctas_per_sm) {
+    if (s.cout % 16 || s.cout < 16 || s.cout > 256) return false;
+    if (!(s.cin == 8 || s.cin % 16 == 0)) return false;
+    const int cpt = s.cin / 8, N = s.cout;
+    p = WsConv{};
+    p.s = s;
+    p.tz = s.cin <= 16 && s.cout <= 16 ? 4 : (s.cin <= 48 ? 2 : 1);
+    while (p.tz > 1 && 2 * p.tz * N > 512) --p.tz;
+    if (2 * p.tz * N > 512) return false;
+    p.box_bytes = (unsigned)((p.tz + 2) * kUHY * kUHX * 16);
+    p.plane_bytes = (p.box_bytes + 127u) & ~127u;
+    auto round128 = [](unsigned v) { return (v + 127u) & ~127u; };
+    const int bars = 8 * (2 * kWsMaxStages + 4) + 16;  // mbarriers, TMEM address, flag
+    const int pair_smem = kSmemPerSM / 2 - kSmemReserved;
+    // resident weights: all channels in one stage if that fits, then smaller
+    // groups (three stages) until two blocks fit an SM
+    for (int cg = cpt; cg >= 1; --cg) {
+        // even groups only (cg = 1 pairs taps, one K step in 28 on a zero chunk,
+        // and measured slower than one block per SM with the whole halo)
+        if (cpt % cg || (cg % 2 && cg != cpt)) continue;
+        const unsigned chunks = 27u * cg + (cg == 1 ? 1u : 0u);  // per group (cg = 1: zero partner)
+        const unsigned stage = round128((unsigned)cg * p.plane_bytes + kUSlack);
+        const int n_st = cg == cpt ? 2 : 3;
+        const long long need = (long long)n_st * stage + (long long)(cpt / cg) * chunks * N * 16 + bars;
+        if (need > kSmemPerBlockMax) continue;
+        if (p.cg != 0 && need > pair_smem) continue;  // a smaller group only to reach two blocks per SM
+        p.cg = cg;
+        p.groups = cpt / cg;
+        p.stages = n_st;
+        p.streamed = 0;
+        p.halo_part = (unsigned)cg * p.plane_bytes + kUSlack;
+        p.stage_bytes = stage;
+        p.w_chunks = chunks;
+        p.tx_bytes = (unsigned)cg * p.box_bytes;
+        smem = (int)need;
+        if (need <= pair_smem) break;
+    }
+    if (p.cg == 0) {  // streamed weights: the largest channel group with 3 stages, else 2
+        for (int want = 3; want >= 2 && p.cg == 0; --want)
+            for (int cg = cpt; cg >= 1; --cg) {
+                if (cpt % cg || (cg > 1 && cg % 2)) continue;
+                const unsigned chunks = 27u * cg + (cg == 1 ? 1u : 0u);
+                const unsigned halo = (unsigned)cg * p.plane_bytes + kUSlack;
+                const unsigned stage = round128(halo + chunks * N * 16);
+                const int fixed = bars;
+                int n_st = (kSmemPerBlockMax - fixed) / (int)stage;
+                if (n_st > kWsMaxStages) n_st = kWsMaxStages;
+                if (n_st < want) continue;
+                p.cg = cg;
+                p.groups = cpt / cg;
+                p.stages = n_st;
+                p.streamed = 1;
+                p.halo_part = halo;
+                p.stage_bytes = stage;
+                p.w_chunks = chunks;
+                p.tx_bytes = (unsigned)cg * p.box_bytes + 27u * cg * N * 16;
+                smem = n_st * (int)stage + fixed;
+                break;
+            }
+        if (p.cg == 0) return false;
+    }
+    p.acc_cols = (unsigned)(p.tz * N);
+    unsigned cols = 32;
+    while (cols < 2 * p.acc_cols) cols <<= 1;
+    p.tmem_cols = cols;
+    p.ystride = N;
+    p.tiles_d = (s.d + p.tz - 1) / p.tz;
+    p.tiles_h = (s.h + kUTY - 1) / kUTY;
+    p.tiles_w = (s.w + kUTX - 1) / kUTX;
+    const long long tiles = (long long)s.n * p.tiles_d * p.tiles_h * p.tiles_w;
+    if (tiles > (1LL << 30)) return false;
+    p.n_tiles = (int)tiles;
+    // at most two blocks per SM, and never more than fit 512 tensor-memory
+    // columns (enforced through the shared-memory request)
+    int by_smem = kSmemPerSM / (smem + kSmemReserved);
+    const int by_tmem = 512 / (int)cols;
+    int per_sm = by_smem < by_tmem ? by_smem : by_tmem;
+    if (per_sm > 2) per_sm = 2;
+    if (per_sm < 1) return false;
+    if (by_smem > per_sm) {
+        smem = kSmemPerSM / per_sm - kSmemReserved;
+        if (smem > kSmemPerBlockMax) smem = kSmemPerBlockMax;
+    }
+    ctas_per_sm = per_sm;
+    return true;
+}
+
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
+                                   const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
+                                   const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                   CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+// The driver's tensor-map encoder, found once through the runtime (no link
+// against the driver library); null when the driver does not offer it.
+EncodeTiledFn encode_tiled() {
+    static const EncodeTiledFn fn = [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            return (EncodeTiledFn) nullptr;
+        return reinterpret_cast<EncodeTiledFn>(f);
+    }();
+    return fn;
+}
+
+// Tensor maps of one launch: the NDHWC bf16 activation (box 8 channels x 10 x
+// 18 x (tz + 2) x 1, zero fill outside) and the [cout][kpad] weights (box 8 x
+// cout).  False when the driver refuses them (the caller then takes another
+// kernel).
+bool ws_tensor_maps(const __nv_bfloat16* x, const __nv_bfloat16* w, const WsConv& p, CUtensorMap& xm,
+                    CUtensorMap& wm) {
+    const EncodeTiledFn enc = encode_tiled();
+    if (!enc) return false;
+    if (reinterpret_cast<uintptr_t>(x) % 16 || reinterpret_cast<uintptr_t>(w) % 16) return false;
+    const ConvShape& s = p.s;
+    const cuuint64_t e = sizeof(__nv_bfloat16);
+    const cuuint64_t xdim[5] = {(cuuint64_t)s.cin, (cuuint64_t)s.w, (cuuint64_t)s.h, (cuuint64_t)s.d,
+                                (cuuint64_t)s.n};
+    const cuuint64_t xstride[4] = {xdim[0] * e, xdim[0] * xdim[1] * e, xdim[0] * xdim[1] * xdim[2] * e,
+                                   xdim[0] * xdim[1] * xdim[2] * xdim[3] * e};
+    const cuuint32_t xbox[5] = {8, (cuuint32_t)kUHX, (cuuint32_t)kUHY, (cuuint32_t)(p.tz + 2), 1};
+    const cuuint32_t ones[5] = {1, 1, 1, 1, 1};
+    if (enc(&xm, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, const_cast<__nv_bfloat16*>(x), xdim, xstride, xbox,
+            ones, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+            CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+        return false;
+    const cuuint64_t wdim[2] = {(cuuint64_t)s.kpad, (cuuint64_t)s.cout};
+    const cuuint64_t wstride[1] = {(cuuint64_t)s.kpad * e};
+    const cuuint32_t wbox[2] = {8, (cuuint32_t)s.cout};
+    return enc(&wm, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<__nv_bfloat16*>(w), wdim, wstride, wbox,
+               ones, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+               CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+template <int CG>
+int launch_ws(const CUtensorMap& xm, const CUtensorMap& wm, const __nv_bfloat16* w, const float* bias,
+              __nv_bfloat16* y, const WsConv& p, int smem, int per_sm, int relu, cudaStream_t st) {
+    int dev = 0, sms = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+        cudaFuncSetAttribute(conv3d_ws_kernel<CG>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) !=
+            cudaSuccess)
+        return -2;
+    const int grid = p.n_tiles < sms * per_sm ? p.n_tiles : sms * per_sm;
+    conv3d_ws_kernel<CG><<<grid, kWsThreads, smem, st>>>(xm, wm, w, bias, y, p, relu);
+    return launched();
+}
+
+// 1 launched (code: 0, or -2 from launched()), -1 when the plan or the tensor
+// maps do not cover the call.
+int try_ws(const __nv_bfloat16* x, const __nv_bfloat16* w, const float* bias, __nv_bfloat16* y,
+           const ConvShape& s, int relu, cudaStream_t st, int& code) {
+    WsConv p{};
+    int smem = 0, per_sm = 0;
+    CUtensorMap xm, wm;
+    if (!ws_plan(s, p, smem, per_sm) || !ws_tensor_maps(x, w, p, xm, wm)) return -1;
+    switch (p.cg) {
+        case 1: code = launch_ws<1>(xm, wm, w, bias, y, p, smem, per_sm, relu, st); return 1;
+        case 2: code = launch_ws<2>(xm, wm, w, bias, y, p, smem, per_sm, relu, st); return 1;
+        case 4: code = launch_ws<4>(xm, wm, w, bias, y, p, smem, per_sm, relu, st); return 1;
+        case 6: code = launch_ws<6>(xm, wm, w, bias, y, p, smem, per_sm, relu, st); return 1;
+        case 8: code = launch_ws<8>(xm, wm, w, bias, y, p, smem, per_sm, relu, st); return 1;
+        case 12: code = launch_ws<12>(xm, wm, w, bias, y, p, smem, per_sm, relu, st); return 1;
+        default: return -1;
+    }
+}
+
 template <int CPT>
 int launch_umma(const __nv_bfloat16* x, const __nv_bfloat16* w, const float* bias, __nv_bfloat16* y,
                 const UmmaConv& u, int smem, int per_sm, int relu, cudaStream_t st) {
@@ -883,6 +1066,14 @@ int pmd_conv3d(const void* x, const void* w, const float* bias, void* y, int n, 
     auto W = (const __nv_bfloat16*)w;
     auto Y = (__nv_bfloat16*)y;
     cudaStream_t st = (cudaStream_t)stream;
+    if (g_conv_impl == 4 || (g_conv_impl == 0 && cin != 8)) {
+        // the warp-specialized tensor-memory kernel (by default everywhere but
+        // the 8-channel input layer, where the single-buffered kernel measured
+        // faster)
+        int code = 0;
+        if (try_ws(X, W, bias, Y, s, relu, st, code) == 1) return code;
+        if (g_conv_impl == 4) return -1;
+    }
     if (g_conv_impl == 3) {
         // the pipelined tensor-memory kernel (opt-in: measured slower than two
         // single-buffered CTAs per SM on the network's layers)
@@ -916,9 +1107,49 @@ int pmd_conv3d(const void* x, const void* w, const float* bias, void* y, int n, 
     return launched();
 }
 
+int pmd_conv3d_plan(int n, int d, int h, int wd, int cin, int cout, int* info) {
+    if (!info || n < 1 || d < 1 || h < 1 || wd < 1 || cin < 8 || cin % 8) return -1;
+    for (int i = 0; i < 8; ++i) info[i] = 0;
+    info[0] = -1;
+    ConvShape s{n, d, h, wd, cin, cout, (27 * cin + 63) / 64 * 64};
+    WsConv p{};
+    UmmaConv u{};
+    int smem = 0, per_sm = 0;
+    if ((g_conv_impl == 4 || (g_conv_impl == 0 && cin != 8)) && ws_plan(s, p, smem, per_sm)) {
+        info[0] = 4;
+        info[1] = p.cg;
+        info[2] = p.groups;
+        info[3] = p.stages;
+        info[4] = p.streamed;
+        info[5] = p.tz;
+        info[6] = per_sm;
+        info[7] = smem;
+        return 0;
+    }
+    if (g_conv_impl == 4) return 0;
+    if (g_conv_impl == 3) {
+        if (umma_pipe_plan(s, u, smem, per_sm)) info[0] = 3;
+        return 0;
+    }
+    if ((g_conv_impl == 0 || g_conv_impl == 2) && umma_plan(s, u, smem, per_sm) &&
+        (g_conv_impl == 2 || u.passes <= 2)) {
+        info[0] = 2;
+        info[5] = u.tz;
+        info[6] = per_sm;
+        info[7] = smem;
+        return 0;
+    }
+    if (g_conv_impl == 2) return 0;
+    switch (cout) {
+        case 8: case 16: case 32: case 48: case 64: case 96: case 128: case 192: info[0] = 1; break;
+        default: break;
+    }
+    return 0;
+}
+
 int pmd_conv3d_impl(int impl) {
     const int previous = g_conv_impl;
-    if (impl >= 0 && impl <= 3) g_conv_impl = impl;
+    if (impl >= 0 && impl <= 4) g_conv_impl = impl;
     return previous;
 }
 

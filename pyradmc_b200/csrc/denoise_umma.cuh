@@ -130,6 +130,57 @@ __device__ __forceinline__ uint32_t tap_offset(int t) {
     return (uint32_t)(((t / 9) * kUHY * kUHX + ((t / 3) % 3) * kUHX + t % 3) * 16);
 }
 
+// Tap t's first halo row relative to the slice's origin, in 16-byte units.
+__host__ __device__ constexpr uint32_t tap_off16(int t) {
+    return (uint32_t)((t / 9) * kUHY * kUHX + ((t / 3) % 3) * kUHX + t % 3);
+}
+
+// Issues the MMAs of all 27 taps over CG 8-channel chunks for the tz slices of
+// a tile: A from the halo planes at a_addr (plane_bytes apart), B from the
+// weight chunks [tap * CG + q][N][8] at b_addr, slice sl into accumulator
+// columns d0 + sl * N, in the order slice, tap, chunk pair.  Every descriptor is
+// the slice's base descriptor plus an offset fixed at compile time within a
+// group of 9 taps (7 tap pairs for CG = 1), so the issuing thread runs no loads
+// and little arithmetic between MMAs (a thread issuing from a descriptor table
+// in shared memory measured ~50-120 cycles per MMA, well above the tensor
+// cores' ~35 for M = 128, N <= 32).  The tap loop stays a loop of such groups
+// and the slice loop is not unrolled: with the 14 or 27 MMAs of a slice
+// unrolled in full for CG = 1 and 2, this build computed wrong sums (tested
+// against the oracle), while the grouped form is exact for every CG.  With CG = 1 a K step
+// pairs two taps: the second half's LBO is the distance between their rows and
+// the last tap pairs with a zero weight chunk.  accumulate: whether the first
+// K step adds to the accumulator (a later channel group of the same tile).
+template <int CG>
+__device__ __forceinline__ void umma_issue_taps(uint32_t d0, uint32_t a_addr, uint32_t plane_bytes,
+                                                uint32_t b_addr, int N, int tz, uint32_t idesc,
+                                                bool accumulate) {
+    constexpr uint64_t slice16 = (uint64_t)(kUHY * kUHX);
+    const uint64_t a0 = umma_smem_desc(a_addr, CG == 1 ? 0u : plane_bytes, kUHX * 16);
+    const uint64_t b0 = umma_smem_desc(b_addr, (uint32_t)N * 16, 128);
+    const uint64_t plane16 = plane_bytes >> 4;
+#pragma unroll 1
+    for (int sl = 0; sl < tz; ++sl) {
+        const uint32_t d = d0 + (uint32_t)(sl * N);
+        const uint64_t as = a0 + slice16 * (uint64_t)sl;
+        if constexpr (CG == 1) {
+#pragma unroll 7
+            for (int tap = 0; tap < 27; tap += 2) {
+                const uint64_t lbo16 = tap + 1 < 27 ? tap_off16(tap + 1) - tap_off16(tap) : 1u;
+                umma_bf16(d, as + tap_off16(tap) + (lbo16 << 16), b0 + (uint64_t)(tap * N), idesc,
+                          (accumulate || tap > 0) ? 1u : 0u);
+            }
+        } else {
+#pragma unroll 9
+            for (int tap = 0; tap < 27; ++tap)
+#pragma unroll
+                for (int q = 0; q < CG; q += 2)
+                    umma_bf16(d, as + tap_off16(tap) + plane16 * (uint64_t)q,
+                              b0 + (uint64_t)((tap * CG + q) * N), idesc,
+                              (accumulate || tap > 0 || q > 0) ? 1u : 0u);
+        }
+    }
+}
+
 // CPT = cin / 8, the 8-channel chunks (halo planes) per tap.
 template <int CPT>
 __global__ void __launch_bounds__(128, 4)
@@ -227,7 +278,11 @@ conv3d_umma_kernel(const __nv_bfloat16* __restrict__ x, const __nv_bfloat16* __r
             cp_async_wait<0>();
             fence_async_smem();
             __syncthreads();
-            if (tid == 0) {
+            if (tid == 0 && u.passes == 1) {
+                tc_fence_after();
+                umma_issue_taps<CPT>(tmem, halo_s, u.plane_bytes, w_s, N, u.tz, idesc, false);
+                umma_commit(mbar);
+            } else if (tid == 0) {
                 tc_fence_after();
                 const int n_k = k_end - k_begin;
                 // slice sl reads the halo kUHY * kUHX rows further: add to the start-address field
@@ -399,7 +454,6 @@ conv3d_umma_pipe_kernel(const __nv_bfloat16* __restrict__ x, const __nv_bfloat16
     extern __shared__ __align__(1024) unsigned char smem[];
     const ConvShape& s = u.s;
     const int N = s.cout;
-    constexpr int cpt = CPT;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const unsigned buf_stride = u.halo_bytes + kUSlack;  // halo + its zeroed slack
     unsigned char* halo0 = smem;
@@ -433,21 +487,9 @@ conv3d_umma_pipe_kernel(const __nv_bfloat16* __restrict__ x, const __nv_bfloat16
         const int n = i % N, jj = i / N;
         cp_async16(wbuf + ((size_t)jj * N + n) * 16, wt + (long long)n * s.kpad + (long long)jj * 8, true);
     }
-    const int n_k = (27 * cpt + 1) / 2;
-    for (int k = tid; k < n_k; k += blockDim.x) {
-        const int j = 2 * k;
-        const int tap = j / cpt, q = j % cpt;
-        const uint32_t a_addr = halo_s + (uint32_t)q * u.plane_bytes + tap_offset(tap);
-        uint32_t a_lbo = u.plane_bytes;
-        if (cpt == 1) a_lbo = tap + 1 < 27 ? tap_offset(tap + 1) - tap_offset(tap) : 16u;
-        dtab[2 * k] = umma_smem_desc(a_addr, a_lbo, kUHX * 16);
-        dtab[2 * k + 1] = umma_smem_desc(w_s + (uint32_t)j * N * 16, N * 16, 128);
-    }
     if ((int)blockIdx.x < u.n_tiles) umma_load_halo<CPT>(x, u, blockIdx.x, halo0, tid);
     cp_async_commit();
 
-    constexpr uint64_t slice_inc = (uint64_t)(kUHY * kUHX * 16) >> 4;
-    const uint64_t buf_inc = (uint64_t)(buf_stride >> 4);
     uint32_t phase = 0;
     int failed = 0, i = 0, prev = -1;
     for (int tile = blockIdx.x; tile < u.n_tiles; tile += gridDim.x, ++i) {
@@ -459,12 +501,8 @@ conv3d_umma_pipe_kernel(const __nv_bfloat16* __restrict__ x, const __nv_bfloat16
         __syncthreads();
         if (tid == 0) {
             tc_fence_after();
-            for (int sl = 0; sl < u.tz; ++sl) {
-                const uint32_t d_tmem = tmem + (uint32_t)b * acc_cols + (uint32_t)(sl * N);
-                const uint64_t a_inc = buf_inc * (uint64_t)b + slice_inc * (uint64_t)sl;
-                for (int k = 0; k < n_k; ++k)
-                    umma_bf16(d_tmem, dtab[2 * k] + a_inc, dtab[2 * k + 1], idesc, k > 0 ? 1u : 0u);
-            }
+            umma_issue_taps<CPT>(tmem + (uint32_t)b * acc_cols, halo_s + (uint32_t)b * buf_stride,
+                                 u.plane_bytes, w_s, N, u.tz, idesc, false);
             umma_commit(mbar);
         }
         // the next tile's halo into the other buffer (its last reader, the MMAs

@@ -90,3 +90,33 @@ def test_network_refuses_to_run_without_a_cuda_device():
 
     with pytest.raises(RuntimeError, match="CUDA device only"):
         UNet3D("cuda:0")
+
+
+def test_convolution_plans_of_the_network_layers():
+    """pmd_conv3d_plan is host arithmetic: the default path's kernel and plan
+    for every layer of a 16-window inference chunk (64 x 64 x 128 windows)."""
+    import ctypes
+
+    lib = _lib.load()
+    level = {"enc0": 0, "enc1": 1, "enc2": 2, "mid_": 3, "dec2": 2, "dec1": 1, "dec0": 0}
+    previous = lib.pmd_conv3d_impl(0)
+    plans = {}
+    try:
+        for l in layout()[0]:
+            f = 2 ** level[l.name[:4]]
+            info = (ctypes.c_int * 8)()
+            assert lib.pmd_conv3d_plan(16, 64 // f, 64 // f, 128 // f, l.cin, l.cout, info) == 0
+            plans[l.name] = list(info)
+        assert lib.pmd_conv3d_plan(1, 1, 1, 1, 12, 16, (ctypes.c_int * 8)()) == -1  # cin % 8
+        assert lib.pmd_conv3d_plan(1, 1, 1, 1, 16, 16, None) == -1
+    finally:
+        lib.pmd_conv3d_impl(previous)
+    assert plans.pop("enc0a")[0] == 2  # the 8-channel input layer: single-buffered kernel
+    for name, (kernel, cg, groups, stages, streamed, tz, per_sm, smem) in plans.items():
+        assert kernel == 4, name  # every other layer: warp-specialized
+        assert 2 <= stages <= 4 and cg * groups * 8 == dict((l.name, l.cin) for l in layout()[0])[name]
+        assert smem <= 232448 and per_sm in (1, 2) and tz in (1, 2, 4), name
+        assert per_sm == 1 or 2 * (smem + 1024) <= 233472, name
+    assert plans["dec0a"][1:7] == [2, 3, 3, 0, 2, 2]  # three resident groups, two blocks per SM
+    assert plans["dec1a"][4] == 0  # 166 KB of weights stay resident
+    assert all(plans[n][4] == 1 for n in ("enc2b", "mid_a", "mid_b", "dec2a", "dec2b"))

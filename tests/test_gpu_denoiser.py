@@ -254,13 +254,41 @@ UMMA_SHAPES = [
     (1, 2, 16, 16, 64, 64),
     (1, 2, 8, 8, 64, 192),
     (1, 2, 8, 8, 64, 128),
+    # beyond the single-buffered kernel: weights streamed in channel groups
+    (1, 2, 16, 16, 192, 64),
+    (2, 3, 8, 8, 128, 128),
 ]
+
+SMEM_MAX = 232448
+
+
+def _umma_single_pass(cin, cout):
+    """Whether the single-buffered tensor-memory kernel stages every weight at
+    once (its plan's shared-memory arithmetic)."""
+    if cin > 96:
+        return False
+    cpt = cin // 8
+    tz = 4 if cin <= 16 and cout <= 16 else (2 if cin <= 48 else 1)
+    chunks = 27 * cpt + (1 if cpt == 1 else 0)
+    return (tz + 2) * 180 * 16 * cpt + 256 + 16 + chunks * (cout * 16 + 8) <= SMEM_MAX
+
+
+def _plan(lib, shape, impl):
+    import ctypes
+
+    info = (ctypes.c_int * 8)()
+    previous = lib.pmd_conv3d_impl(impl)
+    try:
+        assert lib.pmd_conv3d_plan(*shape, info) == 0
+    finally:
+        lib.pmd_conv3d_impl(previous)
+    return list(info)
 
 
 @pytest.mark.parametrize("shape", UMMA_SHAPES)
 def test_tensor_memory_convolution_matches_oracle(gpu, shape):
-    """The tcgen05/TMEM kernel (forced) against the oracle, and against the
-    mma.sync kernel on the same operands."""
+    """The tcgen05/TMEM kernels (each forced) against the oracle, and against
+    the mma.sync kernel on the same operands."""
     import torch
 
     n, d, h, w, cin, cout = shape
@@ -274,13 +302,16 @@ def test_tensor_memory_convolution_matches_oracle(gpu, shape):
     outs = {}
     previous = lib.pmd_conv3d_impl(-1)
     try:
-        for impl in (3, 2, 1):  # pipelined and single-buffered tensor memory, mma.sync
+        # warp-specialized, pipelined and single-buffered tensor memory, mma.sync
+        for impl in (4, 3, 2, 1):
             lib.pmd_conv3d_impl(impl)
             y = torch.full((n, d, h, w, cout), float("nan"), dtype=torch.bfloat16, device=gpu)
             code = lib.pmd_conv3d(dx.data_ptr(), dw.data_ptr(), db.data_ptr(), y.data_ptr(), n, d, h,
                                   w, cin, cout, kpad, 1, None)
             if impl == 3 and code == -1:
                 continue  # weights in several passes: no pipelined plan
+            if impl == 2 and code == -1 and cin > 96:
+                continue  # outside the single-buffered kernel
             assert code == 0, impl
             torch.cuda.synchronize()
             outs[impl] = y.float().cpu().numpy()
@@ -291,10 +322,16 @@ def test_tensor_memory_convolution_matches_oracle(gpu, shape):
         assert np.isfinite(got).all(), impl
         np.testing.assert_allclose(got, ref, rtol=BF16_REL, atol=1e-5 * np.abs(ref).max(),
                                    err_msg=f"impl {impl}")
-    # both accumulate the same products in fp32: at most a bf16 rounding step apart
-    np.testing.assert_allclose(outs[2], outs[1], rtol=2 * BF16_REL, atol=1e-5 * np.abs(ref).max())
+    # all accumulate the same products in fp32: at most a bf16 rounding step apart
+    np.testing.assert_allclose(outs[4], outs[1], rtol=2 * BF16_REL, atol=1e-5 * np.abs(ref).max())
+    if 2 in outs:
+        np.testing.assert_allclose(outs[2], outs[1], rtol=2 * BF16_REL, atol=1e-5 * np.abs(ref).max())
     if 3 in outs:  # the same MMAs in the same order: identical
         np.testing.assert_array_equal(outs[3], outs[2])
+    ws = _plan(lib, shape, 4)
+    if ws[2] == 1 and ws[4] == 0 and 2 in outs and _umma_single_pass(cin, cout):
+        # one channel group, resident weights: the same MMAs in the same order
+        np.testing.assert_array_equal(outs[4], outs[2])
 
 
 def test_tensor_memory_path_rejects_what_it_does_not_cover(gpu):
