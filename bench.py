@@ -366,7 +366,7 @@ def denoiser_leg(args, engine, source, counts, stream, device, plain_s_per_dij):
     D.run_dij_denoised(engine, net, source, c, N_BATCHES, SEED, truncation=1e-3, to_host=False,
                        timings=stages)
 
-    # the dominant convolution (decoder level 0, 48 -> 16 channels, tensor memory)
+    # the dominant convolution (decoder level 0, 48 -> 16 channels, default path)
     lib = _lib.load()
     b, (wx, wy, wz) = 16, window
     x = torch.randn((b, wx, wy, wz, 48), device=device).to(torch.bfloat16)
@@ -405,10 +405,13 @@ def denoiser_leg(args, engine, source, counts, stream, device, plain_s_per_dij):
         "window": list(window),
         "stage_ms": stages,
         "unet_forward_flops_per_dij": forward_flops_per_voxel() * unet_vox,
-        "roofline": {"bound": "tensor", "kernel": "conv3d_umma_kernel (decoder level 0, 48->16)",
+        "roofline": {"bound": "tensor", "kernel": "conv3d_ws_kernel (decoder level 0, 48->16)",
                      "achieved": conv_tflops, "peak": bf16_peak, "unit": "TFLOP/s",
                      "frac": conv_tflops / bf16_peak,
-                     "peak_source": "measured" if "bf16_tflops" in peaks else "fallback"},
+                     "peak_source": "measured" if "bf16_tflops" in peaks else "fallback",
+                     "shape_cap": "M 128 x N 16 x K 16 MMAs read 4.5 KB of shared memory per "
+                                  "65,536 FLOP: ~0.25 of the bf16 peak at most",
+                     "source": "profiles/conv3d_ws_dec0a_ncu.md"},
     }
 
 
