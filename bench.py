@@ -13,9 +13,12 @@ prints one JSON line.  ``value`` is histories/s over the device-resident step
 (``run_dij_device``: transport to CSC, the CSC left in HBM; CUDA events on the
 stream the engine runs on, max over ranks); ``e2e`` is the
 same metric through ``B200Engine.run_dij`` from host data, with the grid, table
-and GS uploads and the CSC readback inside the timed region.  Under torchrun each
-rank computes its own Dij (weak scaling, no data-path collective); the books and
-timings meet in one all-reduce after the timed region.
+and GS uploads and the CSC readback inside the timed region.  Under torchrun the
+N ranks compute one Dij of N x 100 columns (the benchmark fan N times over, each
+copy with its own history keys), each rank its history-balanced share of the
+columns (``column_shards`` / ``run_dij_shard``): weak scaling through the
+product's own sharding, no data-path collective; the books and timings meet in
+all-reduces outside the timed region.
 
 ``--impl reference`` times the CPU oracle (the C restatement of the reference's
 transport, all host threads) on bounded samples of the same workload.
@@ -183,10 +186,10 @@ def all_sum(world, values):
     return _reduce(world, values, "SUM")
 
 
-def weak_scaling_value(world: int, histories_per_rank: int, steps: int, max_total_ms: float) -> float:
-    """Whole-job histories/s: every rank ran `steps` Dijs of its own; the job
-    takes as long as its slowest rank."""
-    return world * histories_per_rank * steps / (max_total_ms / 1e3)
+def job_value(histories_all_ranks: int, steps: int, max_total_ms: float) -> float:
+    """Whole-job histories/s: the histories every rank ran per step, summed
+    over ranks, over `steps` steps that take as long as the slowest rank."""
+    return histories_all_ranks * steps / (max_total_ms / 1e3)
 
 
 # ---- the CPU baseline -----------------------------------------------------------------
@@ -272,6 +275,8 @@ def algorithmic_bytes(c: dict) -> float:
 
 
 DENOISER_WEIGHTS = ROOT / "pyradmc_b200" / "data" / "denoiser_unet.npz"
+# the network trained on coplanar gantry beams (oblique beamlets, 3 mm voxels)
+PLAN_DENOISER_WEIGHTS = ROOT / "pyradmc_b200" / "data" / "denoiser_unet_coplanar.npz"
 REF_HISTORIES = 8_000_000     # per beamlet: the high-statistics judge of the denoiser's error
 LADDER = (1 / 4, 1 / 3, 0.4, 1 / 2, 2 / 3, 1.0, 1.5, 2.0, 3.0, 4.0, 6.0, 8.0)  # scales tried
 
@@ -316,7 +321,8 @@ def denoiser_leg(args, engine, source, counts, stream, device, plain_s_per_dij):
         c = np.maximum(N_BATCHES, np.round(counts * g / N_BATCHES).astype(np.int64) * N_BATCHES)
         view = engine.run_dij_device(source, c, N_BATCHES, SEED + 31, truncation=0.0)
         dose, colmax, sg = D.dense_columns(view, device, with_sigma=True)
-        den = D.denoise_dense(net, dose, colmax, rho, shape, sigma=sg, window=window)
+        den = D.denoise_dense(net, dose, colmax, rho, shape, sigma=sg, window=window,
+                              directions=D.beam_directions(source), spacing=engine.grid.spacing)
         rung = {"scale": g, "histories": int(c.sum()),
                 "denoised": D.error_report(den, ref_dose, ref_sigma),
                 "plain": D.error_report(dose, ref_dose, ref_sigma)}
@@ -489,10 +495,15 @@ def plan_leg(args, device, stream):
     c = engine.last_counters()
     nnz = int(view.nnz)
     reached = held_error(n_2pct)
+    den = None
+    if not args.no_denoiser:
+        den = plan_denoiser(engine, plan, held_source, ref_dose, ref_sigma, n_2pct, seconds, device,
+                            stream)
     del ref_dose, ref_sigma
     torch.cuda.empty_cache()
     return {
         "workload": "plan_256x256x128_3mm_7beams_2800beamlets_6MV",
+        "denoiser": den,
         "beams_deg": [round(a, 2) for a in angles],
         "columns": int(plan.n_beamlets),
         "held_out_columns": int(len(held)),
@@ -505,6 +516,67 @@ def plan_leg(args, device, stream):
                   "transport_ms": c["transport_ms"], "reduce_ms": c["reduce_ms"],
                   "measured": "timed at the 2 % count (not extrapolated)"},
     }
+
+
+PLAN_WINDOW = (64, 64, 64)  # lateral x lateral x depth chunk of the plan's denoising windows
+PLAN_GROUP = 100            # columns whose dense maps are on the device at once
+
+
+def plan_denoiser(engine, plan, held_source, ref_dose, ref_sigma, n_plain, plain_seconds, device,
+                  stream):
+    """MC + denoiser on the plan.  Untimed: the held-out columns at 1/32 ..
+    1/2 of the plain 2 % count, denoised along their beamlets (windows of
+    PLAN_WINDOW oriented by each beam's direction), until the held-out error
+    reaches 2 %.  Timed (CUDA events): ``run_dij_denoised`` of the whole plan
+    at that count, PLAN_GROUP columns at a time, CSC left in HBM."""
+    import torch
+
+    from pyradmc_b200 import denoise_dij as D
+    from pyradmc_b200.denoiser import UNet3D
+
+    weights = PLAN_DENOISER_WEIGHTS if PLAN_DENOISER_WEIGHTS.exists() else DENOISER_WEIGHTS
+    net = UNet3D.load(weights, device=device)
+    shape = tuple(engine.grid.shape)
+    dirs = D.beam_directions(held_source)
+    rho = torch.from_numpy(np.ascontiguousarray(engine.grid.density, dtype=np.float32).ravel()).to(device)
+    ladder, chosen = [], None
+    for frac in (1 / 32, 1 / 16, 1 / 8, 1 / 4, 1 / 2):
+        n = max(N_BATCHES, int(round(n_plain * frac / N_BATCHES)) * N_BATCHES)
+        view = engine.run_dij_device(held_source, n, N_BATCHES, SEED, truncation=0.0)
+        dose, colmax, sg = D.dense_columns(view, device, with_sigma=True)
+        den = D.denoise_dense(net, dose, colmax, rho, shape, sigma=sg, window=PLAN_WINDOW,
+                              directions=dirs, spacing=engine.grid.spacing)
+        row = {"histories_per_beamlet": n, "fraction_of_plain": frac,
+               "denoised": D.error_report(den, ref_dose, ref_sigma),
+               "plain_same_histories": D.error_report(dose, ref_dose, ref_sigma)}
+        ladder.append(row)
+        del dose, sg, den
+        if row["denoised"]["0.5"]["sigma_eq"] <= 0.02:
+            chosen = n
+            break
+    torch.cuda.empty_cache()
+    out = {"weights": str(weights.relative_to(ROOT)), "window": list(PLAN_WINDOW),
+           "group_columns": PLAN_GROUP, "ladder": ladder,
+           "threshold": "metric: held-out voxels >= 50 % of the column maximum"}
+    if chosen is None:
+        out["reached_2pct"] = False
+        return out
+    stages: dict = {}
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    dij = D.run_dij_denoised(engine, net, plan, chosen, N_BATCHES, SEED, truncation=1e-3,
+                             lateral=PLAN_WINDOW[0], depth=PLAN_WINDOW[2], to_host=False,
+                             group_columns=PLAN_GROUP, timings=stages)
+    e1.record(stream)
+    e1.synchronize()
+    seconds = e0.elapsed_time(e1) / 1e3
+    out.update({"reached_2pct": True, "histories_per_beamlet": chosen,
+                "histories": int(chosen * plan.n_beamlets), "s_per_plan": seconds,
+                "speedup_vs_plain": plain_seconds / seconds, "nnz": int(dij.indptr[-1]),
+                "stage_ms": stages})
+    del dij
+    torch.cuda.empty_cache()
+    return out
 
 
 def conv_arm(args, local):
@@ -625,6 +697,18 @@ def b200_arm(args, world, rank, local):
     device = f"cuda:{local}"
     torch.cuda.set_device(local)
     grid, xs, source, counts = workload(rank)
+    # N > 1: one Dij of N x 100 columns (the benchmark fan N times over, every
+    # copy with its own history keys), each rank its share of the columns
+    # (engine.column_shards, history-balanced): weak scaling through the
+    # product's own sharding, no collective on the data path
+    whole, whole_counts, span = source, counts, None
+    if world > 1:
+        from pyradmc_b200.engine import column_shards
+        from pyradmc_b200.model import ConcatenatedBeamletSource
+
+        whole = ConcatenatedBeamletSource([source] * world)
+        whole_counts = np.tile(counts, world)
+        span = column_shards(whole_counts, world)[rank]
     engine = B200Engine(grid, xs, device=device, use_graph=not args.no_graph)
     tune_report = None
     if not args.no_autotune:
@@ -637,12 +721,15 @@ def b200_arm(args, world, rank, local):
     stream = torch.cuda.Stream(device=device)  # an explicit stream: the legacy default is 0
     torch.cuda.set_stream(stream)
     engine.use_stream(stream.cuda_stream)
-    kw = dict(n_histories_per_beamlet=counts, n_batches=N_BATCHES, seed=SEED + rank)
-    histories = int(np.sum(counts))
+    kw = dict(n_histories_per_beamlet=whole_counts, n_batches=N_BATCHES, seed=SEED)
+    if span is not None:
+        kw["columns"] = span
+    histories = int(np.sum(whole_counts[span[0]:span[1]])) if span is not None else int(np.sum(counts))
+    histories_all = int(all_sum(world, [histories])[0])
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=device)  # > 126 MB L2
 
     for _ in range(args.warmup):
-        view = engine.run_dij_device(source, truncation=1e-3, **kw)
+        view = engine.run_dij_device(whole, truncation=1e-3, **kw)
     peaks_path = ROOT / "MEASURED_PEAKS.json"
     peaks = json.loads(peaks_path.read_text()) if peaks_path.exists() else {}
     hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
@@ -657,7 +744,7 @@ def b200_arm(args, world, rank, local):
             start = torch.cuda.Event(enable_timing=True)
             end = torch.cuda.Event(enable_timing=True)
             start.record(stream)
-            view = engine.run_dij_device(source, truncation=1e-3, **kw)  # CSC stays in HBM
+            view = engine.run_dij_device(whole, truncation=1e-3, **kw)  # CSC stays in HBM
             end.record(stream)
             end.synchronize()
             step_ms.append(start.elapsed_time(end))
@@ -665,17 +752,23 @@ def b200_arm(args, world, rank, local):
         torch.cuda.synchronize()
         barrier(world)
     total_ms = all_max(world, [sum(step_ms)])[0]
-    value = weak_scaling_value(world, histories, args.steps, total_ms)
+    value = job_value(histories_all, args.steps, total_ms)
 
     # end to end from host data: uploads and readback inside the timed region.
     # Warm-up first: each result holds its CSC in page-locked host blocks that
     # the caching allocator recycles once the result is dropped; the loop keeps
     # one result alive while the next runs, so two sets get pinned (a first
     # pinning of ~200 MB costs ~0.1 s) before timing starts.
+    def e2e_call():
+        if span is None:
+            return engine.run_dij(whole, **kw)
+        e2e_kw = {k: v for k, v in kw.items() if k != "columns"}
+        return engine.run_dij_shard(whole, rank=rank, world=world, **e2e_kw)[0]
+
     dij = None
     for _ in range(max(args.warmup, 2)):
         engine.drop_uploads()
-        dij = engine.run_dij(source, **kw)
+        dij = e2e_call()
     e2e_ms, h2d, d2h = [], [], []
     barrier(world)
     torch.cuda.synchronize()
@@ -683,7 +776,7 @@ def b200_arm(args, world, rank, local):
         engine.drop_uploads()
         before = engine.last_counters()
         t0 = time.perf_counter()
-        dij = engine.run_dij(source, **kw)
+        dij = e2e_call()
         dense_ok = dij.indptr[-1] == dij.indices.size
         e2e_ms.append(1e3 * (time.perf_counter() - t0))
         after = engine.last_counters()
@@ -693,13 +786,14 @@ def b200_arm(args, world, rank, local):
     torch.cuda.synchronize()
     barrier(world)
     e2e_total = all_max(world, [sum(e2e_ms)])[0]
-    e2e_value = weak_scaling_value(world, histories, args.steps, e2e_total)
+    e2e_value = job_value(histories_all, args.steps, e2e_total)
 
     c = counters[-1]
-    den = None if args.no_denoiser else denoiser_leg(args, engine, source, counts, stream, device,
-                                                     total_ms / args.steps / 1e3)
+    # the method comparisons are one-GPU workloads: rank 0 of a one-rank run
+    den = None if args.no_denoiser or world > 1 else denoiser_leg(
+        args, engine, source, counts, stream, device, total_ms / args.steps / 1e3)
     plan = None
-    if not args.no_plan:
+    if not args.no_plan and world == 1:
         engine.drop_uploads()
         torch.cuda.empty_cache()
         plan = plan_leg(args, device, stream)

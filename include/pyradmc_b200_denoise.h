@@ -151,6 +151,26 @@ int pmd_scatter_windows(const float* win, const float* scale, int nx, int ny, in
                         const int32_t* origins, int n_windows, int wx, int wy, int wz, double* dst,
                         int64_t dst_stride, void* stream);
 
+/* Oriented windows (beamlets along any direction).  Window w is
+ * win[7w .. 7w+6] = (ox, oy, oz, orient, col, shear1, shear2), int32: orient =
+ * 2 * d + f names the depth axis d (0 x, 1 y, 2 z), read from its high end
+ * when f = 1; the two other axes, in increasing order, are the window's first
+ * two dimensions, shifted by s1(k) = round(k * shear1 / 65536) and s2(k)
+ * voxels at window depth k (an oblique beamlet stays centred).  Window voxel
+ * (a, b, k) of the wa*wb*wd window is voxel g of volume col with g[first] =
+ * o[first] + a + s1(k), g[second] = o[second] + b + s2(k), g[d] = o[d] + k
+ * (f = 0) or o[d] + wd - 1 - k (f = 1).  Gather: out[w][a][b][k] (zero outside
+ * the grid).  Scatter: dst[col * dst_stride + g] = max(data, 0) * scale[w]
+ * (float64; scale NULL or zero: 1) for window voxels inside the grid; windows
+ * of one column must not overlap.  orient = 4, col = w and no shear is the
+ * window of pmd_gather_windows / pmd_scatter_windows. */
+int pmd_gather_windows_oriented(const float* src, int64_t src_stride, int nx, int ny, int nz,
+                                const int32_t* win, int n_windows, int wa, int wb, int wd, float* out,
+                                void* stream);
+int pmd_scatter_windows_oriented(const float* data, const float* scale, int nx, int ny, int nz,
+                                 const int32_t* win, int n_windows, int wa, int wb, int wd, double* dst,
+                                 int64_t dst_stride, void* stream);
+
 /* Back to dose units: mean[m] = max(out[m], 0) * colmax[m / vox] (float64). */
 int pmd_unscale(const float* out, const float* colmax, int64_t vox, double* mean, int64_t m,
                 void* stream);

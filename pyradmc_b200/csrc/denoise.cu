@@ -676,6 +676,74 @@ __global__ void scatter_windows_kernel(const float* win, const float* scale, int
     }
 }
 
+// Oriented windows.  Window w is win[7w..7w+6] = (ox, oy, oz, orient, col,
+// shear1, shear2): orient = 2 * d + f names the depth axis d (0 x, 1 y, 2 z),
+// read from its high end when f = 1; the two other axes, in increasing order,
+// are the window's first two dimensions; shear1/2 move them by
+// round(k * shear / 65536) voxels at window depth k, so that a window can
+// follow an oblique beamlet.  Window voxel (a, b, k) is grid voxel g with
+// g[first] = o[first] + a + s1(k), g[second] = o[second] + b + s2(k) and
+// g[d] = o[d] + k (f = 0) or o[d] + wd - 1 - k (f = 1), of volume col.  For a
+// fixed k the shift is the same for every (a, b), so the map is one to one.
+constexpr int kWinInts = 7;
+
+__device__ __forceinline__ bool oriented_voxel(const int* wdesc, int a, int b, int k, int wd, int nx,
+                                               int ny, int nz, long long& flat) {
+    const int d = wdesc[3] >> 1, f = wdesc[3] & 1;
+    const int l1 = d == 0 ? 1 : 0, l2 = d == 2 ? 1 : 2;
+    const int s1 = (int)(((long long)k * wdesc[5] + 32768) >> 16);
+    const int s2 = (int)(((long long)k * wdesc[6] + 32768) >> 16);
+    int g[3];
+    g[l1] = wdesc[l1] + a + s1;
+    g[l2] = wdesc[l2] + b + s2;
+    g[d] = wdesc[d] + (f ? wd - 1 - k : k);
+    if ((unsigned)g[0] >= (unsigned)nx || (unsigned)g[1] >= (unsigned)ny || (unsigned)g[2] >= (unsigned)nz)
+        return false;
+    flat = ((long long)g[0] * ny + g[1]) * nz + g[2];
+    return true;
+}
+
+__global__ void gather_oriented_kernel(const float* src, long long src_stride, int nx, int ny, int nz,
+                                       const int* win, int wa, int wb, int wd, float* out,
+                                       long long total) {
+    const long long per = (long long)wa * wb * wd;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += stride) {
+        const int w = (int)(i / per);
+        long long r = i - (long long)w * per;
+        const int k = (int)(r % wd); r /= wd;
+        const int b = (int)(r % wb);
+        const int a = (int)(r / wb);
+        const int* wdesc = win + kWinInts * w;
+        long long flat;
+        float v = 0.0f;
+        if (oriented_voxel(wdesc, a, b, k, wd, nx, ny, nz, flat))
+            v = src[(long long)wdesc[4] * src_stride + flat];
+        out[i] = v;
+    }
+}
+
+__global__ void scatter_oriented_kernel(const float* data, const float* scale, int nx, int ny, int nz,
+                                        const int* win, int wa, int wb, int wd, double* dst,
+                                        long long dst_stride, long long total) {
+    const long long per = (long long)wa * wb * wd;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += stride) {
+        const int w = (int)(i / per);
+        long long r = i - (long long)w * per;
+        const int k = (int)(r % wd); r /= wd;
+        const int b = (int)(r % wb);
+        const int a = (int)(r / wb);
+        const int* wdesc = win + kWinInts * w;
+        long long flat;
+        if (oriented_voxel(wdesc, a, b, k, wd, nx, ny, nz, flat)) {
+            const float sc = scale ? scale[w] : 1.0f;
+            dst[(long long)wdesc[4] * dst_stride + flat] =
+                (double)fmaxf(data[i], 0.0f) * (double)(sc > 0.0f ? sc : 1.0f);
+        }
+    }
+}
+
 // CSC -> dense float64 columns (the caller zeroes dense).
 __global__ void csc_to_dense_f64_kernel(const int64_t* indptr, const int64_t* indices,
                                         const double* values, long long vox, double* dense) {
@@ -1330,6 +1398,30 @@ int pmd_scatter_windows(const float* win, const float* scale, int nx, int ny, in
     if (total == 0) return 0;
     scatter_windows_kernel<<<grid_for(total), 256, 0, (cudaStream_t)stream>>>(
         win, scale, nx, ny, nz, origins, wx, wy, wz, dst, dst_stride, total);
+    return launched();
+}
+
+int pmd_gather_windows_oriented(const float* src, int64_t src_stride, int nx, int ny, int nz,
+                                const int32_t* win, int n_windows, int wa, int wb, int wd, float* out,
+                                void* stream) {
+    if (nx < 1 || ny < 1 || nz < 1 || wa < 1 || wb < 1 || wd < 1 || n_windows < 0 || src_stride < 0)
+        return -1;
+    const long long total = (long long)n_windows * wa * wb * wd;
+    if (total == 0) return 0;
+    gather_oriented_kernel<<<grid_for(total), 256, 0, (cudaStream_t)stream>>>(
+        src, src_stride, nx, ny, nz, win, wa, wb, wd, out, total);
+    return launched();
+}
+
+int pmd_scatter_windows_oriented(const float* data, const float* scale, int nx, int ny, int nz,
+                                 const int32_t* win, int n_windows, int wa, int wb, int wd, double* dst,
+                                 int64_t dst_stride, void* stream) {
+    if (nx < 1 || ny < 1 || nz < 1 || wa < 1 || wb < 1 || wd < 1 || n_windows < 0 || dst_stride < 0)
+        return -1;
+    const long long total = (long long)n_windows * wa * wb * wd;
+    if (total == 0) return 0;
+    scatter_oriented_kernel<<<grid_for(total), 256, 0, (cudaStream_t)stream>>>(
+        data, scale, nx, ny, nz, win, wa, wb, wd, dst, dst_stride, total);
     return launched();
 }
 

@@ -6,9 +6,13 @@ No counterpart in pyRadMC.  Every step runs on the device through the C-ABI of
 final truncation + CSC); torch allocates the buffers and supplies the stream.
 
 Columns are dense volumes in the Dij's voxel order (x-major, z fastest).  Each
-column is denoised in a lateral window centred on the column's dose centroid
-over the full depth (the beamlets travel along +z); voxels outside the window
-keep their Monte Carlo values.
+column is denoised in windows that follow its beamlet: the grid axis closest
+to the beamlet's direction is the window's depth axis (read from the far end
+when the beam travels towards lower indices, so that every window sees the
+beam enter at its first depth plane), the lateral axes shift with depth along
+the beamlet (whole voxels, no resampling), the depth is cut into chunks, and
+each chunk's window is centred on the column's dose within the chunk.  Voxels
+outside every window keep their Monte Carlo values.
 """
 
 from __future__ import annotations
@@ -74,29 +78,6 @@ def dense_columns_f64(view, device):
     return mean, sigma
 
 
-def lateral_origins(dose, grid_shape, window: tuple[int, int, int], z0=None):
-    """int32 [C, 3] window origins: laterally centred on each column's dose
-    centroid (clamped into the grid), at depth z0 (0 when None; an array gives
-    one depth per column)."""
-    torch = _torch()
-    nx, ny, nz = grid_shape
-    wx, wy, _ = window
-    vol = dose.view(-1, nx, ny, nz)
-    lateral = vol.sum(dim=3)                                   # [C, nx, ny]
-    total = lateral.sum(dim=(1, 2)).clamp_min(1e-30)
-    xs = torch.arange(nx, device=dose.device, dtype=torch.float32)
-    ys = torch.arange(ny, device=dose.device, dtype=torch.float32)
-    cx = (lateral.sum(dim=2) * xs).sum(dim=1) / total
-    cy = (lateral.sum(dim=1) * ys).sum(dim=1) / total
-    ox = torch.clamp(torch.round(cx - wx / 2), 0, max(nx - wx, 0)).to(torch.int32)
-    oy = torch.clamp(torch.round(cy - wy / 2), 0, max(ny - wy, 0)).to(torch.int32)
-    if z0 is None:
-        oz = torch.zeros_like(ox)
-    else:
-        oz = torch.as_tensor(z0, dtype=torch.int32, device=dose.device).expand_as(ox).contiguous()
-    return torch.stack([ox, oy, oz], dim=1).contiguous()
-
-
 def gather(src, grid_shape, origins, window, shared: bool = False):
     """Windows [C, wx, wy, wz] of src ([C, vox], or one shared [vox] volume)."""
     torch = _torch()
@@ -119,6 +100,166 @@ def scatter(win, scale, grid_shape, origins, dst) -> None:
                                            nx, ny, nz, origins.data_ptr(), n, wx, wy, wz,
                                            dst.data_ptr(), int(np.prod(grid_shape)),
                                            _stream(win.device)), "scatter windows")
+
+
+def beam_directions(source) -> np.ndarray:
+    """Unit travel direction [n_beamlets, 3] of every column's central ray:
+    aperture centre minus focal spot for a divergent fan, +z for a lattice
+    (and for sources whose geometry is not known here), part by part for a
+    concatenation."""
+    parts = getattr(source, "sources", None)
+    if parts is not None and hasattr(source, "part_of"):
+        return np.concatenate([beam_directions(p) for p in parts]) if parts else np.zeros((0, 3))
+    n = int(source.n_beamlets)
+    focal, centers = getattr(source, "focal_point", None), getattr(source, "centers", None)
+    if focal is None or centers is None:
+        return np.tile([0.0, 0.0, 1.0], (n, 1))
+    d = np.asarray(centers, dtype=np.float64) - np.asarray(focal, dtype=np.float64)[None, :]
+    return d / np.linalg.norm(d, axis=1, keepdims=True)
+
+
+def orientation_codes(directions) -> np.ndarray:
+    """int32 [n]: 2 * (axis of the largest |component|) + (1 if it is negative)."""
+    d = np.asarray(directions, dtype=np.float64).reshape(-1, 3)
+    axis = np.argmax(np.abs(d), axis=1)
+    neg = d[np.arange(d.shape[0]), axis] < 0
+    return (2 * axis + neg).astype(np.int32)
+
+
+def _frame(orient: int):
+    """(lateral axis 1, lateral axis 2, depth axis, reversed) of an orientation code."""
+    d, f = orient >> 1, orient & 1
+    lat = [a for a in range(3) if a != d]
+    return lat[0], lat[1], d, bool(f)
+
+
+WIN_INTS = 7      # (ox, oy, oz, orient, col, shear1, shear2) per oriented window
+SHEAR_ONE = 65536  # shear unit: 1/65536 voxel per depth plane
+
+
+SHEAR_MIN = 0.1  # voxels per depth plane: beamlets closer to their axis keep plain windows
+
+
+def oriented_windows(dose, grid_shape, directions, window, starts=None, spacing=None):
+    """int32 [W, 7] oriented windows (ox, oy, oz, orient, col, shear1, shear2)
+    of dense columns dose [C, vox] (pmd_gather_windows_oriented).
+    `directions` [C, 3] are the beamlets' travel directions and `window` =
+    (wa, wb, wd) the lateral and depth extent.  A window's depth axis is the
+    grid axis closest to its beamlet, read from the beam's entry side, and for
+    a beamlet that drifts at least SHEAR_MIN voxels per depth plane its lateral
+    axes shear with depth along the beamlet (1/65536-voxel steps), so an
+    oblique beamlet runs straight down the window (a near-axial one keeps the
+    plain window: whole-voxel steps ten or more planes apart would only add
+    jitter).  Without `starts` every
+    column is covered along its whole depth by consecutive depth chunks of wd
+    planes (the last may reach past the grid); with `starts` ([C], depth planes
+    counted from the entry side) each column gets one window there.  A
+    window's lateral position is the dose-weighted mean of the beamlet's
+    sheared axis over its depth range (the column's own where that range
+    holds no dose), clamped so that its middle plane lies inside the grid."""
+    torch = _torch()
+    dev = dose.device
+    n_cols = dose.shape[0]
+    dirs = np.asarray(directions, dtype=np.float64).reshape(n_cols, 3)
+    orient = orientation_codes(dirs)
+    sp = np.ones(3) if spacing is None else np.asarray(spacing, dtype=np.float64)
+    wa, wb, wd = window
+    vol = dose.view(n_cols, *grid_shape)
+    out = []
+    for code in np.unique(orient):
+        cols = np.nonzero(orient == code)[0]
+        l1, l2, d, rev = _frame(int(code))
+        n1, n2, nd = grid_shape[l1], grid_shape[l2], grid_shape[d]
+        idx = torch.from_numpy(cols).to(dev)
+        # voxels moved along l1, l2 per plane of depth, and the same in 1/65536 units
+        per_depth = np.abs(dirs[cols, d]) / sp[d]
+        slope1 = (dirs[cols, l1] / sp[l1]) / per_depth
+        slope2 = (dirs[cols, l2] / sp[l2]) / per_depth
+        sheared = np.maximum(np.abs(slope1), np.abs(slope2)) >= SHEAR_MIN
+        q1 = np.where(sheared, np.round(slope1 * SHEAR_ONE), 0).astype(np.int64)
+        q2 = np.where(sheared, np.round(slope2 * SHEAR_ONE), 0).astype(np.int64)
+        # lateral marginals per depth plane, a few columns at a time (no copy
+        # of the columns): m1 [c, n1, nd], m2 [c, n2, nd], depth from the entry side
+        m1 = torch.empty((len(cols), n1, nd), dtype=torch.float32, device=dev)
+        m2 = torch.empty((len(cols), n2, nd), dtype=torch.float32, device=dev)
+        j = 0
+        while j < len(cols):  # runs of consecutive columns, 16 at a time, as views
+            k = j + 1
+            while k < len(cols) and k - j < 16 and cols[k] == cols[k - 1] + 1:
+                k += 1
+            v = vol[int(cols[j]):int(cols[k - 1]) + 1].permute(0, 1 + l1, 1 + l2, 1 + d)
+            m1[j:k] = v.sum(dim=2)
+            m2[j:k] = v.sum(dim=1)
+            j = k
+        if rev:
+            m1, m2 = m1.flip(2), m2.flip(2)
+        t = torch.arange(nd, device=dev, dtype=torch.float32)
+        x1 = torch.arange(n1, device=dev, dtype=torch.float32)
+        x2 = torch.arange(n2, device=dev, dtype=torch.float32)
+        mass = m1.sum(dim=1)                                   # [c, nd] dose per depth plane
+        s1 = torch.as_tensor(q1, dtype=torch.float32, device=dev).view(-1, 1) / SHEAR_ONE
+        s2 = torch.as_tensor(q2, dtype=torch.float32, device=dev).view(-1, 1) / SHEAR_ONE
+        # first moments of the sheared lateral coordinates x - s * t, per plane
+        f1 = (m1 * x1.view(1, -1, 1)).sum(dim=1) - s1 * t * mass
+        f2 = (m2 * x2.view(1, -1, 1)).sum(dim=1) - s2 * t * mass
+        if starts is None:
+            n_ch = -(-nd // wd)
+            lo = (torch.arange(n_ch, device=dev) * wd).expand(len(cols), n_ch)
+        else:
+            lo = torch.as_tensor(np.asarray(starts)[cols], dtype=torch.int64, device=dev).view(-1, 1)
+        tt = torch.arange(nd, device=dev).view(1, 1, -1)
+        mask = ((tt >= lo.unsqueeze(2)) & (tt < lo.unsqueeze(2) + wd)).float()  # [c, chunks, nd]
+        w_ch = torch.einsum("ct,cjt->cj", mass, mask)
+        i1 = torch.einsum("ct,cjt->cj", f1, mask)
+        i2 = torch.einsum("ct,cjt->cj", f2, mask)
+        whole = mass.sum(dim=1, keepdim=True).clamp_min(1e-30)
+        ok = w_ch > 0
+        c1 = torch.where(ok, i1 / w_ch.clamp_min(1e-30), f1.sum(dim=1, keepdim=True) / whole)
+        c2 = torch.where(ok, i2 / w_ch.clamp_min(1e-30), f2.sum(dim=1, keepdim=True) / whole)
+        # window origin at its first plane; the middle plane is kept inside the grid
+        mid = lo.float() + wd / 2
+        o1 = torch.clamp(torch.round(c1 + s1 * mid - wa / 2), 0, max(n1 - wa, 0)) - torch.round(s1 * wd / 2)
+        o2 = torch.clamp(torch.round(c2 + s2 * mid - wb / 2), 0, max(n2 - wb, 0)) - torch.round(s2 * wd / 2)
+        od = (nd - (lo + wd)) if rev else lo
+        w = torch.zeros((*o1.shape, WIN_INTS), dtype=torch.int32, device=dev)
+        w[..., l1] = o1.to(torch.int32)
+        w[..., l2] = o2.to(torch.int32)
+        w[..., d] = od.to(torch.int32)
+        w[..., 3] = int(code)
+        w[..., 4] = idx.to(torch.int32).view(-1, 1)
+        w[..., 5] = torch.as_tensor(q1, dtype=torch.int32, device=dev).view(-1, 1)
+        w[..., 6] = torch.as_tensor(q2, dtype=torch.int32, device=dev).view(-1, 1)
+        out.append(w.view(-1, WIN_INTS))
+    if not out:
+        return torch.zeros((0, WIN_INTS), dtype=torch.int32, device=dev)
+    win = torch.cat(out)
+    order = torch.argsort(win[:, 4], stable=True)  # windows of a column together, in depth order
+    return win[order].contiguous()
+
+
+def gather_oriented(src, grid_shape, win, window, shared: bool = False):
+    """Oriented windows [W, wa, wb, wd] of src ([C, vox] read through each
+    window's column, or one shared [vox] volume)."""
+    torch = _torch()
+    nx, ny, nz = grid_shape
+    wa, wb, wd = window
+    n = win.shape[0]
+    out = torch.empty((n, wa, wb, wd), dtype=torch.float32, device=src.device)
+    stride = 0 if shared else int(np.prod(grid_shape))
+    _check(_lib.load().pmd_gather_windows_oriented(src.data_ptr(), stride, nx, ny, nz, win.data_ptr(),
+                                                   n, wa, wb, wd, out.data_ptr(), _stream(src.device)),
+           "gather oriented windows")
+    return out
+
+
+def scatter_oriented(data, scale, grid_shape, win, dst) -> None:
+    """dst[col] (f64 [C, vox]) <- max(data, 0) * scale[w] inside each window."""
+    nx, ny, nz = grid_shape
+    n, wa, wb, wd = data.shape
+    _check(_lib.load().pmd_scatter_windows_oriented(
+        data.data_ptr(), None if scale is None else scale.data_ptr(), nx, ny, nz, win.data_ptr(), n,
+        wa, wb, wd, dst.data_ptr(), int(np.prod(grid_shape)), _stream(data.device)),
+        "scatter oriented windows")
 
 
 # ---- training pairs --------------------------------------------------------------------
@@ -151,8 +292,9 @@ def make_pairs(grid, cross_sections, source, *, n_low, n_high: int, n_batches: i
                rng=None) -> PairSet:
     """Pairs of one phantom: the engine runs the beamlets at n_high histories
     each and at every count of n_low (an int or a sequence; independent
-    seeds), and each (low run, column) gives one window, laterally centred on
-    the column's dose and at a random depth."""
+    seeds), and each (low run, column) gives one window along the column's
+    beamlet (:func:`oriented_windows`, centred on the high-history dose) at a
+    random depth."""
     from .denoiser import loss_weight
     from .engine import B200Engine
 
@@ -163,19 +305,20 @@ def make_pairs(grid, cross_sections, source, *, n_low, n_high: int, n_batches: i
     hi = engine.run_dij_device(source, n_high, n_batches, seed + 7919, truncation=0.0)
     hi_dose, _, hi_sigma = dense_columns(hi, device, with_sigma=True)
     rho = torch.from_numpy(np.ascontiguousarray(grid.density, dtype=np.float32).ravel()).to(device)
+    directions = beam_directions(source)
+    depth_extent = np.array([shape[o >> 1] for o in orientation_codes(directions)])
     sets = []
     for k, n in enumerate(np.atleast_1d(n_low)):
         lo = engine.run_dij_device(source, int(n), n_batches, seed + 31 * k, truncation=0.0)
         lo_dose, lo_max, lo_sigma = dense_columns(lo, device, with_sigma=True)
-        n_cols = lo.n_beamlets
-        z0 = rng.integers(0, max(shape[2] - window[2], 0) + 1, size=n_cols)
-        origins = lateral_origins(hi_dose, shape, window, z0)
-        scale = (1.0 / lo_max.clamp_min(1e-30)).view(-1, 1, 1, 1)
-        x = gather(lo_dose, shape, origins, window) * scale
-        t = gather(hi_dose, shape, origins, window) * scale
-        s = gather(hi_sigma, shape, origins, window) * scale
-        d = gather(rho, shape, origins, window, shared=True)
-        e = gather(lo_sigma, shape, origins, window) * scale
+        starts = rng.integers(0, np.maximum(depth_extent - window[2], 0) + 1)
+        win = oriented_windows(hi_dose, shape, directions, window, starts, spacing=grid.spacing)
+        scale = (1.0 / lo_max.clamp_min(1e-30))[win[:, 4].to(torch.int64)].view(-1, 1, 1, 1)
+        x = gather_oriented(lo_dose, shape, win, window) * scale
+        t = gather_oriented(hi_dose, shape, win, window) * scale
+        s = gather_oriented(hi_sigma, shape, win, window) * scale
+        d = gather_oriented(rho, shape, win, window, shared=True)
+        e = gather_oriented(lo_sigma, shape, win, window) * scale
         sets.append(PairSet(x, t, s, d, loss_weight(t, s, precision), e))
         del lo_dose, lo_sigma
     del hi_dose, hi_sigma
@@ -197,12 +340,14 @@ def concat(sets: list[PairSet]) -> PairSet:
 
 def train(net: UNet3D, pairs: PairSet, *, steps: int, batch: int = 4, seed: int = 0,
           lr_final: float | None = None, log_every: int = 100, log=None,
-          keep_best: bool = True) -> list[float]:
+          keep_best: bool = True, warmup: int = 0) -> list[float]:
     """Adam steps over random mini-batches of the pairs; returns the mean loss of
     every ``log_every`` steps.  With lr_final the learning rate decays
-    geometrically from net.lr to lr_final.  With keep_best the network ends
-    with the parameters of the interval whose mean loss was lowest (a late
-    divergence cannot lose a good network)."""
+    geometrically from net.lr to lr_final; the first ``warmup`` steps ramp it
+    up linearly from zero (Adam's first steps move every parameter by about the
+    learning rate, too far for a network that is already trained).  With
+    keep_best the network ends with the parameters of the interval whose mean
+    loss was lowest (a late divergence cannot lose a good network)."""
     torch = _torch()
     g = torch.Generator(device="cpu").manual_seed(seed)
     lr0 = net.lr
@@ -210,8 +355,11 @@ def train(net: UNet3D, pairs: PairSet, *, steps: int, batch: int = 4, seed: int 
     best, best_params = float("inf"), None
     n = len(pairs)
     for step in range(steps):
+        net.lr = lr0
         if lr_final is not None:
             net.lr = lr0 * (lr_final / lr0) ** (step / max(steps - 1, 1))
+        if step < warmup:
+            net.lr *= (step + 1) / warmup
         idx = torch.randint(0, n, (batch,), generator=g).to(net.device)
         acc += net.train_step(pairs.inputs[idx].contiguous(), pairs.density[idx].contiguous(),
                               pairs.targets[idx].contiguous(), pairs.weight[idx].contiguous(),
@@ -231,39 +379,44 @@ def train(net: UNet3D, pairs: PairSet, *, steps: int, batch: int = 4, seed: int 
 
 
 # ---- the denoised Dij ------------------------------------------------------------------
-def inference_window(grid_shape, lateral: int = 64) -> tuple[int, int, int]:
-    """The denoising window: `lateral` voxels (at most the grid, a multiple of 8)
-    across, the full depth rounded up to a multiple of 8."""
-    nx, ny, nz = grid_shape
-    wx = min(lateral, nx - nx % 8) or 8
-    wy = min(lateral, ny - ny % 8) or 8
-    return wx, wy, -(-nz // 8) * 8
+def inference_window(grid_shape, lateral: int = 64, depth: int | None = None) -> tuple[int, int, int]:
+    """The denoising window (wa, wb, wd): `lateral` voxels across (at most the
+    smallest grid extent, a multiple of 8) and `depth` planes deep (default:
+    the z extent rounded up to a multiple of 8, one chunk for beams along z)."""
+    smallest = min(grid_shape)
+    wa = min(lateral, smallest - smallest % 8) or 8
+    wd = depth if depth is not None else -(-grid_shape[2] // 8) * 8
+    return wa, wa, wd
 
 
 def denoise_dense(net: UNet3D, dose, colmax, density, grid_shape, *, sigma=None, window=None,
-                  chunk: int = 32, out=None):
+                  chunk: int = 32, out=None, directions=None, spacing=None):
     """Denoised dense columns, float64 [C, vox]: the Monte Carlo columns
     (float32 dose [C, vox] with their maxima and, optionally, their sigma; or
-    `out`, float64, written in place) with every column's window replaced by
-    the network's estimate.  `density` is the shared [vox] volume."""
+    `out`, float64, written in place) with every window along each column's
+    beamlet replaced by the network's estimate.  `density` is the shared [vox]
+    volume; `directions` [C, 3] the beamlets' travel directions (default +z)
+    and `spacing` the voxel size (default isotropic)."""
     torch = _torch()
     window = window or inference_window(grid_shape)
-    origins = lateral_origins(dose, grid_shape, window)
+    n = dose.shape[0]
+    dirs = np.tile([0.0, 0.0, 1.0], (n, 1)) if directions is None else np.asarray(directions)
+    win = oriented_windows(dose, grid_shape, dirs, window, spacing=spacing)
     if out is None:
         out = dose.to(torch.float64)
-    n = dose.shape[0]
-    chunk = -(-n // -(-n // chunk))  # equal chunks of at most `chunk` windows: no padded work
-    for c0 in range(0, n, chunk):
-        c1 = min(c0 + chunk, n)
-        idx = torch.arange(c0, c0 + chunk, device=dose.device).clamp_max(n - 1)  # fixed batch shape
-        org = origins[idx].contiguous()
-        x = gather(dose[idx].contiguous(), grid_shape, org, window)
-        rho = gather(density, grid_shape, org, window, shared=True)
-        sg = None if sigma is None else gather(sigma[idx].contiguous(), grid_shape, org, window)
-        cm = colmax[idx].contiguous()
+    scale = colmax[win[:, 4].to(torch.int64)].contiguous()
+    n_win = win.shape[0]
+    chunk = -(-n_win // -(-n_win // chunk))  # equal chunks of at most `chunk` windows: no padded work
+    for w0 in range(0, n_win, chunk):
+        w1 = min(w0 + chunk, n_win)
+        idx = torch.arange(w0, w0 + chunk, device=dose.device).clamp_max(n_win - 1)  # fixed batch shape
+        wsel = win[idx].contiguous()
+        x = gather_oriented(dose, grid_shape, wsel, window)
+        rho = gather_oriented(density, grid_shape, wsel, window, shared=True)
+        sg = None if sigma is None else gather_oriented(sigma, grid_shape, wsel, window)
+        cm = scale[idx].contiguous()
         y = net.predict(x, rho, colmax=cm, sigma=sg)
-        scatter(y[: c1 - c0], cm[: c1 - c0], grid_shape, org[: c1 - c0].contiguous(),
-                out[c0:c1])
+        scatter_oriented(y[: w1 - w0], cm[: w1 - w0], grid_shape, wsel[: w1 - w0].contiguous(), out)
     return out
 
 
@@ -298,14 +451,19 @@ def compact(mean, sigma, truncation: float, to_host: bool = True):
 
 
 def run_dij_denoised(engine, net: UNet3D | None, source, n_histories_per_beamlet, n_batches: int,
-                     seed: int, *, truncation: float = 1.0e-3, lateral: int = 64, chunk: int = 32,
-                     to_host: bool = True, timings: dict | None = None):
+                     seed: int, *, truncation: float = 1.0e-3, lateral: int = 64,
+                     depth: int | None = None, chunk: int = 32, to_host: bool = True,
+                     timings: dict | None = None, group_columns: int | None = None):
     """A Dij from low-history Monte Carlo plus the denoiser: the engine runs the
-    beamlets (``run_dij_device``), every column's window around its beamlet is
-    replaced by the network's estimate, and the dense columns are truncated and
-    compacted to CSC on the device.  With ``to_host`` False the CSC entries
-    stay on the device (torch tensors in the result).  With ``net`` None this is
-    plain Monte Carlo (``engine.run_dij``), the method's fallback.
+    beamlets (``run_dij_device``), the windows along every column's beamlet
+    (``lateral`` voxels across, ``depth`` planes per chunk; see
+    :func:`oriented_windows`) are replaced by the network's estimate, and the
+    dense columns are truncated and compacted to CSC on the device.  Columns
+    go through in groups of ``group_columns`` (all at once when None: the dense
+    maps of a group must fit the device), each group with the same history
+    keys as in the whole Dij.  With ``to_host`` False the CSC entries stay on
+    the device (torch tensors in the result).  With ``net`` None this is plain
+    Monte Carlo (``engine.run_dij``), the method's fallback.
 
     The per-entry ``sigma`` of the result is the batch sigma of the
     low-history Monte Carlo input, not an uncertainty of the denoised value:
@@ -320,6 +478,12 @@ def run_dij_denoised(engine, net: UNet3D | None, source, n_histories_per_beamlet
     if net is None:
         return engine.run_dij(source, n_histories_per_beamlet, n_batches, seed,
                               truncation=truncation)
+    n_cols = int(source.n_beamlets)
+    counts = (np.full(n_cols, int(n_histories_per_beamlet), dtype=np.int64)
+              if np.ndim(n_histories_per_beamlet) == 0
+              else np.asarray(n_histories_per_beamlet, dtype=np.int64))
+    directions = beam_directions(source)
+    group = n_cols if not group_columns else int(group_columns)
     marks = []
 
     def mark(name):  # CUDA events between the stages, read when `timings` is given
@@ -328,30 +492,49 @@ def run_dij_denoised(engine, net: UNet3D | None, source, n_histories_per_beamlet
             ev.record()
             marks.append((name, ev))
 
+    pieces, books, shape = [], np.zeros(4, dtype=np.int64), None
+    rho = None
     mark("start")
-    view = engine.run_dij_device(source, n_histories_per_beamlet, n_batches, seed, truncation=0.0)
-    device = torch.device(view.device)
-    shape = tuple(view.grid_shape)
-    mark("monte_carlo")
-    dose, colmax, sigma32 = dense_columns(view, device, with_sigma=True)
-    mean, sigma = dense_columns_f64(view, device)
-    rho = torch.from_numpy(np.ascontiguousarray(engine.grid.density, dtype=np.float32).ravel()).to(device)
-    mark("dense_columns")
-    denoise_dense(net, dose, colmax, rho, shape, sigma=sigma32,
-                  window=inference_window(shape, lateral), chunk=chunk, out=mean)
-    del dose, sigma32
-    mark("unet")
-    indptr, indices, dose_v, sigma_v = compact(mean, sigma, truncation, to_host=to_host)
-    mark("compaction")
+    for lo in range(0, n_cols, group):
+        hi = min(lo + group, n_cols)
+        view = engine.run_dij_device(source, counts, n_batches, seed, truncation=0.0,
+                                     columns=(lo, hi))
+        device = torch.device(view.device)
+        shape = tuple(view.grid_shape)
+        mark("monte_carlo")
+        dose, colmax, sigma32 = dense_columns(view, device, with_sigma=True)
+        mean, sigma = dense_columns_f64(view, device)
+        books += np.asarray(view.books, dtype=np.int64)
+        if rho is None:
+            rho = torch.from_numpy(np.ascontiguousarray(engine.grid.density, dtype=np.float32)
+                                   .ravel()).to(device)
+        mark("dense_columns")
+        denoise_dense(net, dose, colmax, rho, shape, sigma=sigma32,
+                      window=inference_window(shape, lateral, depth), chunk=chunk, out=mean,
+                      directions=directions[lo:hi], spacing=engine.grid.spacing)
+        del dose, sigma32
+        mark("unet")
+        pieces.append(compact(mean, sigma, truncation, to_host=False))
+        del mean, sigma
+        mark("compaction")
     if timings is not None:
         marks[-1][1].synchronize()
         for (_, a), (name, b) in zip(marks, marks[1:]):
             timings[name] = timings.get(name, 0.0) + a.elapsed_time(b)
-    deposited, escaped, unscored, emitted = view.books
-    counts = np.asarray(view.counts)
+    indptr = np.zeros(n_cols + 1, dtype=np.int64)
+    col = 0
+    for ptr, *_ in pieces:
+        k = len(ptr) - 1
+        indptr[col + 1:col + k + 1] = indptr[col] + ptr[1:]
+        col += k
+    joined = [torch.cat([p[i] for p in pieces]) for i in (1, 2, 3)]
+    if to_host:
+        joined = [t.cpu().numpy() for t in joined]
+    indices, dose_v, sigma_v = joined
+    deposited, escaped, unscored, emitted = books
     _, _, DijResult = _result_types()
     return DijResult(
-        grid_shape=shape, n_beamlets=view.n_beamlets,
+        grid_shape=shape, n_beamlets=n_cols,
         n_histories_per_beamlet=int(counts.max()), n_batches=n_batches, truncation=truncation,
         indptr=indptr, indices=indices, dose=dose_v, sigma=sigma_v,
         energy_emitted=float(emitted) * ENERGY_QUANTUM_MEV,

@@ -60,31 +60,36 @@ def beamlet_fan(grid, n_x=10, n_y=10, pitch=0.5, width=0.5, sad=100.0, spectrum=
     return model.SpectralBeamletSource(spectrum, focal, centers, width, width)
 
 
-def coplanar_plan(grid, n_beams=7, n_u=20, n_v=20, pitch=0.5, width=0.5, sad=100.0,
-                  spectrum=None, first_angle_deg=0.0):
-    """A coplanar treatment plan: `n_beams` equi-spaced gantry angles around the
-    z axis through the phantom centre (the isocentre), each beam an n_u x n_v
-    lattice of pitch-spaced beamlet apertures at the isocentre plane.
-
-    Gantry angle t points the beam along (sin t, cos t, 0) from a focal spot
-    `sad` cm before the isocentre; the aperture axes are (cos t, -sin t, 0) and
-    z.  Returns a ConcatenatedBeamletSource of one SpectralBeamletSource per
-    beam (beam-major column order) and the gantry angles in degrees.
-    """
+def gantry_beam(grid, angle_deg, n_u=10, n_v=10, pitch=0.5, width=0.5, sad=100.0, spectrum=None):
+    """One coplanar beam at gantry angle `angle_deg` about the z axis through
+    the phantom centre (the isocentre): the beam travels along (sin t, cos t, 0)
+    from a focal spot `sad` cm before the isocentre, through an n_u x n_v
+    lattice of pitch-spaced `width` apertures on the axes (cos t, -sin t, 0)
+    and z."""
     extent = np.array(grid.shape) * np.array(grid.spacing)
     iso = np.asarray(grid.origin) + 0.5 * extent
     spectrum = spectrum if spectrum is not None else model.ali_rogers_varian_6mv()
-    beams, angles = [], []
-    for k in range(n_beams):
-        t = np.deg2rad(first_angle_deg + 360.0 * k / n_beams)
-        d = np.array([np.sin(t), np.cos(t), 0.0])
-        u = np.array([np.cos(t), -np.sin(t), 0.0])
-        v = np.array([0.0, 0.0, 1.0])
-        centers = [tuple(iso + (i - (n_u - 1) / 2) * pitch * u + (j - (n_v - 1) / 2) * pitch * v)
-                   for i in range(n_u) for j in range(n_v)]
-        beams.append(model.SpectralBeamletSource(spectrum, tuple(iso - sad * d), centers, width,
-                                                 width, tuple(u), tuple(v)))
-        angles.append(float(np.rad2deg(t)))
+    t = np.deg2rad(angle_deg)
+    d = np.array([np.sin(t), np.cos(t), 0.0])
+    u = np.array([np.cos(t), -np.sin(t), 0.0])
+    v = np.array([0.0, 0.0, 1.0])
+    centers = [tuple(iso + (i - (n_u - 1) / 2) * pitch * u + (j - (n_v - 1) / 2) * pitch * v)
+               for i in range(n_u) for j in range(n_v)]
+    return model.SpectralBeamletSource(spectrum, tuple(iso - sad * d), centers, width, width,
+                                       tuple(u), tuple(v))
+
+
+def coplanar_plan(grid, n_beams=7, n_u=20, n_v=20, pitch=0.5, width=0.5, sad=100.0,
+                  spectrum=None, first_angle_deg=0.0):
+    """A coplanar treatment plan: `n_beams` equi-spaced gantry angles
+    (:func:`gantry_beam`), each an n_u x n_v lattice of beamlet apertures at
+    the isocentre plane.  Returns a ConcatenatedBeamletSource of one
+    SpectralBeamletSource per beam (beam-major column order) and the gantry
+    angles in degrees.
+    """
+    spectrum = spectrum if spectrum is not None else model.ali_rogers_varian_6mv()
+    angles = [float(first_angle_deg + 360.0 * k / n_beams) for k in range(n_beams)]
+    beams = [gantry_beam(grid, a, n_u, n_v, pitch, width, sad, spectrum) for a in angles]
     return model.ConcatenatedBeamletSource(beams), angles
 
 

@@ -1,14 +1,21 @@
 """Train the Dij-column denoiser on pairs the engine makes, and evaluate it.
 
 ``python -m pyradmc_b200.train_denoiser --out weights.npz`` builds the training
-set of the denoiser workload: seeded CT-like phantoms (128^3 at 2.5 mm, water
-plus 6-12 random ellipsoids), a 10x10 lattice of 5x5 mm 6 MV beamlets on each,
-every column run at each ``--n-low`` count and at ``--n-high`` histories per
-beamlet, cropped to 64^3 windows around the beamlet (input: the low-history
-dose and its Monte Carlo sigma, plus the density); then trains the U-Net with Adam on the
-device (the project's own forward and backward kernels) and evaluates it on a
-held-out phantom against high-statistics Monte Carlo.  One JSON line with the
-loss curve and the evaluation goes to stdout.
+set of the denoiser workload: seeded CT-like phantoms (128^3, water plus 6-12
+random ellipsoids), each with one 10x10 lattice of 6 MV beamlets, every column
+run at each ``--n-low`` count and at ``--n-high`` histories per beamlet,
+cropped to 64^3 windows along the beamlet (input: the low-history dose and its
+Monte Carlo sigma, plus the density).  With ``--geometry mixed`` (the default)
+the phantoms alternate 2.5 and 3 mm voxels and the beams vary: a third travel
+along +z as in the benchmark Dij, the rest come from a random gantry angle in
+the x-y plane as in a coplanar plan, with beamlet widths of 3-10 mm and focal
+distances of 80-120 cm; ``--geometry axial`` keeps the benchmark's 5 mm fan at
+100 cm on 2.5 mm phantoms; ``--geometry coplanar`` draws gantry beams only
+(mostly 3 mm voxels and 5 mm beamlets, focal distances 90-110 cm), the
+training set of the network a coplanar plan uses.  The U-Net then trains with Adam on the device (the
+project's own forward and backward kernels) and is evaluated on held-out
+phantoms against high-statistics Monte Carlo.  One JSON line with the loss
+curve and the evaluation goes to stdout.
 """
 
 from __future__ import annotations
@@ -23,7 +30,7 @@ import numpy as np
 from . import denoise_dij as D
 from .denoiser import UNet3D
 from .model import AnalyticWaterTables
-from .phantoms import beamlet_fan, ellipsoid_phantom
+from .phantoms import beamlet_fan, ellipsoid_phantom, gantry_beam
 
 TRAIN_SEED0 = 1000      # phantom seeds of the training set: TRAIN_SEED0 + i
 HELD_OUT_SEED = 999     # the evaluation phantom
@@ -35,13 +42,58 @@ def phantom(seed: int):
     return grid, xs, beamlet_fan(grid)
 
 
-def build_pairs(n_phantoms: int, n_low, n_high: int, n_batches: int, device: str, log):
+BEAMLET_WIDTHS_CM = (0.3, 0.5, 0.7, 1.0)
+
+
+def training_case(i: int, geometry: str = "mixed"):
+    """(grid, cross sections, beamlet source) of training phantom i."""
+    if geometry == "axial":
+        return phantom(TRAIN_SEED0 + i)
+    rng = np.random.default_rng(TRAIN_SEED0 + 7 * i)
+    if geometry == "coplanar":  # gantry beams as in a coplanar plan, mostly 5 mm at 3 mm voxels
+        spacing = 0.3 if i % 4 else 0.25
+        grid = ellipsoid_phantom(seed=TRAIN_SEED0 + i, spacing=(spacing,) * 3)
+        xs = AnalyticWaterTables(geometry_densities=grid.max_density_by_material())
+        width = 0.5 if i % 2 == 0 else float(rng.choice(BEAMLET_WIDTHS_CM))
+        return grid, xs, gantry_beam(grid, float(rng.uniform(0.0, 360.0)), pitch=width,
+                                     width=width, sad=float(rng.uniform(90.0, 110.0)))
+    spacing = 0.25 if i % 2 == 0 else 0.3
+    grid = ellipsoid_phantom(seed=TRAIN_SEED0 + i, spacing=(spacing,) * 3)
+    xs = AnalyticWaterTables(geometry_densities=grid.max_density_by_material())
+    width = float(rng.choice(BEAMLET_WIDTHS_CM))
+    sad = float(rng.uniform(80.0, 120.0))
+    if i % 3 == 0:
+        return grid, xs, beamlet_fan(grid, pitch=width, width=width, sad=sad)
+    return grid, xs, gantry_beam(grid, float(rng.uniform(0.0, 360.0)), pitch=width, width=width,
+                                 sad=sad)
+
+
+def held_out_oblique():
+    """A held-out geometry outside the training draws: a phantom seed the
+    training set does not use at 3 mm, 8 mm beamlets from a focal spot 90 cm
+    away at gantry angle 33 degrees."""
+    grid = ellipsoid_phantom(seed=HELD_OUT_SEED - 1, spacing=(0.3, 0.3, 0.3))
+    xs = AnalyticWaterTables(geometry_densities=grid.max_density_by_material())
+    return grid, xs, gantry_beam(grid, 33.0, n_u=10, n_v=1, pitch=0.8, width=0.8, sad=90.0)
+
+
+def held_out_plan_like():
+    """A held-out case shaped like one beam of the coplanar plan: 3 mm voxels, a
+    row of ten 5 mm beamlets at SAD 100 from gantry angle 102.86 degrees (the
+    plan's third beam), on a phantom seed the training set does not use."""
+    grid = ellipsoid_phantom(seed=HELD_OUT_SEED - 2, spacing=(0.3, 0.3, 0.3))
+    xs = AnalyticWaterTables(geometry_densities=grid.max_density_by_material())
+    return grid, xs, gantry_beam(grid, 360.0 * 2 / 7, n_u=10, n_v=1)
+
+
+def build_pairs(n_phantoms: int, n_low, n_high: int, n_batches: int, device: str, log,
+                geometry: str = "mixed"):
     import torch
 
     sets = []
     for i in range(n_phantoms):
         t0 = time.perf_counter()
-        grid, xs, fan = phantom(TRAIN_SEED0 + i)
+        grid, xs, fan = training_case(i, geometry)
         sets.append(D.make_pairs(grid, xs, fan, n_low=n_low, n_high=n_high, n_batches=n_batches,
                                  seed=20260726 + 101 * i, device=device,
                                  rng=np.random.default_rng(i)))
@@ -50,15 +102,18 @@ def build_pairs(n_phantoms: int, n_low, n_high: int, n_batches: int, device: str
     return D.concat(sets)
 
 
-def evaluate(net: UNet3D, n_levels, n_ref: int, n_batches: int, device: str, laterals=(64,)):
+def evaluate(net: UNet3D, n_levels, n_ref: int, n_batches: int, device: str, laterals=(64,),
+             case=None, depth=None):
     """Per-beamlet sigma-equivalent error of plain MC and of MC + denoiser (for
-    each lateral window size) at each history level, on the held-out phantom,
-    against an n_ref-history run."""
+    each lateral window size) at each history level, on a held-out case (the
+    axial fan on phantom HELD_OUT_SEED by default), against an n_ref-history
+    run; ``depth`` is the window's depth chunk (default: the z extent)."""
     import torch
 
     from .engine import B200Engine
 
-    grid, xs, fan = phantom(HELD_OUT_SEED)
+    grid, xs, fan = case if case is not None else phantom(HELD_OUT_SEED)
+    directions = D.beam_directions(fan)
     engine = B200Engine(grid=grid, cross_sections=xs, device=device)
     shape = tuple(grid.shape)
     ref = engine.run_dij_device(fan, n_ref, n_batches, 424242, truncation=0.0)
@@ -71,11 +126,13 @@ def evaluate(net: UNet3D, n_levels, n_ref: int, n_batches: int, device: str, lat
         plain = D.sigma_equivalent_error(dose, ref_dose, ref_sigma)
         level = {"n_per_beamlet": int(n), "plain": float(np.nanmean(plain))}
         for lateral in laterals:
-            window = D.inference_window(shape, lateral)
-            D.denoise_dense(net, dose, colmax, rho, shape, sigma=sg, window=window)  # warm-up
+            window = D.inference_window(shape, lateral, depth)
+            D.denoise_dense(net, dose, colmax, rho, shape, sigma=sg, window=window,
+                            directions=directions, spacing=grid.spacing)  # warm-up
             torch.cuda.synchronize()
             t0 = time.perf_counter()
-            den = D.denoise_dense(net, dose, colmax, rho, shape, sigma=sg, window=window)
+            den = D.denoise_dense(net, dose, colmax, rho, shape, sigma=sg, window=window,
+                                  directions=directions, spacing=grid.spacing)
             torch.cuda.synchronize()
             t_den = time.perf_counter() - t0
             denoised = D.sigma_equivalent_error(den, ref_dose, ref_sigma)
@@ -101,12 +158,18 @@ def main(argv=None) -> int:
     ap.add_argument("--lr", type=float, default=3.0e-4)
     ap.add_argument("--lr-final", type=float, default=3.0e-5)
     ap.add_argument("--loss-lambda", type=float, default=50.0)
+    ap.add_argument("--warmup", type=int, default=1000,
+                    help="steps of linear learning-rate warm-up (a fine-tune from --init at full "
+                         "rate measured a collapse to the identity)")
     ap.add_argument("--init", default=None, help="start from these weights")
     ap.add_argument("--eval-only", action="store_true",
                     help="evaluate the --init weights without training")
     ap.add_argument("--eval-levels", default="10000,30000,100000,300000")
     ap.add_argument("--n-ref", type=int, default=4_000_000)
     ap.add_argument("--eval-lateral", default="64")
+    ap.add_argument("--geometry", choices=("mixed", "axial", "coplanar"), default="mixed",
+                    help="training beams: mixed gantry angles, widths and focal distances; the "
+                         "benchmark's axial 5 mm fan; or coplanar gantry beams as in a plan")
     args = ap.parse_args(argv)
 
     def log(msg):
@@ -122,12 +185,13 @@ def main(argv=None) -> int:
         net = UNet3D(args.device, seed=0, lr=args.lr, loss_lambda=args.loss_lambda)
     if not args.eval_only:
         t0 = time.perf_counter()
-        pairs = build_pairs(args.phantoms, n_low, args.n_high, args.n_batches, args.device, log)
+        pairs = build_pairs(args.phantoms, n_low, args.n_high, args.n_batches, args.device, log,
+                            args.geometry)
         n_pairs = len(pairs)
         t_data = time.perf_counter() - t0
         t0 = time.perf_counter()
         history = D.train(net, pairs, steps=args.steps, batch=args.batch, lr_final=args.lr_final,
-                          log_every=max(args.steps // 40, 1), log=log)
+                          log_every=max(args.steps // 40, 1), log=log, warmup=args.warmup)
         t_train = time.perf_counter() - t0
         net.save(args.out)
         del pairs
@@ -136,9 +200,17 @@ def main(argv=None) -> int:
     levels = [int(v) for v in args.eval_levels.split(",") if v]
     laterals = [int(v) for v in args.eval_lateral.split(",") if v]
     ev = evaluate(net, levels, args.n_ref, args.n_batches, args.device, laterals)
+    log(f"axial evaluation: {ev}")
+    ev_oblique = evaluate(net, levels, args.n_ref, args.n_batches, args.device, laterals,
+                          case=held_out_oblique(), depth=64)
+    log(f"oblique evaluation: {ev_oblique}")
+    ev_plan = evaluate(net, levels, args.n_ref, args.n_batches, args.device, laterals,
+                       case=held_out_plan_like(), depth=64)
     print(json.dumps({"pairs": n_pairs, "n_low": n_low, "n_high": args.n_high,
-                      "loss_lambda": args.loss_lambda, "data_s": t_data, "train_s": t_train,
-                      "steps": args.steps, "loss": history, "evaluation": ev}))
+                      "geometry": args.geometry, "loss_lambda": args.loss_lambda,
+                      "data_s": t_data, "train_s": t_train, "steps": args.steps, "loss": history,
+                      "evaluation": ev, "evaluation_oblique": ev_oblique,
+                      "evaluation_plan_beam": ev_plan}))
     return 0
 
 

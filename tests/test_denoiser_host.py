@@ -120,3 +120,66 @@ def test_convolution_plans_of_the_network_layers():
     assert plans["dec0a"][1:7] == [2, 3, 3, 0, 2, 2]  # three resident groups, two blocks per SM
     assert plans["dec1a"][4] == 0  # 166 KB of weights stay resident
     assert all(plans[n][4] == 1 for n in ("enc2b", "mid_a", "mid_b", "dec2a", "dec2b"))
+
+
+def _window_map(win, window, shape):
+    """(grid index or -1) of every voxel of one oriented window: the map of
+    pmd_gather_windows_oriented restated in numpy."""
+    ox, oy, oz, orient, _, q1, q2 = (int(v) for v in win)
+    d, f = orient >> 1, orient & 1
+    l1, l2 = [a for a in range(3) if a != d]
+    wa, wb, wd = window
+    out = np.full((wa, wb, wd, 3), -1, dtype=np.int64)
+    o = (ox, oy, oz)
+    for k in range(wd):
+        s1, s2 = (k * q1 + 32768) >> 16, (k * q2 + 32768) >> 16
+        for a in range(wa):
+            for b in range(wb):
+                g = [0, 0, 0]
+                g[l1], g[l2] = o[l1] + a + s1, o[l2] + b + s2
+                g[d] = o[d] + (wd - 1 - k if f else k)
+                if all(0 <= g[i] < shape[i] for i in range(3)):
+                    out[a, b, k] = g
+    return out
+
+
+def test_oriented_windows_follow_each_beamlet():
+    """Window planning (torch on the CPU): an oblique beamlet travelling
+    towards -x and drifting in +y gets depth chunks along x from its entry side,
+    sheared so that the beamlet stays within a voxel of the window's centre line
+    at every depth; a +z beamlet gets the plain, unsheared window."""
+    from pyradmc_b200 import denoise_dij as D
+
+    shape = (40, 24, 16)
+    dose = torch.zeros((2, *shape))
+    beam = {}
+    for x in range(40):
+        t = 39 - x  # depth from the entry side (the beam enters at x = 39)
+        y = int(round(4 + 0.4 * t))
+        dose[0, x, y, 8] = 1.0 + 0.01 * t
+        beam[(x, y, 8)] = t
+    dose[1, 5, 7, :] = 1.0
+    dirs = np.array([[-1.0, 0.4, 0.0], [0.0, 0.0, 1.0]])
+    dirs /= np.linalg.norm(dirs, axis=1, keepdims=True)
+    assert D.orientation_codes(dirs).tolist() == [1, 4]
+    window = (8, 8, 16)
+    win = D.oriented_windows(dose.view(2, -1), shape, dirs, window).numpy()
+    assert win.shape[1] == 7 and win[:, 4].tolist() == [0, 0, 0, 1]
+    first = win[win[:, 4] == 0]
+    assert (first[:, 3] == 1).all() and (first[:, 5] == round(0.4 * 65536)).all()
+    assert (first[:, 6] == 0).all()
+    assert first[:, 0].tolist() == [40 - 16, 40 - 32, 40 - 48]  # chunks from the entry side
+    seen = 0
+    for w in first:
+        m = _window_map(w, window, shape)
+        for a in range(8):
+            for b in range(8):
+                for k in range(16):
+                    g = tuple(m[a, b, k])
+                    if g in beam:  # the beamlet runs down the window's centre line
+                        assert abs(a - 3.5) <= 1.5 and b == 8 - int(w[2]), (g, a, b, k)
+                        seen += 1
+    assert seen == 40  # every beamlet voxel lies in one window
+    assert win[3].tolist() == [1, 3, 0, 4, 1, 0, 0]  # x 5 - 4, y 7 - 4, full depth, no shear
+    one = D.oriented_windows(dose.view(2, -1), shape, dirs, window, starts=np.array([10, 0]))
+    assert one.shape == (2, 7) and one[0, 0] == 40 - 26  # one window per column at that depth

@@ -75,7 +75,7 @@ def _rank_main(rank, world, port, out_dir):
                   and merged.n_beamlets == len(counts)
                   and merged.energy_emitted == float(sum(counts))
                   and mx == [float(world), 10.0] and sm == [float(world * (world + 1) // 2)]
-                  and bench.weak_scaling_value(world, 1000, 4, 2000.0) == world * 2000.0)
+                  and bench.job_value(world * 1000, 4, 2000.0) == world * 2000.0)
             with open(os.path.join(out_dir, "ok"), "w") as f:
                 f.write("1" if ok else f"0 {mx} {sm}")
     finally:

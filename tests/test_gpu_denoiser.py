@@ -342,3 +342,59 @@ def test_tensor_memory_path_rejects_what_it_does_not_cover(gpu):
                               None) == -1
     finally:
         lib.pmd_conv3d_impl(previous)
+
+
+def _oriented_reference(src, shape, win, window):
+    """numpy restatement of the oriented window map: (a, b, k) -> grid voxel."""
+    wa, wb, wd = window
+    out = np.zeros((len(win), wa, wb, wd), dtype=np.float32)
+    where = np.full((len(win), wa, wb, wd), -1, dtype=np.int64)
+    for n, (ox, oy, oz, orient, col, q1, q2) in enumerate(win):
+        d, f = orient >> 1, orient & 1
+        l1, l2 = [a for a in range(3) if a != d]
+        o = (ox, oy, oz)
+        for a in range(wa):
+            for b in range(wb):
+                for k in range(wd):
+                    s1, s2 = (k * int(q1) + 32768) >> 16, (k * int(q2) + 32768) >> 16
+                    g = [0, 0, 0]
+                    g[l1], g[l2] = o[l1] + a + s1, o[l2] + b + s2
+                    g[d] = o[d] + (wd - 1 - k if f else k)
+                    if all(0 <= g[i] < shape[i] for i in range(3)):
+                        flat = (g[0] * shape[1] + g[1]) * shape[2] + g[2]
+                        out[n, a, b, k] = src[col, flat]
+                        where[n, a, b, k] = col * int(np.prod(shape)) + flat
+    return out, where
+
+
+def test_oriented_window_gather_and_scatter(gpu):
+    """Every orientation, shears of up to one voxel per plane either way,
+    windows partly outside the grid, several windows per column: the CUDA
+    gather against the numpy map, and the scatter writes max(x, 0) * scale into
+    exactly the gathered voxels."""
+    import torch
+
+    from pyradmc_b200 import denoise_dij as D
+
+    shape, window = (9, 7, 6), (4, 3, 5)
+    rng = np.random.default_rng(7)
+    src = rng.normal(size=(3, int(np.prod(shape)))).astype(np.float32)
+    win = np.array([[ox, oy, oz, orient, col, q1, q2] for orient in range(6) for col in range(3)
+                    for ox, oy, oz in [tuple(rng.integers(-3, 8, size=3))]
+                    for q1, q2 in [tuple(rng.integers(-65536, 65537, size=2))]], dtype=np.int32)
+    ref, where = _oriented_reference(src, shape, win, window)
+    dsrc = torch.from_numpy(src).to(gpu)
+    dwin = torch.from_numpy(win).to(gpu)
+    got = D.gather_oriented(dsrc, shape, dwin, window).cpu().numpy()
+    np.testing.assert_array_equal(got, ref)
+    # scatter, one window per (orientation, column) pair at a time (windows of
+    # one column must not overlap)
+    for n in range(len(win)):
+        dst = torch.full((3, int(np.prod(shape))), -7.0, dtype=torch.float64, device=gpu)
+        data = torch.from_numpy(rng.normal(size=(1, *window)).astype(np.float32)).to(gpu)
+        scale = torch.tensor([2.5], dtype=torch.float32, device=gpu)
+        D.scatter_oriented(data, scale, shape, dwin[n:n + 1].contiguous(), dst)
+        expect = np.full(3 * int(np.prod(shape)), -7.0)
+        sel = where[n] >= 0
+        expect[where[n][sel]] = np.maximum(data.cpu().numpy()[0][sel], 0.0) * 2.5
+        np.testing.assert_allclose(dst.cpu().numpy().ravel(), expect, rtol=1e-7)
