@@ -518,16 +518,16 @@ def plan_leg(args, device, stream):
     }
 
 
-PLAN_WINDOW = (64, 64, 64)  # lateral x lateral x depth chunk of the plan's denoising windows
+PLAN_WINDOW = (64, 64, 128)  # lateral x lateral x depth chunk of the plan's denoising windows
 PLAN_GROUP = 100            # columns whose dense maps are on the device at once
 
 
 def plan_denoiser(engine, plan, held_source, ref_dose, ref_sigma, n_plain, plain_seconds, device,
                   stream):
-    """MC + denoiser on the plan.  Untimed: the held-out columns at 1/32 ..
-    1/2 of the plain 2 % count, denoised along their beamlets (windows of
-    PLAN_WINDOW oriented by each beam's direction), until the held-out error
-    reaches 2 %.  Timed (CUDA events): ``run_dij_denoised`` of the whole plan
+    """MC + denoiser on the plan.  Untimed: the held-out columns at 1/16 ..
+    3/4 of the plain 2 % count, denoised along their beamlets (windows of
+    PLAN_WINDOW oriented by each beam's direction, sheared along oblique
+    beamlets), until the held-out error reaches 2 %.  Timed (CUDA events): ``run_dij_denoised`` of the whole plan
     at that count, PLAN_GROUP columns at a time, CSC left in HBM."""
     import torch
 
@@ -540,7 +540,7 @@ def plan_denoiser(engine, plan, held_source, ref_dose, ref_sigma, n_plain, plain
     dirs = D.beam_directions(held_source)
     rho = torch.from_numpy(np.ascontiguousarray(engine.grid.density, dtype=np.float32).ravel()).to(device)
     ladder, chosen = [], None
-    for frac in (1 / 32, 1 / 16, 1 / 8, 1 / 4, 1 / 2):
+    for frac in (1 / 16, 1 / 8, 1 / 4, 1 / 2, 3 / 4):
         n = max(N_BATCHES, int(round(n_plain * frac / N_BATCHES)) * N_BATCHES)
         view = engine.run_dij_device(held_source, n, N_BATCHES, SEED, truncation=0.0)
         dose, colmax, sg = D.dense_columns(view, device, with_sigma=True)

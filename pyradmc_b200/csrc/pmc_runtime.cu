@@ -60,7 +60,9 @@ struct pmc_engine {
     int max_material = 0;
     GridInfo gi{};
     float2* d_vox = nullptr;
-    std::vector<double> default_mass;  // density * volume for the default scoring grid
+    size_t vox_cap = 0;           // bytes allocated behind d_vox (reused while large enough)
+    double voxel_volume = 0.0;    // product of the float64 spacings of the grid
+    DevBuf stage;                 // raw grid / GS arrays on their way to their packed form
 
     // scoring geometry
     GridInfo si{};
@@ -70,6 +72,7 @@ struct pmc_engine {
     float* d_cyl_r2 = nullptr;
     bool custom_scoring = false;
     double* d_mass = nullptr;
+    size_t mass_cap = 0;
     long long mass_len = 0;
 
     // tables
@@ -78,6 +81,7 @@ struct pmc_engine {
     Tables tab{};
     std::vector<void*> table_allocs;
     float4* d_gs4 = nullptr;
+    size_t gs_cap = 0;
 
     // transport buffers
     DevBuf q[4];
@@ -109,6 +113,7 @@ struct pmc_engine {
 
     pmc_counters counters{};
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    std::vector<cudaEvent_t> batch_ev;  // three per batch of a group, read once per group
     unsigned long long h2d_bytes = 0;  // cumulative over the engine's life
     unsigned long long d2h_bytes = 0;
     pmc_progress_fn progress = nullptr;
@@ -147,6 +152,56 @@ int ensure(pmc_engine* e, DevBuf& b, size_t bytes) {
     return PMC_OK;
 }
 
+// A device array behind a raw pointer, reallocated only when it must grow
+// (a re-upload of the same grid, scoring grid or GS window reuses it).
+template <typename T>
+int ensure_ptr(pmc_engine* e, T*& p, size_t& cap, size_t bytes) {
+    if (p && cap >= bytes) return PMC_OK;
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+    PMC_CUDA(e, cudaMalloc((void**)&p, std::max<size_t>(bytes, 16)));
+    cap = std::max<size_t>(bytes, 16);
+    return PMC_OK;
+}
+
+// voxel (density, material bits) and, when mass is not null, the default
+// scoring mass density * volume in float64 (the host arithmetic of the
+// scorer: one correctly rounded product).
+__global__ void pack_voxels_kernel(const float* density, const uint8_t* material, long long n,
+                                   double volume, float2* vox, double* mass) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        const float d = density[i];
+        vox[i] = make_float2(d, __int_as_float((int)material[i]));
+        if (mass) mass[i] = __dmul_rn((double)d, volume);
+    }
+}
+
+__global__ void mass_from_voxels_kernel(const float2* vox, long long n, double volume, double* mass) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x)
+        mass[i] = __dmul_rn((double)vox[i].x, volume);
+}
+
+// The four bilinear corners of every GS bin in one 16-byte row.
+__global__ void pack_gs_kernel(const float* v, int n_eta, int n_t2, int n_u, float4* g4) {
+    const long long cells = (long long)(n_eta - 1) * (n_t2 - 1) * n_u;
+    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < cells;
+         c += (long long)gridDim.x * blockDim.x) {
+        const int u = (int)(c % n_u);
+        const long long r = c / n_u;
+        const int j = (int)(r % (n_t2 - 1)), i = (int)(r / (n_t2 - 1));
+        auto at = [&](int a, int b) { return v[((long long)a * n_t2 + b) * n_u + u]; };
+        g4[c] = make_float4(at(i, j), at(i + 1, j), at(i, j + 1), at(i + 1, j + 1));
+    }
+}
+
+int grid_blocks(long long n) {
+    const long long b = (n + 255) / 256;
+    return (int)std::min<long long>(std::max<long long>(b, 1), 148LL * 16);
+}
+
 template <typename T>
 int upload_vec(pmc_engine* e, const std::vector<T>& v, const T** out) {
     void* p = nullptr;
@@ -155,6 +210,16 @@ int upload_vec(pmc_engine* e, const std::vector<T>& v, const T** out) {
     e->h2d_bytes += (unsigned long long)(v.size() * sizeof(T));
     e->run_allocs.push_back(p);
     *out = (const T*)p;
+    return PMC_OK;
+}
+
+// At least n timing events for the batches of a group (created once, reused).
+int ensure_batch_events(pmc_engine* e, size_t n) {
+    while (e->batch_ev.size() < n) {
+        cudaEvent_t ev = nullptr;
+        PMC_CUDA(e, cudaEventCreate(&ev));
+        e->batch_ev.push_back(ev);
+    }
     return PMC_OK;
 }
 
@@ -807,13 +872,15 @@ void pmc_destroy(pmc_engine* e) {
     if (e->d_cyl_r2) cudaFree(e->d_cyl_r2);
     for (DevBuf* b : {&e->q[0], &e->q[1], &e->q[2], &e->q[3], &e->edep, &e->s1, &e->s2,
                       &e->tile_counts, &e->tile_offsets, &e->col_counts, &e->out_idx,
-                      &e->out_dose, &e->out_sigma, &e->col_nhist})
+                      &e->out_dose, &e->out_sigma, &e->col_nhist, &e->dirty, &e->touched,
+                      &e->stage})
         if (b->p) cudaFree(b->p);
     for (void* p : {(void*)e->d_sched, (void*)e->d_counters, (void*)e->d_gen,
                     (void*)e->d_total_q, (void*)e->d_colmax, (void*)e->d_nnz})
         if (p) cudaFree(p);
     for (cudaEvent_t ev : e->ev)
         if (ev) cudaEventDestroy(ev);
+    for (cudaEvent_t ev : e->batch_ev) cudaEventDestroy(ev);
     if (e->own_stream) cudaStreamDestroy(e->own_stream);
     delete e;
 }
@@ -829,34 +896,37 @@ int pmc_upload_grid(pmc_engine* e, int32_t nx, int32_t ny, int32_t nz, const dou
         if (!(spacing[i] > 0.0)) return fail(e, PMC_ERR_INVALID, "non-positive spacing");
     PMC_CUDA(e, cudaSetDevice(e->device));
     const long long n = (long long)nx * ny * nz;
-    std::vector<float2> vox((size_t)n);
-    e->default_mass.resize((size_t)n);
-    const double volume = spacing[0] * spacing[1] * spacing[2];
     int max_mat = 0;
     for (long long i = 0; i < n; ++i) {
         if (!(density[i] > 0.0f)) return fail(e, PMC_ERR_INVALID, "non-positive voxel density; vacuum is not supported");
         max_mat = std::max(max_mat, (int)material[i]);
-        vox[i].x = density[i];
-        int m = material[i];
-        std::memcpy(&vox[i].y, &m, sizeof(float));
-        e->default_mass[i] = (double)density[i] * volume;
     }
-    if (e->d_vox) cudaFree(e->d_vox);
-    e->d_vox = nullptr;
-    PMC_CUDA(e, cudaMalloc(&e->d_vox, sizeof(float2) * n));
-    PMC_CUDA(e, cudaMemcpy(e->d_vox, vox.data(), sizeof(float2) * n, cudaMemcpyHostToDevice));
-    e->h2d_bytes += (unsigned long long)(sizeof(float2) * n);
+    // the raw arrays cross the bus once; the device packs voxels (and the
+    // default scoring masses) from them
+    const size_t dens_bytes = sizeof(float) * (size_t)n;
+    const size_t mat_off = (dens_bytes + 255) & ~(size_t)255;
+    int rc = ensure(e, e->stage, mat_off + (size_t)n);
+    if (!rc) rc = ensure_ptr(e, e->d_vox, e->vox_cap, sizeof(float2) * (size_t)n);
+    const bool default_mass = !e->custom_scoring;
+    if (!rc && default_mass) rc = ensure_ptr(e, e->d_mass, e->mass_cap, sizeof(double) * (size_t)n);
+    if (rc) return rc;
+    float* d_density = (float*)e->stage.p;
+    uint8_t* d_material = (uint8_t*)e->stage.p + mat_off;
+    PMC_CUDA(e, cudaMemcpyAsync(d_density, density, dens_bytes, cudaMemcpyHostToDevice, e->stream));
+    PMC_CUDA(e, cudaMemcpyAsync(d_material, material, (size_t)n, cudaMemcpyHostToDevice, e->stream));
+    e->h2d_bytes += (unsigned long long)(dens_bytes + (size_t)n);
+    const double volume = spacing[0] * spacing[1] * spacing[2];
+    e->voxel_volume = volume;
+    pack_voxels_kernel<<<grid_blocks(n), 256, 0, e->stream>>>(d_density, d_material, n, volume, e->d_vox,
+                                                               default_mass ? e->d_mass : nullptr);
+    PMC_CUDA(e, cudaGetLastError());
+    PMC_CUDA(e, cudaStreamSynchronize(e->stream));
     e->gi = make_grid(nx, ny, nz, origin, spacing);
     e->has_grid = true;
     e->max_material = max_mat;
-    if (!e->custom_scoring) {
+    if (default_mass) {
         e->score_mode = 0;
         e->si = e->gi;
-        if (e->d_mass) cudaFree(e->d_mass);
-        e->d_mass = nullptr;
-        PMC_CUDA(e, cudaMalloc(&e->d_mass, sizeof(double) * n));
-        PMC_CUDA(e, cudaMemcpy(e->d_mass, e->default_mass.data(), sizeof(double) * n, cudaMemcpyHostToDevice));
-    e->h2d_bytes += (unsigned long long)(sizeof(double) * n);
         e->mass_len = n;
     }
     return PMC_OK;
@@ -871,11 +941,12 @@ int pmc_set_scoring(pmc_engine* e, const pmc_scoring_desc* s) {
         e->score_mode = 0;
         e->si = e->gi;
         const long long n = e->gi.n_voxels;
-        if (e->d_mass) cudaFree(e->d_mass);
-        e->d_mass = nullptr;
-        PMC_CUDA(e, cudaMalloc(&e->d_mass, sizeof(double) * n));
-        PMC_CUDA(e, cudaMemcpy(e->d_mass, e->default_mass.data(), sizeof(double) * n, cudaMemcpyHostToDevice));
-    e->h2d_bytes += (unsigned long long)(sizeof(double) * n);
+        int rc = ensure_ptr(e, e->d_mass, e->mass_cap, sizeof(double) * (size_t)n);
+        if (rc) return rc;
+        mass_from_voxels_kernel<<<grid_blocks(n), 256, 0, e->stream>>>(e->d_vox, n, e->voxel_volume,
+                                                                       e->d_mass);
+        PMC_CUDA(e, cudaGetLastError());
+        PMC_CUDA(e, cudaStreamSynchronize(e->stream));
         e->mass_len = n;
         return PMC_OK;
     }
@@ -923,9 +994,8 @@ int pmc_set_scoring(pmc_engine* e, const pmc_scoring_desc* s) {
         e->si = make_grid(s->nx, s->ny, s->nz, s->origin, s->spacing);
         e->score_mode = 0;
     }
-    if (e->d_mass) cudaFree(e->d_mass);
-    e->d_mass = nullptr;
-    PMC_CUDA(e, cudaMalloc(&e->d_mass, sizeof(double) * n));
+    int rc_mass = ensure_ptr(e, e->d_mass, e->mass_cap, sizeof(double) * (size_t)n);
+    if (rc_mass) return rc_mass;
     PMC_CUDA(e, cudaMemcpy(e->d_mass, s->voxel_mass, sizeof(double) * n, cudaMemcpyHostToDevice));
     e->h2d_bytes += (unsigned long long)(sizeof(double) * n);
     e->mass_len = n;
@@ -1018,18 +1088,16 @@ int pmc_upload_gs(pmc_engine* e, const float* values, int32_t ix0, int32_t iy0, 
         return fail(e, PMC_ERR_INVALID, "invalid Goudsmit-Saunderson grid");
     PMC_CUDA(e, cudaSetDevice(e->device));
     const size_t cells = (size_t)(n_eta - 1) * (n_theta2 - 1) * n_u;
-    std::vector<float4> g4(cells);
-    auto at = [&](int i, int j, int u) { return values[((size_t)i * n_theta2 + j) * n_u + u]; };
-    for (int i = 0; i < n_eta - 1; ++i)
-        for (int j = 0; j < n_theta2 - 1; ++j)
-            for (int u = 0; u < n_u; ++u)
-                g4[((size_t)i * (n_theta2 - 1) + j) * n_u + u] =
-                    make_float4(at(i, j, u), at(i + 1, j, u), at(i, j + 1, u), at(i + 1, j + 1, u));
-    if (e->d_gs4) cudaFree(e->d_gs4);
-    e->d_gs4 = nullptr;
-    PMC_CUDA(e, cudaMalloc(&e->d_gs4, sizeof(float4) * cells));
-    PMC_CUDA(e, cudaMemcpy(e->d_gs4, g4.data(), sizeof(float4) * cells, cudaMemcpyHostToDevice));
-    e->h2d_bytes += (unsigned long long)(sizeof(float4) * cells);
+    const size_t raw = sizeof(float) * (size_t)n_eta * n_theta2 * n_u;
+    int rc = ensure(e, e->stage, raw);
+    if (!rc) rc = ensure_ptr(e, e->d_gs4, e->gs_cap, sizeof(float4) * cells);
+    if (rc) return rc;
+    PMC_CUDA(e, cudaMemcpyAsync(e->stage.p, values, raw, cudaMemcpyHostToDevice, e->stream));
+    e->h2d_bytes += (unsigned long long)raw;
+    pack_gs_kernel<<<grid_blocks((long long)cells), 256, 0, e->stream>>>((const float*)e->stage.p, n_eta,
+                                                                         n_theta2, n_u, e->d_gs4);
+    PMC_CUDA(e, cudaGetLastError());
+    PMC_CUDA(e, cudaStreamSynchronize(e->stream));
     e->tab.gs4 = e->d_gs4;
     e->tab.gs_ix0 = ix0;
     e->tab.gs_iy0 = iy0;
@@ -1316,9 +1384,13 @@ int pmc_run_dij(pmc_engine* e, const pmc_beamlet_desc* src, const int64_t* count
         PMC_CUDA(e, cudaMemcpy(e->col_nhist.p, nh.data(), sizeof(double) * gs, cudaMemcpyHostToDevice));
     e->h2d_bytes += (unsigned long long)(sizeof(double) * gs);
         rc = begin_maps(e, gs);
+        if (!rc) rc = ensure_batch_events(e, 3 * (size_t)p->n_batches);
         if (rc) return rc;
         TransportParams P = make_params(e, p, plan);
+        // every batch is enqueued back to back; its timing events are read
+        // once the group's last batch is done (no host round trip per batch)
         for (int b = 0; b < p->n_batches; ++b) {
+            cudaEvent_t* bev = e->batch_ev.data() + 3 * b;
             if (G.type == 3) {  // this batch's primaries, sampled on the host
                 for (int k = 0; k < gs; ++k) {
                     const long long r0 = (long long)b * pb[k];
@@ -1336,17 +1408,20 @@ int pmc_run_dij(pmc_engine* e, const pmc_beamlet_desc* src, const int64_t* count
                 PMC_CUDA(e, cudaMemcpyAsync((void*)G.up_weight, up_weight.data(), 4 * n, cudaMemcpyHostToDevice, e->stream));
                 e->h2d_bytes += 32ull * n;
             }
-            PMC_CUDA(e, cudaEventRecord(e->ev[0], e->stream));
+            PMC_CUDA(e, cudaEventRecord(bev[0], e->stream));
             rc = run_batch(e, p, plan, P, b, (unsigned long long)pre[gs]);
             if (rc) return rc;
-            PMC_CUDA(e, cudaEventRecord(e->ev[1], e->stream));
+            PMC_CUDA(e, cudaEventRecord(bev[1], e->stream));
             rc = launch_fold(e, n_vox, gs, (const double*)e->col_nhist.p);
             if (rc) return rc;
-            PMC_CUDA(e, cudaEventRecord(e->ev[2], e->stream));
-            PMC_CUDA(e, cudaEventSynchronize(e->ev[2]));
+            PMC_CUDA(e, cudaEventRecord(bev[2], e->stream));
+        }
+        PMC_CUDA(e, cudaEventSynchronize(e->batch_ev[3 * (size_t)p->n_batches - 1]));
+        for (int b = 0; b < p->n_batches; ++b) {
+            const cudaEvent_t* bev = e->batch_ev.data() + 3 * b;
             float a = 0, c = 0;
-            cudaEventElapsedTime(&a, e->ev[0], e->ev[1]);
-            cudaEventElapsedTime(&c, e->ev[1], e->ev[2]);
+            cudaEventElapsedTime(&a, bev[0], bev[1]);
+            cudaEventElapsedTime(&c, bev[1], bev[2]);
             t_tr += a;
             t_red += c;
         }

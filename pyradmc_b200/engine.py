@@ -460,6 +460,7 @@ class B200Engine:
     smem_tables: bool | None = None
     _natives: dict = field(default_factory=dict, init=False, repr=False, compare=False)
     _table_cache: dict = field(default_factory=dict, init=False, repr=False, compare=False)
+    _host_arrays: dict = field(default_factory=dict, init=False, repr=False, compare=False)
     _table_cache_lock: threading.Lock = field(
         default_factory=threading.Lock, init=False, repr=False, compare=False
     )
@@ -473,6 +474,29 @@ class B200Engine:
                 native = _Native(key)
                 self._natives[key] = native
         return native
+
+    def _grid_arrays(self):
+        """The transport grid as the C-ABI takes it (float32 density, uint8
+        material), converted once per grid object, like the uploads."""
+        key = ("grid", id(self.grid))
+        hit = self._host_arrays.get(key)
+        if hit is None:
+            hit = (np.ascontiguousarray(np.asarray(self.grid.density), dtype=np.float32),
+                   np.ascontiguousarray(np.asarray(self.grid.material).astype(np.uint8)))
+            self._host_arrays[key] = hit
+        return hit
+
+    def _default_mass(self):
+        """Voxel masses of the default scoring grid (density x volume, float64,
+        ScoringGrid.for_grid's arithmetic), computed once per grid object."""
+        key = ("mass", id(self.grid))
+        hit = self._host_arrays.get(key)
+        if hit is None:
+            hit = np.ascontiguousarray(
+                np.asarray(model.ScoringGrid.for_grid(self.grid).voxel_mass).reshape(-1),
+                dtype=np.float64)
+            self._host_arrays[key] = hit
+        return hit
 
     def _host_tables(self, e_max: float, pcut: float, ecut: float):
         key = (ecut, pcut, e_max)
@@ -516,8 +540,7 @@ class B200Engine:
                     f"this source declares {self.cross_sections.n_materials}"
                 )
             shape = tuple(int(n) for n in grid.shape)
-            density = np.ascontiguousarray(np.asarray(grid.density), dtype=np.float32)
-            material = np.ascontiguousarray(np.asarray(grid.material).astype(np.uint8))
+            density, material = self._grid_arrays()
             origin = np.asarray(grid.origin, dtype=np.float64)
             spacing = np.asarray(grid.spacing, dtype=np.float64)
             native.check(lib.pmc_upload_grid(
@@ -563,10 +586,11 @@ class B200Engine:
                 native.gs_key = gkey2
         skey = id(scoring) if scoring is not None else ("default", gkey)
         if native.scoring_key != skey:
-            if scoring is None:
-                scoring = model.ScoringGrid.for_grid(grid)
-            mass = np.ascontiguousarray(np.asarray(scoring.voxel_mass).reshape(-1), dtype=np.float64)
-            if _type_name(scoring) == "CylindricalScoringGrid":  # scoring/cylinder.py:172
+            if scoring is None:  # the transport grid itself (ScoringGrid.for_grid)
+                mass = self._default_mass()
+            else:
+                mass = np.ascontiguousarray(np.asarray(scoring.voxel_mass).reshape(-1), dtype=np.float64)
+            if scoring is not None and _type_name(scoring) == "CylindricalScoringGrid":  # scoring/cylinder.py:172
                 depth = np.ascontiguousarray(scoring.depth_edges, dtype=np.float64)
                 radial = np.ascontiguousarray(scoring.radial_edges, dtype=np.float64)
                 native._keep = [mass, depth, radial]
@@ -575,10 +599,11 @@ class B200Engine:
                 sdesc.depth_edges = _lib.ptr(depth, C.c_double)
                 sdesc.radial_edges = _lib.ptr(radial, C.c_double)
             else:
-                sdesc = _lib.ScoringDesc(nx=int(scoring.shape[0]), ny=int(scoring.shape[1]),
-                                         nz=int(scoring.shape[2]))
-                sdesc.origin[:] = [float(v) for v in scoring.origin]
-                sdesc.spacing[:] = [float(v) for v in scoring.spacing]
+                box = grid if scoring is None else scoring
+                sdesc = _lib.ScoringDesc(nx=int(box.shape[0]), ny=int(box.shape[1]),
+                                         nz=int(box.shape[2]))
+                sdesc.origin[:] = [float(v) for v in box.origin]
+                sdesc.spacing[:] = [float(v) for v in box.spacing]
             sdesc.voxel_mass = _lib.ptr(mass, C.c_double)
             native.check(lib.pmc_set_scoring(native.handle, C.byref(sdesc)))
             native.scoring_key = skey
