@@ -1441,9 +1441,19 @@ int pmc_run_dij(pmc_engine* e, const pmc_beamlet_desc* src, const int64_t* count
         PMC_CUDA(e, cudaEventRecord(e->ev[1], e->stream));
         rc = truncate_count(e, n_vox, gs, p->truncation, &g_nnz, &g_counts);
         if (rc) return rc;
-        rc = grow_keep(e, e->out_idx, sizeof(long long) * (e->csc_nnz + g_nnz), sizeof(long long) * e->csc_nnz);
-        if (!rc) rc = grow_keep(e, e->out_dose, sizeof(double) * (e->csc_nnz + g_nnz), sizeof(double) * e->csc_nnz);
-        if (!rc) rc = grow_keep(e, e->out_sigma, sizeof(double) * (e->csc_nnz + g_nnz), sizeof(double) * e->csc_nnz);
+        // room for this group's entries; after the first of several groups,
+        // for all of them at its density plus a quarter (a few large grows
+        // instead of one per group: each grow is an allocation and a copy)
+        unsigned long long want = e->csc_nnz + g_nnz;
+        if (g0 == 0 && n_beam > gs) {
+            const unsigned long long est = (unsigned long long)((double)g_nnz * (double)n_beam / gs * 1.25);
+            size_t free_b = 0, total_b = 0;
+            if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess && est * 24ull < free_b / 2)
+                want = std::max(want, est);  // 24 bytes per entry: index, mean, sigma
+        }
+        rc = grow_keep(e, e->out_idx, sizeof(long long) * want, sizeof(long long) * e->csc_nnz);
+        if (!rc) rc = grow_keep(e, e->out_dose, sizeof(double) * want, sizeof(double) * e->csc_nnz);
+        if (!rc) rc = grow_keep(e, e->out_sigma, sizeof(double) * want, sizeof(double) * e->csc_nnz);
         if (rc) return rc;
         PMC_CUDA(e, cudaEventRecord(e->ev[2], e->stream));
         rc = truncate_compact(e, n_vox, gs, p->truncation, g_nnz, g_counts);

@@ -445,8 +445,8 @@ def compact(mean, sigma, truncation: float, to_host: bool = True):
     k = nnz.value
     indptr = np.zeros(n_cols + 1, dtype=np.int64)
     np.cumsum(counts.cpu().numpy(), out=indptr[1:])
-    if not to_host:
-        return indptr, idx[:k], dose[:k], sig[:k]
+    if not to_host:  # copies, so the capacity-sized buffers are freed
+        return indptr, idx[:k].clone(), dose[:k].clone(), sig[:k].clone()
     return indptr, idx[:k].cpu().numpy(), dose[:k].cpu().numpy(), sig[:k].cpu().numpy()
 
 

@@ -461,6 +461,7 @@ class B200Engine:
     _natives: dict = field(default_factory=dict, init=False, repr=False, compare=False)
     _table_cache: dict = field(default_factory=dict, init=False, repr=False, compare=False)
     _host_arrays: dict = field(default_factory=dict, init=False, repr=False, compare=False)
+    _streams: dict = field(default_factory=dict, init=False, repr=False, compare=False)
     _table_cache_lock: threading.Lock = field(
         default_factory=threading.Lock, init=False, repr=False, compare=False
     )
@@ -472,6 +473,9 @@ class B200Engine:
             native = self._natives.get(key)
             if native is None:
                 native = _Native(key)
+                stream = self._streams.get(key)
+                if stream:
+                    native.check(native.lib.pmc_set_stream(native.handle, C.c_void_p(stream)))
                 self._natives[key] = native
         return native
 
@@ -657,8 +661,21 @@ class B200Engine:
         as an int, e.g. ``torch.cuda.current_stream().cuda_stream``); None
         restores the engine's own stream."""
         native = self._native(device)
+        self._streams[device or self.device] = stream or 0
         with native.lock:
             native.check(native.lib.pmc_set_stream(native.handle, C.c_void_p(stream or 0)))
+
+    def release_device_memory(self, device: str | None = None) -> None:
+        """Free every device buffer of this engine on ``device`` (all devices
+        when None): maps, queues, tables, the last Dij's CSC (a ``DeviceDij``
+        of it is no longer valid).  The next call allocates and uploads again,
+        on the stream set by :meth:`use_stream`."""
+        with self._table_cache_lock:
+            keys = [k for k in self._natives if device is None or k == device]
+            natives = [self._natives.pop(k) for k in keys]
+        for native in natives:
+            with native.lock:
+                native.__del__()
 
     def drop_uploads(self, device: str | None = None) -> None:
         """Forget what is resident, so the next call uploads grid, tables, GS

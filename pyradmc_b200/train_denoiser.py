@@ -11,8 +11,11 @@ along +z as in the benchmark Dij, the rest come from a random gantry angle in
 the x-y plane as in a coplanar plan, with beamlet widths of 3-10 mm and focal
 distances of 80-120 cm; ``--geometry axial`` keeps the benchmark's 5 mm fan at
 100 cm on 2.5 mm phantoms; ``--geometry coplanar`` draws gantry beams only
-(mostly 3 mm voxels and 5 mm beamlets, focal distances 90-110 cm), the
-training set of the network a coplanar plan uses.  The U-Net then trains with Adam on the device (the
+(mostly 3 mm voxels and 5 mm beamlets, focal distances 90-110 cm);
+``--geometry plan`` uses the coplanar plan's own phantom family (256x256x128 at
+3 mm, ellipsoids scaled with the box) with one 10x10 gantry beam of 5 mm
+beamlets at SAD 100 from a random angle each, the training set of the network
+the plan uses.  The U-Net then trains with Adam on the device (the
 project's own forward and backward kernels) and is evaluated on held-out
 phantoms against high-statistics Monte Carlo.  One JSON line with the loss
 curve and the evaluation goes to stdout.
@@ -50,6 +53,10 @@ def training_case(i: int, geometry: str = "mixed"):
     if geometry == "axial":
         return phantom(TRAIN_SEED0 + i)
     rng = np.random.default_rng(TRAIN_SEED0 + 7 * i)
+    if geometry == "plan":  # the coplanar plan's phantom family and beamlets, one gantry beam
+        grid = plan_phantom(TRAIN_SEED0 + i)
+        xs = AnalyticWaterTables(geometry_densities=grid.max_density_by_material())
+        return grid, xs, gantry_beam(grid, float(rng.uniform(0.0, 360.0)))
     if geometry == "coplanar":  # gantry beams as in a coplanar plan, mostly 5 mm at 3 mm voxels
         spacing = 0.3 if i % 4 else 0.25
         grid = ellipsoid_phantom(seed=TRAIN_SEED0 + i, spacing=(spacing,) * 3)
@@ -66,6 +73,15 @@ def training_case(i: int, geometry: str = "mixed"):
         return grid, xs, beamlet_fan(grid, pitch=width, width=width, sad=sad)
     return grid, xs, gantry_beam(grid, float(rng.uniform(0.0, 360.0)), pitch=width, width=width,
                                  sad=sad)
+
+
+def plan_phantom(seed: int, shape=(256, 256, 128), spacing: float = 0.3):
+    """The coplanar plan's phantom family: water plus seeded ellipsoids of
+    density U(0.2, 1.9), semi-axes scaled with the box from the 128^3 at 2.5 mm
+    case's 1-4 cm."""
+    scale = shape[0] * spacing / (128 * 0.25)
+    return ellipsoid_phantom(shape=shape, spacing=(spacing,) * 3, seed=seed,
+                             semi_axis_range=(1.0 * scale, 4.0 * scale))
 
 
 def held_out_oblique():
@@ -167,9 +183,10 @@ def main(argv=None) -> int:
     ap.add_argument("--eval-levels", default="10000,30000,100000,300000")
     ap.add_argument("--n-ref", type=int, default=4_000_000)
     ap.add_argument("--eval-lateral", default="64")
-    ap.add_argument("--geometry", choices=("mixed", "axial", "coplanar"), default="mixed",
+    ap.add_argument("--geometry", choices=("mixed", "axial", "coplanar", "plan"), default="mixed",
                     help="training beams: mixed gantry angles, widths and focal distances; the "
-                         "benchmark's axial 5 mm fan; or coplanar gantry beams as in a plan")
+                         "benchmark's axial 5 mm fan; coplanar gantry beams as in a plan; or the "
+                         "plan's own 256x256x128 phantom family with one gantry beam each")
     args = ap.parse_args(argv)
 
     def log(msg):

@@ -210,6 +210,27 @@ def test_beamlet_group_size_is_bit_inert(gpu, group):
     assert a.energy_deposited == b.energy_deposited and a.energy_escaped == b.energy_escaped
 
 
+def test_released_device_memory_is_rebuilt_bit_for_bit(gpu):
+    """release_device_memory frees the engine's buffers; the next call uploads
+    and allocates again (on the stream the caller set) and gives the same Dij,
+    also when the second upload reuses the freed sizes."""
+    import torch
+
+    engine, src, run = _engine("dij_lattice")
+    run["truncation"] = 1e-3
+    stream = torch.cuda.Stream(device=gpu)
+    engine.use_stream(stream.cuda_stream)
+    a = engine.run_dij(src, **run)
+    engine.release_device_memory()
+    b = engine.run_dij(src, **run)
+    engine.drop_uploads()  # same sizes again: the buffers are reused, not reallocated
+    c = engine.run_dij(src, **run)
+    for f in ("indptr", "indices", "dose", "sigma"):
+        np.testing.assert_array_equal(getattr(a, f), getattr(b, f))
+        np.testing.assert_array_equal(getattr(a, f), getattr(c, f))
+    assert engine._streams[engine.device] == stream.cuda_stream  # re-applied to the new engine
+
+
 def test_uneven_counts_reproduce_equal_count_columns(gpu):
     """Correlated keys are the within-beamlet index r, so a column depends only
     on its own count: uneven counts give, column by column, the equal-count Dij."""
