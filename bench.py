@@ -521,6 +521,65 @@ def plan_leg(args, device, stream):
     }
 
 
+# ---- parity of the benchmark's phantom family ---------------------------------------
+def batched_chi2(a, sa, n_a, b, sb, n_b):
+    """chi2 over voxels of two batch means with batch-estimated sigmas, and its
+    null (each voxel's z^2 is F(1, nu), nu by Welch-Satterthwaite: E = nu/(nu-2),
+    Var = 2 nu^2 (nu-1) / ((nu-2)^2 (nu-4))); the one-sided normal p-value."""
+    from math import erfc, sqrt
+
+    va, vb = sa**2, sb**2
+    nu = (va + vb) ** 2 / (va**2 / (n_a - 1) + vb**2 / (n_b - 1))
+    chi2 = float(np.sum((a - b) ** 2 / (va + vb)))
+    mean = float(np.sum(nu / (nu - 2.0)))
+    var = float(np.sum(2.0 * nu**2 * (nu - 1.0) / ((nu - 2.0) ** 2 * (nu - 4.0))))
+    z = (chi2 - mean) / sqrt(var)
+    return chi2, mean, 0.5 * erfc(z / sqrt(2.0))
+
+
+def parity_block(device):
+    """The benchmark Dij's phantom family at reduced size against pyRadMC's
+    ReferenceEngine (the committed fixtures tests/golden/ref_ct_beamlets_*.npz,
+    made by tests/golden/make_golden.py): a 40^3 CT-like phantom at 2.5 mm, a
+    2x2 fan of 5 mm 6 MV beamlets, uneven per-column counts; batched chi-squared
+    per column on the voxels >= 10 % and >= 1 % of the column maximum.  Also
+    quotes the test session's chi-squared report when it was written on this
+    host ($PMC_PARITY_REPORT or .parity/chi2.json)."""
+    from pyradmc_b200 import B200Engine, phantoms
+    from pyradmc_b200.model import AnalyticWaterTables
+
+    golden = ROOT / "tests" / "golden"
+    grid = phantoms.ellipsoid_phantom(shape=(40, 40, 40), spacing=(0.25, 0.25, 0.25), seed=20260805)
+    src = phantoms.beamlet_fan(grid, n_x=2, n_y=2, pitch=0.5, width=0.5, sad=100.0)
+    xs = AnalyticWaterTables(geometry_densities=grid.max_density_by_material())
+    counts = [40_000, 120_000, 40_000, 120_000]
+    dij = B200Engine(grid, xs, device=device).run_dij(
+        src, n_histories_per_beamlet=[4 * c for c in counts], n_batches=10, seed=SEED + 1,
+        truncation=0.0)
+    records = []
+    for j, c in enumerate(counts):
+        with np.load(golden / f"ref_ct_beamlets_{c}.npz") as z:
+            a, sa, n_a = z["dose"][j], z["dose_sigma"][j], int(z["n_batches"])
+        b, sb = dij.column_dense(j).reshape(-1), dij.sigma_dense(j).reshape(-1)
+        for fraction in (0.1, 0.01):
+            m = (a > fraction * a.max()) & (sa > 0) & (sb > 0)
+            chi2, mean, p = batched_chi2(a[m], sa[m], n_a, b[m], sb[m], dij.n_batches)
+            records.append({"case": f"ct_beamlets column {j} ({c} histories, >= {fraction:g} of max)",
+                            "chi2_per_dof": chi2 / m.sum(), "null_mean_per_dof": mean / m.sum(),
+                            "p": p, "n_voxels": int(m.sum()), "passed": p > 0.01})
+    out = {"reference": "pyRadMC ReferenceEngine fixtures (tests/golden/ref_ct_beamlets_*.npz)",
+           "records": records, "passed": sum(r["passed"] for r in records),
+           "total": len(records)}
+    report = Path(os.environ.get("PMC_PARITY_REPORT", str(ROOT / ".parity" / "chi2.json")))
+    if report.exists():
+        tests = json.loads(report.read_text())
+        tests = tests.get("records", tests) if isinstance(tests, dict) else tests
+        out["test_session"] = {"file": str(report), "cases": len(tests),
+                               "passed": sum(1 for r in tests if r.get("passed")),
+                               "min_p": min((r["p"] for r in tests), default=None)}
+    return out
+
+
 PLAN_WINDOW = (64, 64, 128)  # lateral x lateral x depth chunk of the plan's denoising windows
 PLAN_GROUP = 100            # columns whose dense maps are on the device at once
 
@@ -803,6 +862,7 @@ def b200_arm(args, world, rank, local):
     # the method comparisons are one-GPU workloads: rank 0 of a one-rank run
     den = None if args.no_denoiser or world > 1 else denoiser_leg(
         args, engine, source, counts, stream, device, total_ms / args.steps / 1e3)
+    parity = parity_block(device) if world == 1 else None
     plan = None
     if not args.no_plan and world == 1:
         engine.drop_uploads()
@@ -848,6 +908,7 @@ def b200_arm(args, world, rank, local):
         "plain_2pct": "extrapolated: measured s per Dij x (per-beamlet sigma / 2 %)^2 (1/sqrt(N) scaling)",
         "denoiser": den,
         "plan": plan,
+        "parity": parity,
         "e2e": {"value": e2e_value, "unit": "histories/s",
                 "h2d_bytes_per_step": int(np.median(h2d)), "d2h_bytes_per_step": int(np.median(d2h)),
                 "ms_per_step": e2e_total / args.steps},
