@@ -338,8 +338,8 @@ def denoiser_leg(args, engine, source, counts, stream, device, plain_s_per_dij):
         return {"reached_2pct": False, "ladder": ladder,
                 "reference_histories_per_beamlet": REF_HISTORIES}
 
-    def timed(c):
-        kw = dict(n_histories_per_beamlet=c, n_batches=N_BATCHES, seed=SEED)
+    def timed(c, **extra):
+        kw = dict(n_histories_per_beamlet=c, n_batches=N_BATCHES, seed=SEED, **extra)
         for _ in range(max(1, args.warmup)):
             D.run_dij_denoised(engine, net, source, truncation=1e-3, to_host=False, **kw)
         times, launches0 = [], net.launches
@@ -357,7 +357,11 @@ def denoiser_leg(args, engine, source, counts, stream, device, plain_s_per_dij):
 
     regions = {}
     for t, (g, c) in chosen.items():
-        s_den, unet_launches, dij = timed(c)
+        # one group, and DEN_GROUP-column groups whose denoising overlaps the next
+        # group's transport (the same Dij bit for bit); the faster is the method's time
+        s_seq, unet_launches, dij = timed(c)
+        s_pipe, _, _ = timed(c, group_columns=DEN_GROUP, overlap=True)
+        s_den = min(s_seq, s_pipe)
         plain_err = plain_at_counts[t]["sigma_eq"]
         plain_s = plain_s_per_dij * (plain_err / 0.02) ** 2
         rung = next(r for r in ladder if r["scale"] == g)
@@ -365,7 +369,9 @@ def denoiser_leg(args, engine, source, counts, stream, device, plain_s_per_dij):
                       "s_per_dij_at_2pct": s_den, "plain_sigma_eq_at_benchmark_counts": plain_err,
                       "plain_s_per_dij_at_2pct": plain_s, "speedup_vs_plain": plain_s / s_den,
                       "denoised": rung["denoised"], "plain_same_histories": rung["plain"],
-                      "unet_launches_per_dij": unet_launches, "nnz": int(dij.indptr[-1])}
+                      "unet_launches_per_dij": unet_launches, "nnz": int(dij.indptr[-1]),
+                      "s_one_group": s_seq, "s_pipelined": s_pipe,
+                      "pipelined_group_columns": DEN_GROUP}
     head = regions["0.5"]
     g, c = chosen["0.5"]
     stages: dict = {}
@@ -580,6 +586,7 @@ def parity_block(device):
     return out
 
 
+DEN_GROUP = 25  # columns per group when MC and denoising overlap across groups
 PLAN_WINDOW = (64, 64, 128)  # lateral x lateral x depth chunk of the plan's denoising windows
 PLAN_GROUP = 100            # columns whose dense maps are on the device at once
 
@@ -635,7 +642,7 @@ def plan_denoiser(engine, plan, held_source, ref_dose, ref_sigma, n_plain, plain
     e0.record(stream)
     dij = D.run_dij_denoised(engine, net, plan, chosen, N_BATCHES, SEED, truncation=1e-3,
                              lateral=PLAN_WINDOW[0], depth=PLAN_WINDOW[2], to_host=False,
-                             group_columns=PLAN_GROUP, timings=stages)
+                             group_columns=PLAN_GROUP, overlap=True, timings=stages)
     e1.record(stream)
     e1.synchronize()
     seconds = e0.elapsed_time(e1) / 1e3

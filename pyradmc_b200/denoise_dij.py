@@ -453,7 +453,8 @@ def compact(mean, sigma, truncation: float, to_host: bool = True):
 def run_dij_denoised(engine, net: UNet3D | None, source, n_histories_per_beamlet, n_batches: int,
                      seed: int, *, truncation: float = 1.0e-3, lateral: int = 64,
                      depth: int | None = None, chunk: int = 32, to_host: bool = True,
-                     timings: dict | None = None, group_columns: int | None = None):
+                     timings: dict | None = None, group_columns: int | None = None,
+                     overlap: bool = False):
     """A Dij from low-history Monte Carlo plus the denoiser: the engine runs the
     beamlets (``run_dij_device``), the windows along every column's beamlet
     (``lateral`` voxels across, ``depth`` planes per chunk; see
@@ -461,9 +462,12 @@ def run_dij_denoised(engine, net: UNet3D | None, source, n_histories_per_beamlet
     dense columns are truncated and compacted to CSC on the device.  Columns
     go through in groups of ``group_columns`` (all at once when None: the dense
     maps of a group must fit the device), each group with the same history
-    keys as in the whole Dij.  With ``to_host`` False the CSC entries stay on
-    the device (torch tensors in the result).  With ``net`` None this is plain
-    Monte Carlo (``engine.run_dij``), the method's fallback.
+    keys as in the whole Dij.  With ``overlap`` a group's denoising and
+    compaction run on a second stream while the engine transports the next
+    group (the engine's kernels are latency-bound, the U-Net's tensor-bound);
+    ``timings`` then holds the whole call only.  With ``to_host`` False the
+    CSC entries stay on the device (torch tensors in the result).  With ``net``
+    None this is plain Monte Carlo (``engine.run_dij``), the method's fallback.
 
     The per-entry ``sigma`` of the result is the batch sigma of the
     low-history Monte Carlo input, not an uncertainty of the denoised value:
@@ -494,6 +498,15 @@ def run_dij_denoised(engine, net: UNet3D | None, source, n_histories_per_beamlet
 
     pieces, books, shape = [], np.zeros(4, dtype=np.int64), None
     rho = None
+    pipelined = overlap and group < n_cols
+    main = torch.cuda.current_stream()
+    side = torch.cuda.Stream(device=main.device) if pipelined else None
+    pending = None  # the previous group's dense mean and sigma, denoised on `side`
+
+    def finish(item):
+        with torch.cuda.stream(side):
+            pieces.append(compact(item[0], item[1], truncation, to_host=False))
+
     mark("start")
     for lo in range(0, n_cols, group):
         hi = min(lo + group, n_cols)
@@ -501,22 +514,47 @@ def run_dij_denoised(engine, net: UNet3D | None, source, n_histories_per_beamlet
                                      columns=(lo, hi))
         device = torch.device(view.device)
         shape = tuple(view.grid_shape)
-        mark("monte_carlo")
+        if not pipelined:
+            mark("monte_carlo")
         dose, colmax, sigma32 = dense_columns(view, device, with_sigma=True)
         mean, sigma = dense_columns_f64(view, device)
         books += np.asarray(view.books, dtype=np.int64)
         if rho is None:
             rho = torch.from_numpy(np.ascontiguousarray(engine.grid.density, dtype=np.float32)
                                    .ravel()).to(device)
+        window = inference_window(shape, lateral, depth)
+        if pipelined:
+            ready = torch.cuda.Event()
+            ready.record(main)
+            ready.synchronize()  # the engine's next run overwrites the CSC these were read from
+            if pending is not None:
+                finish(pending)
+            side.wait_event(ready)
+            for t in (dose, colmax, sigma32, mean, sigma, rho):
+                t.record_stream(side)
+            with torch.cuda.stream(side):
+                denoise_dense(net, dose, colmax, rho, shape, sigma=sigma32, window=window,
+                              chunk=chunk, out=mean, directions=directions[lo:hi],
+                              spacing=engine.grid.spacing)
+            pending = (mean, sigma)
+            del dose, sigma32, mean, sigma
+            continue
         mark("dense_columns")
-        denoise_dense(net, dose, colmax, rho, shape, sigma=sigma32,
-                      window=inference_window(shape, lateral, depth), chunk=chunk, out=mean,
-                      directions=directions[lo:hi], spacing=engine.grid.spacing)
+        denoise_dense(net, dose, colmax, rho, shape, sigma=sigma32, window=window, chunk=chunk,
+                      out=mean, directions=directions[lo:hi], spacing=engine.grid.spacing)
         del dose, sigma32
         mark("unet")
         pieces.append(compact(mean, sigma, truncation, to_host=False))
         del mean, sigma
         mark("compaction")
+    if pipelined:
+        finish(pending)
+        pending = None
+        main.wait_stream(side)
+        for piece in pieces:
+            for t in piece[1:]:
+                t.record_stream(main)
+        mark("pipelined")
     if timings is not None:
         marks[-1][1].synchronize()
         for (_, a), (name, b) in zip(marks, marks[1:]):

@@ -99,3 +99,25 @@ def test_denoiser_gains_on_an_oblique_beam_outside_the_training_set(gpu):
     plain, den = _gain(gpu, grid, fan, 30_000, window=(64, 64, 64), weights=COPLANAR_WEIGHTS)
     assert den["0.5"]["sigma_eq"] < 0.7 * plain["0.5"]["sigma_eq"], (plain, den)
     assert abs(den["0.5"]["bias_integral"]) < 0.02, den
+
+
+def test_pipelined_groups_give_the_same_dij(gpu):
+    """run_dij_denoised with the denoising of one column group overlapping the
+    transport of the next (a second stream) equals the one-group call bit for
+    bit: every column keeps its history keys and every kernel is deterministic."""
+    from pyradmc_b200 import B200Engine, denoise_dij as D, phantoms
+    from pyradmc_b200.denoiser import UNet3D
+    from pyradmc_b200.model import AnalyticWaterTables
+
+    grid = phantoms.ellipsoid_phantom(shape=(64, 64, 64), seed=4244)
+    xs = AnalyticWaterTables(geometry_densities=grid.max_density_by_material())
+    fan = phantoms.beamlet_fan(grid, n_x=3, n_y=2)
+    engine = B200Engine(grid, xs, device=gpu)
+    net = UNet3D.load(D.__file__.replace("denoise_dij.py", WEIGHTS), device=gpu)
+    kw = dict(truncation=1e-3, lateral=32)
+    one = D.run_dij_denoised(engine, net, fan, 20_000, 10, 3, **kw)
+    two = D.run_dij_denoised(engine, net, fan, 20_000, 10, 3, group_columns=2, overlap=True, **kw)
+    for f in ("indptr", "indices", "dose", "sigma"):
+        np.testing.assert_array_equal(getattr(one, f), getattr(two, f))
+    assert one.energy_deposited == two.energy_deposited
+    assert net.lib.pmd_conv3d_failures() == 0
