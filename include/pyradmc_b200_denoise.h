@@ -38,6 +38,16 @@ extern "C" {
 int pmd_conv3d(const void* x, const void* w, const float* bias, void* y, int n, int d, int h,
                int w_, int cin, int cout, int kpad, int relu, void* stream);
 
+/* pmd_conv3d followed by the 1x1x1 head, fused in the warp-specialized
+ * kernel's epilogue: out[m] = head_b[0] + base[m] + sum_c head_w[c] *
+ * y[m][c] (float32; base may be NULL), y the bf16 convolution output, which
+ * is not stored.  The same values as pmd_conv3d then pmd_head.  -1 (nothing
+ * launched) where the warp-specialized kernel does not cover the shape or
+ * another kernel is selected; the caller then runs the two steps. */
+int pmd_conv3d_head(const void* x, const void* w, const float* bias, const float* head_w,
+                    const float* head_b, const float* base, float* out, int n, int d, int h,
+                    int w_, int cin, int cout, int kpad, int relu, void* stream);
+
 /* Selects the convolution kernels of pmd_conv3d: 0 (default) the warp-specialized
  * kernel below wherever it applies except cin = 8, then the single-buffered
  * tensor-memory kernel (tcgen05.mma, accumulators in TMEM; cout a multiple of 16 up to 192,

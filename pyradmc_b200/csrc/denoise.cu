@@ -1061,7 +1061,8 @@ bool ws_tensor_maps(const __nv_bfloat16* x, const __nv_bfloat16* w, const WsConv
 
 template <int CG>
 int launch_ws(const CUtensorMap& xm, const CUtensorMap& wm, const __nv_bfloat16* w, const float* bias,
-              __nv_bfloat16* y, const WsConv& p, int smem, int per_sm, int relu, cudaStream_t st) {
+              __nv_bfloat16* y, const WsConv& p, int smem, int per_sm, int relu, cudaStream_t st,
+              const WsHead& head) {
     int dev = 0, sms = 0;
     if (cudaGetDevice(&dev) != cudaSuccess ||
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
@@ -1069,25 +1070,25 @@ int launch_ws(const CUtensorMap& xm, const CUtensorMap& wm, const __nv_bfloat16*
             cudaSuccess)
         return -2;
     const int grid = p.n_tiles < sms * per_sm ? p.n_tiles : sms * per_sm;
-    conv3d_ws_kernel<CG><<<grid, kWsThreads, smem, st>>>(xm, wm, w, bias, y, p, relu);
+    conv3d_ws_kernel<CG><<<grid, kWsThreads, smem, st>>>(xm, wm, w, bias, y, p, relu, head);
     return launched();
 }
 
 // 1 launched (code: 0, or -2 from launched()), -1 when the plan or the tensor
 // maps do not cover the call.
 int try_ws(const __nv_bfloat16* x, const __nv_bfloat16* w, const float* bias, __nv_bfloat16* y,
-           const ConvShape& s, int relu, cudaStream_t st, int& code) {
+           const ConvShape& s, int relu, cudaStream_t st, int& code, const WsHead& head = WsHead{}) {
     WsConv p{};
     int smem = 0, per_sm = 0;
     CUtensorMap xm, wm;
     if (!ws_plan(s, p, smem, per_sm) || !ws_tensor_maps(x, w, p, xm, wm)) return -1;
     switch (p.cg) {
-        case 1: code = launch_ws<1>(xm, wm, w, bias, y, p, smem, per_sm, relu, st); return 1;
-        case 2: code = launch_ws<2>(xm, wm, w, bias, y, p, smem, per_sm, relu, st); return 1;
-        case 4: code = launch_ws<4>(xm, wm, w, bias, y, p, smem, per_sm, relu, st); return 1;
-        case 6: code = launch_ws<6>(xm, wm, w, bias, y, p, smem, per_sm, relu, st); return 1;
-        case 8: code = launch_ws<8>(xm, wm, w, bias, y, p, smem, per_sm, relu, st); return 1;
-        case 12: code = launch_ws<12>(xm, wm, w, bias, y, p, smem, per_sm, relu, st); return 1;
+        case 1: code = launch_ws<1>(xm, wm, w, bias, y, p, smem, per_sm, relu, st, head); return 1;
+        case 2: code = launch_ws<2>(xm, wm, w, bias, y, p, smem, per_sm, relu, st, head); return 1;
+        case 4: code = launch_ws<4>(xm, wm, w, bias, y, p, smem, per_sm, relu, st, head); return 1;
+        case 6: code = launch_ws<6>(xm, wm, w, bias, y, p, smem, per_sm, relu, st, head); return 1;
+        case 8: code = launch_ws<8>(xm, wm, w, bias, y, p, smem, per_sm, relu, st, head); return 1;
+        case 12: code = launch_ws<12>(xm, wm, w, bias, y, p, smem, per_sm, relu, st, head); return 1;
         default: return -1;
     }
 }
@@ -1173,6 +1174,26 @@ int pmd_conv3d(const void* x, const void* w, const float* bias, void* y, int n, 
         default: return -1;
     }
     return launched();
+}
+
+int pmd_conv3d_head(const void* x, const void* w, const float* bias, const float* head_w,
+                    const float* head_b, const float* base, float* out, int n, int d, int h, int wd,
+                    int cin, int cout, int kpad, int relu, void* stream) {
+    ConvShape s{n, d, h, wd, cin, cout, kpad};
+    if (n < 1 || d < 1 || h < 1 || wd < 1 || cin < 8 || cin % 8 || kpad % 64 || kpad < 27 * cin ||
+        !head_w || !head_b || !out)
+        return -1;
+    if (g_conv_impl != 0 && g_conv_impl != 4) return -1;
+    WsHead head;
+    head.w = head_w;
+    head.b = head_b;
+    head.base = base;
+    head.out = out;
+    int code = 0;
+    if (try_ws((const __nv_bfloat16*)x, (const __nv_bfloat16*)w, bias, nullptr, s, relu,
+               (cudaStream_t)stream, code, head) == 1)
+        return code;
+    return -1;
 }
 
 int pmd_conv3d_plan(int n, int d, int h, int wd, int cin, int cout, int* info) {

@@ -55,6 +55,15 @@ struct WsConv {
     int ystride;             // channels per voxel of the output tensor
 };
 
+// An optional 1x1x1 head fused into the epilogue: out[m] = b + base[m] +
+// sum_c w[c] * y[m][c] over the bf16 outputs, which are then not stored.
+struct WsHead {
+    const float* w = nullptr;     // [cout]; null: no head, y is written
+    const float* b = nullptr;     // [1]
+    const float* base = nullptr;  // [voxels] or null
+    float* out = nullptr;         // [voxels]
+};
+
 __device__ __forceinline__ void mbar_arrive_expect_tx(uint32_t mbar, uint32_t bytes) {
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mbar), "r"(bytes)
                  : "memory");
@@ -121,7 +130,7 @@ template <int CG>
 __global__ void __launch_bounds__(kWsThreads, 1)
 conv3d_ws_kernel(const __grid_constant__ CUtensorMap xmap, const __grid_constant__ CUtensorMap wmap,
                  const __nv_bfloat16* __restrict__ wt, const float* __restrict__ bias,
-                 __nv_bfloat16* __restrict__ y, WsConv p, int relu) {
+                 __nv_bfloat16* __restrict__ y, WsConv p, int relu, WsHead head) {
     extern __shared__ __align__(1024) unsigned char smem[];
     const ConvShape& s = p.s;
     const int N = s.cout;
@@ -262,8 +271,13 @@ conv3d_ws_kernel(const __grid_constant__ CUtensorMap xmap, const __grid_constant
             for (int sl = 0; sl < p.tz; ++sl) {
                 const int z = z0 + sl;
                 const bool in = z < s.d && yg < s.h && xg < s.w;
-                __nv_bfloat16* out = y + ((((long long)nb * s.d + (in ? z : 0)) * s.h + (in ? yg : 0)) * s.w +
-                                          (in ? xg : 0)) * p.ystride;
+                const long long m = (((long long)nb * s.d + (in ? z : 0)) * s.h + (in ? yg : 0)) * s.w +
+                                    (in ? xg : 0);
+                __nv_bfloat16* out = y + m * p.ystride;
+                // the fused head: bias + base + its weights over the stored bf16
+                // channel values, in channel order (pmd_head's arithmetic)
+                float hacc = 0.0f;
+                if (head.w && in) hacc = __ldg(head.b) + (head.base ? head.base[m] : 0.0f);
                 for (int c = 0; c < N / 16; ++c) {
                     float v[16];
                     tmem_ld16(tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)a * p.acc_cols +
@@ -286,11 +300,20 @@ conv3d_ws_kernel(const __grid_constant__ CUtensorMap xmap, const __grid_constant
                             }
                             pk.h[e] = __floats2bfloat162_rn(lo, hi);
                         }
-                        uint4* o = reinterpret_cast<uint4*>(out + c * 16);
-                        o[0] = pk.u4[0];
-                        o[1] = pk.u4[1];
+                        if (head.w) {
+#pragma unroll
+                            for (int e = 0; e < 8; ++e) {
+                                hacc += __ldg(head.w + c * 16 + 2 * e) * __low2float(pk.h[e]);
+                                hacc += __ldg(head.w + c * 16 + 2 * e + 1) * __high2float(pk.h[e]);
+                            }
+                        } else {
+                            uint4* o = reinterpret_cast<uint4*>(out + c * 16);
+                            o[0] = pk.u4[0];
+                            o[1] = pk.u4[1];
+                        }
                     }
                 }
+                if (head.w && in) head.out[m] = hacc;
             }
             tc_fence_before();
             mbar_arrive(acc_free(a));

@@ -198,6 +198,7 @@ class UNet3D:
         self.steps = 0
         self._ws: dict[tuple, _Workspace] = {}
         self.launches = 0
+        self.fuse_head = True  # predict: the head in the last convolution's epilogue
 
     # ---- parameters -------------------------------------------------------------------
     def parameters(self) -> np.ndarray:
@@ -300,7 +301,27 @@ class UNet3D:
                                        ws.m, self._stream()), "pack input")
         self.launches += 1
 
-    def forward(self, ws: _Workspace) -> None:
+    def _conv_head(self, x, layer: ConvLayer, ws: _Workspace, dims) -> bool:
+        """The last convolution with the 1x1x1 head in its epilogue (ws.out
+        directly, its features not stored); False where the kernel does not
+        cover the shape and nothing ran."""
+        n, d, h, w = dims
+        code = self.lib.pmd_conv3d_head(x.data_ptr(), self._ptr16(layer.w_off),
+                                        self._ptr32(self.p32, layer.b_off),
+                                        self._ptr32(self.p32, self.head_w),
+                                        self._ptr32(self.p32, self.head_b), ws.base.data_ptr(),
+                                        ws.out.data_ptr(), n, d, h, w, layer.cin, layer.cout,
+                                        layer.kpad, 1, self._stream())
+        if code == -1:
+            return False
+        _check(code, f"conv {layer.name} + head")
+        self.launches += 1
+        return True
+
+    def forward(self, ws: _Workspace, keep_features: bool = True) -> None:
+        """keep_features False (inference): the last convolution's output is not
+        needed by a backward pass, so the head is fused into it where the
+        kernel allows; the prediction is the same either way."""
         a, L = ws.a, self._by_name
         c0, c1, c2, c3 = LEVELS
         d0, d1, d2, d3 = ws.dims
@@ -323,6 +344,8 @@ class UNet3D:
         self._conv(a["d1a"], L["dec1b"], a["d1"], d1)
         self._upcat(a["d1"], a["e0"], a["u0"], d0, c1, c0)
         self._conv(a["u0"], L["dec0a"], a["d0a"], d0)
+        if not keep_features and self.fuse_head and self._conv_head(a["d0a"], L["dec0b"], ws, d0):
+            return
         self._conv(a["d0a"], L["dec0b"], a["d0"], d0)
         _check(self.lib.pmd_head(a["d0"].data_ptr(), self._ptr32(self.p32, self.head_w),
                                  self._ptr32(self.p32, self.head_b), ws.base.data_ptr(),
@@ -413,7 +436,7 @@ class UNet3D:
         overwritten by the next call of the same shape)."""
         ws = self.workspace(tuple(dose.shape))
         self.pack(ws, dose, density, colmax, density_shared, sigma)
-        self.forward(ws)
+        self.forward(ws, keep_features=False)
         return ws.out.view(dose.shape)
 
 

@@ -398,3 +398,65 @@ def test_oriented_window_gather_and_scatter(gpu):
         sel = where[n] >= 0
         expect[where[n][sel]] = np.maximum(data.cpu().numpy()[0][sel], 0.0) * 2.5
         np.testing.assert_allclose(dst.cpu().numpy().ravel(), expect, rtol=1e-7)
+
+
+@pytest.mark.parametrize("shape", [(2, 5, 17, 9, 16, 16), (1, 8, 32, 24, 16, 16), (1, 3, 18, 10, 32, 32)])
+def test_head_fused_into_the_last_convolution_is_bit_identical(gpu, shape):
+    """pmd_conv3d_head (the 1x1x1 head in the warp-specialized kernel's
+    epilogue) against pmd_conv3d then pmd_head: the same bf16 features and the
+    same float32 sum in channel order, so equal bit for bit."""
+    import torch
+
+    n, d, h, w, cin, cout = shape
+    rng = np.random.default_rng(7 + sum(shape))
+    x = bf16(rng.normal(size=(n, d, h, w, cin)))
+    wt, kpad = _weights(rng, cin, cout)
+    bias = rng.normal(size=cout).astype(np.float32)
+    hw = rng.normal(size=cout).astype(np.float32)
+    hb = np.array([0.25], np.float32)
+    m = n * d * h * w
+    base = rng.normal(size=m).astype(np.float32)
+    lib = _lib.load()
+    dx, dw = _dev(x, torch.bfloat16), _dev(wt, torch.bfloat16)
+    db, dhw, dhb, dbase = (_dev(a, torch.float32) for a in (bias, hw, hb, base))
+    for with_base in (True, False):
+        feat = torch.empty((m, cout), dtype=torch.bfloat16, device=gpu)
+        two = torch.full((m,), float("nan"), dtype=torch.float32, device=gpu)
+        one = torch.full((m,), float("nan"), dtype=torch.float32, device=gpu)
+        bp = dbase.data_ptr() if with_base else None
+        assert lib.pmd_conv3d(dx.data_ptr(), dw.data_ptr(), db.data_ptr(), feat.data_ptr(), n, d, h, w,
+                              cin, cout, kpad, 1, None) == 0
+        assert lib.pmd_head(feat.data_ptr(), dhw.data_ptr(), dhb.data_ptr(), bp, two.data_ptr(), m,
+                            cout, None) == 0
+        assert lib.pmd_conv3d_head(dx.data_ptr(), dw.data_ptr(), db.data_ptr(), dhw.data_ptr(),
+                                   dhb.data_ptr(), bp, one.data_ptr(), n, d, h, w, cin, cout, kpad, 1,
+                                   None) == 0
+        torch.cuda.synchronize()
+        a, b = one.cpu().numpy(), two.cpu().numpy()
+        assert np.isfinite(a).all()
+        np.testing.assert_array_equal(a, b)
+    assert lib.pmd_conv3d_failures() == 0
+    # outside the kernel (cin = 8 is not a warp-specialized shape): nothing launched
+    assert lib.pmd_conv3d_head(dx.data_ptr(), dw.data_ptr(), db.data_ptr(), dhw.data_ptr(),
+                               dhb.data_ptr(), None, one.data_ptr(), n, d, h, w, 4, cout, kpad, 1,
+                               None) == -1
+
+
+def test_predict_with_the_fused_head_equals_the_unfused_network(gpu):
+    import torch
+
+    rng = np.random.default_rng(12)
+    params = init_parameters(seed=4)
+    _, head_w, head_b, _ = layout()
+    params[head_w:head_w + LEVELS[0]] = rng.normal(0, 0.5, LEVELS[0])
+    params[head_b] = 0.01
+    noisy, density, _, _ = _batch(rng, 2, 16)
+    net = UNet3D(gpu, params=params)
+    args = (_dev(noisy, torch.float32), _dev(density, torch.float32))
+    fused = net.predict(*args).clone()
+    launches = net.launches
+    net.fuse_head = False
+    plain = net.predict(*args).clone()
+    assert net.launches - launches == launches + 1  # one more launch: the separate head
+    np.testing.assert_array_equal(fused.cpu().numpy(), plain.cpu().numpy())
+    assert not np.array_equal(plain.cpu().numpy(), noisy)  # the head contributes
