@@ -85,7 +85,8 @@ def config_dict(counts, l2_note):
 
 # ---- clocks -----------------------------------------------------------------------
 class ClockSampler:
-    """nvidia-smi samples during the timed region (every 200 ms)."""
+    """nvidia-smi samples during the timed region (every 50 ms); entering waits
+    (at most 5 s) for the first sample, so sampling is live when timing starts."""
 
     QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -101,12 +102,17 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", "50"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self._t = threading.Thread(target=self._read, daemon=True)
             self._t.start()
         except OSError:
             self.proc = None
+            return self
+        t0 = time.monotonic()
+        while not self.lines and self.proc.poll() is None and time.monotonic() - t0 < 5.0:
+            time.sleep(0.01)
+        self.lines.clear()  # samples from before the timed region
         return self
 
     def _read(self):
@@ -733,8 +739,31 @@ def conv_arm(args, local):
             e1.synchronize()
             row[name] = round(e0.elapsed_time(e1) / args.steps, 4)
             row[name + "_tflops"] = round(lflops / row[name] / 1e9, 1)
+        # the layer's weight gradient (training): tensor cores (default) and mma.sync
+        gy = ly.clone()
+        gw = torch.zeros((layer.cout, layer.kpad), device=device, dtype=torch.float32)
+        gb = torch.zeros(layer.cout, device=device, dtype=torch.float32)
+        winfo = (ctypes.c_int * 8)()
+        row["wgrad_plan"] = list(winfo) if lib.pmd_conv3d_wgrad_plan(*dims, layer.cin, layer.cout,
+                                                                     winfo) == 0 else None
+        for name, impl in (("wgrad", 0), ("wgrad_mma_sync", 1)):
+            lib.pmd_conv3d_impl(impl)
+            call = lambda: lib.pmd_conv3d_wgrad(lx.data_ptr(), gy.data_ptr(), gw.data_ptr(), gb.data_ptr(),
+                                                *dims, layer.cin, layer.cout, layer.kpad,
+                                                stream.cuda_stream)
+            if call() != 0:
+                row[name] = -1
+                continue
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(args.steps):
+                call()
+            e1.record(stream)
+            e1.synchronize()
+            row[name] = round(e0.elapsed_time(e1) / args.steps, 4)
+            row[name + "_tflops"] = round(lflops / row[name] / 1e9, 1)
         layers[layer.name] = row
-        del lx, lw, ly
+        del lx, lw, ly, gy, gw, gb
     lib.pmd_conv3d_impl(previous)
     out["layers_ms"] = layers
 
@@ -761,6 +790,25 @@ def conv_arm(args, local):
         out[name] = {"ms": ms, "tflops": flops_net / ms / 1e9,
                      "launches": (net.launches - launches) / args.steps}
     lib.pmd_conv3d_impl(previous)
+
+    # one training step (forward, loss, backward with the tensor-core weight
+    # gradients, Adam) on a batch of the trainer's shape: 4 windows of 64^3
+    tb = (4, 64, 64, 64)
+    t_dose = torch.rand(tb, device=device, generator=gen)
+    t_rho = torch.ones(tb, device=device)
+    t_target = 0.9 * t_dose
+    t_sigma = 0.1 * t_dose
+    trainer = UNet3D.load(DENOISER_WEIGHTS, device=device)
+    trainer.lr = 1e-5
+    for _ in range(args.warmup):
+        trainer.train_step(t_dose, t_rho, t_target, sigma=t_sigma)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        trainer.train_step(t_dose, t_rho, t_target, sigma=t_sigma)
+    e1.record(stream)
+    e1.synchronize()
+    out["train_step_ms"] = {"batch": list(tb), "ms": round(e0.elapsed_time(e1) / args.steps, 3)}
     out["failures"] = lib.pmd_conv3d_failures()
     print(json.dumps(out), flush=True)
     return 0

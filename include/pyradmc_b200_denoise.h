@@ -79,9 +79,22 @@ int pmd_conv3d_failures(void);
 
 /* Weight gradient, ADDED into fp32 dw [cout][kpad] (and dbias [cout] when not
  * NULL): dw[co][k] += sum over voxels of g[v][co] * im2col(x)[v][k].
- * cout in {16, 32, 64, 128}.  The sum order is not fixed (fp32 atomics). */
+ * cout in {16, 32, 64, 128}.  Runs on the tensor cores (tcgen05.mma, both
+ * operands voxel-major, the sums in tensor memory; one CTA per SM per tap
+ * group, its partial sums added with fp32 atomics) unless pmd_conv3d_impl(1)
+ * selected the mma.sync kernels or the shape is outside the plan
+ * (pmd_conv3d_wgrad_plan); then the mma.sync kernel.  The sum order is not
+ * fixed (fp32 atomics). */
 int pmd_conv3d_wgrad(const void* x, const void* g, float* dw, float* dbias, int n, int d, int h,
                      int w_, int cin, int cout, int kpad, void* stream);
+
+/* The tensor-core weight-gradient plan for this shape, written to info[8]:
+ * output slices per tile, 8-channel chunks per stage, stages per tile (channel
+ * groups), accumulator units per group (taps; with cin = 8 rows of three
+ * taps), unit groups, stage buffers, shared memory bytes per stage,
+ * tensor-memory columns.  Returns 0, or -1 when that kernel does not
+ * cover the shape (or info is NULL). */
+int pmd_conv3d_wgrad_plan(int n, int d, int h, int w_, int cin, int cout, int* info);
 
 /* Data-gradient weights: wd[ci][tap * cout + co] = w[co][(26 - tap) * cin + ci],
  * bf16 [cin][kpad_d], columns past 27 * cout zero. */

@@ -285,6 +285,7 @@ SIGNATURES.update({
     "pmd_conv3d_wgrad": (_i, [_v, _v, _v, _v, _i, _i, _i, _i, _i, _i, _i, _v]),
     "pmd_conv3d_impl": (_i, [_i]),
     "pmd_conv3d_plan": (_i, [_i, _i, _i, _i, _i, _i, _ip]),
+    "pmd_conv3d_wgrad_plan": (_i, [_i, _i, _i, _i, _i, _i, _ip]),
     "pmd_conv3d_head": (_i, [_v, _v, _v, _v, _v, _v, _v, _i, _i, _i, _i, _i, _i, _i, _i, _v]),
     "pmd_gather_windows_oriented": (_i, [_v, _l, _i, _i, _i, _v, _i, _i, _i, _i, _v, _v]),
     "pmd_scatter_windows_oriented": (_i, [_v, _v, _i, _i, _i, _v, _i, _i, _i, _i, _v, _l, _v]),

@@ -758,6 +758,7 @@ __global__ void csc_to_dense_f64_kernel(const int64_t* indptr, const int64_t* in
 
 #include "denoise_umma.cuh"
 #include "denoise_ws.cuh"
+#include "denoise_wgrad.cuh"
 
 using namespace pmd;
 
@@ -1034,6 +1035,23 @@ EncodeTiledFn encode_tiled() {
 // 18 x (tz + 2) x 1, zero fill outside) and the [cout][kpad] weights (box 8 x
 // cout).  False when the driver refuses them (the caller then takes another
 // kernel).
+// The halo map alone: the NDHWC bf16 activation x of shape s, box 8 channels
+// x 10 x 18 x (tz + 2) x 1, zero fill outside.
+bool halo_tensor_map(const __nv_bfloat16* x, const ConvShape& s, int tz, CUtensorMap& xm) {
+    const EncodeTiledFn enc = encode_tiled();
+    if (!enc || reinterpret_cast<uintptr_t>(x) % 16) return false;
+    const cuuint64_t e = sizeof(__nv_bfloat16);
+    const cuuint64_t xdim[5] = {(cuuint64_t)s.cin, (cuuint64_t)s.w, (cuuint64_t)s.h, (cuuint64_t)s.d,
+                                (cuuint64_t)s.n};
+    const cuuint64_t xstride[4] = {xdim[0] * e, xdim[0] * xdim[1] * e, xdim[0] * xdim[1] * xdim[2] * e,
+                                   xdim[0] * xdim[1] * xdim[2] * xdim[3] * e};
+    const cuuint32_t xbox[5] = {8, (cuuint32_t)kUHX, (cuuint32_t)kUHY, (cuuint32_t)(tz + 2), 1};
+    const cuuint32_t ones[5] = {1, 1, 1, 1, 1};
+    return enc(&xm, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, const_cast<__nv_bfloat16*>(x), xdim, xstride, xbox,
+               ones, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+               CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 bool ws_tensor_maps(const __nv_bfloat16* x, const __nv_bfloat16* w, const WsConv& p, CUtensorMap& xm,
                     CUtensorMap& wm) {
     const EncodeTiledFn enc = encode_tiled();
@@ -1041,16 +1059,8 @@ bool ws_tensor_maps(const __nv_bfloat16* x, const __nv_bfloat16* w, const WsConv
     if (reinterpret_cast<uintptr_t>(x) % 16 || reinterpret_cast<uintptr_t>(w) % 16) return false;
     const ConvShape& s = p.s;
     const cuuint64_t e = sizeof(__nv_bfloat16);
-    const cuuint64_t xdim[5] = {(cuuint64_t)s.cin, (cuuint64_t)s.w, (cuuint64_t)s.h, (cuuint64_t)s.d,
-                                (cuuint64_t)s.n};
-    const cuuint64_t xstride[4] = {xdim[0] * e, xdim[0] * xdim[1] * e, xdim[0] * xdim[1] * xdim[2] * e,
-                                   xdim[0] * xdim[1] * xdim[2] * xdim[3] * e};
-    const cuuint32_t xbox[5] = {8, (cuuint32_t)kUHX, (cuuint32_t)kUHY, (cuuint32_t)(p.tz + 2), 1};
     const cuuint32_t ones[5] = {1, 1, 1, 1, 1};
-    if (enc(&xm, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, const_cast<__nv_bfloat16*>(x), xdim, xstride, xbox,
-            ones, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-            CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
-        return false;
+    if (!halo_tensor_map(x, s, p.tz, xm)) return false;
     const cuuint64_t wdim[2] = {(cuuint64_t)s.kpad, (cuuint64_t)s.cout};
     const cuuint64_t wstride[1] = {(cuuint64_t)s.kpad * e};
     const cuuint32_t wbox[2] = {8, (cuuint32_t)s.cout};
@@ -1091,6 +1101,88 @@ int try_ws(const __nv_bfloat16* x, const __nv_bfloat16* w, const float* bias, __
         case 12: code = launch_ws<12>(xm, wm, w, bias, y, p, smem, per_sm, relu, st, head); return 1;
         default: return -1;
     }
+}
+
+// ---- weight gradient on the tensor cores ---------------------------------------------
+// The plan of conv3d_wgrad_umma_kernel: the largest tile depth (2, else 1) and
+// halo channel group (all chunks, else fewer, an even count) for which two or
+// three stages fit shared memory; groups of accumulator units (taps, or with
+// cin = 8 rows of three taps) as large as 512 tensor-memory columns allow.  False outside the kernel: cout not 16/32/64/128, cin not 8
+// or a multiple of 16.
+bool wg_plan(const ConvShape& s, WgConv& p, int& smem) {
+    if (s.cout != 16 && s.cout != 32 && s.cout != 64 && s.cout != 128) return false;
+    if (s.cin != 8 && (s.cin % 16 || s.cin > 256)) return false;
+    const int cpt = s.cin / 8;
+    p = WgConv{};
+    p.s = s;
+    p.dx_fold = s.cin == 8 ? 1 : 0;
+    p.m64 = s.cout <= 64 ? 1 : 0;
+    p.n_units = p.dx_fold ? 9 : 27;
+    p.cols_per_unit = p.dx_fold ? 32u : (unsigned)s.cin;
+    p.units = 512 / (int)p.cols_per_unit < p.n_units ? 512 / (int)p.cols_per_unit : p.n_units;
+    p.unit_groups = (p.n_units + p.units - 1) / p.units;
+    unsigned cols = 32;
+    while (cols < (unsigned)p.units * p.cols_per_unit) cols *= 2;
+    p.tmem_cols = cols;
+    p.dy_lbo = (unsigned)(s.cout / 8) * 128u;
+    for (int tz = 2; tz >= 1; --tz) {
+        const unsigned box = (unsigned)((tz + 2) * kUHY * kUHX * 16);
+        const unsigned plane = (box + 127u) / 128u * 128u;
+        for (int ncg = cpt; ncg >= 1; --ncg) {
+            if (cpt % ncg || (ncg % 2 && !(ncg == 1 && cpt == 1)) || 8 * ncg > 256) continue;
+            const unsigned halo = (unsigned)(ncg == 1 ? 2 : ncg) * plane;
+            const unsigned dyb = (unsigned)(tz * kUTY) * p.dy_lbo + 2048u;
+            const unsigned stage = (halo + dyb + 1023u) / 1024u * 1024u;
+            int stages = (kSmemPerBlockMax - 1024) / (int)stage;
+            if (stages > 3) stages = 3;
+            if (stages < 2) continue;
+            p.tz = tz;
+            p.tiles_d = (s.d + tz - 1) / tz;
+            p.tiles_h = (s.h + kUTY - 1) / kUTY;
+            p.tiles_w = (s.w + kUTX - 1) / kUTX;
+            p.n_tiles = s.n * p.tiles_d * p.tiles_h * p.tiles_w;
+            p.ncg = ncg;
+            p.chunk_groups = cpt / ncg;
+            p.n_mma = p.dx_fold ? 32 : 8 * ncg;
+            p.b_sbo = p.dx_fold ? 16u : plane;
+            p.stages = stages;
+            p.plane_bytes = plane;
+            p.box_bytes = box;
+            p.halo_bytes = halo;
+            p.dy_bytes = dyb;
+            p.stage_bytes = stage;
+            p.tx_bytes = (unsigned)ncg * box;
+            smem = stages * (int)stage + 1024;
+            // one block per SM: its accumulators take all 512 tensor-memory columns
+            if (smem < kSmemPerSM / 2 + 1024) smem = kSmemPerSM / 2 + 1024;
+            return true;
+        }
+    }
+    return false;
+}
+
+// 1 launched (code: 0 or -2), -1 when the plan or the tensor map does not cover the call.
+int try_wgrad_umma(const __nv_bfloat16* x, const __nv_bfloat16* g, float* dw, float* db,
+                   const ConvShape& s, cudaStream_t st, int& code) {
+    WgConv p;
+    int smem = 0;
+    CUtensorMap xm;
+    if (!wg_plan(s, p, smem) || !halo_tensor_map(x, s, p.tz, xm)) return -1;
+    if (reinterpret_cast<uintptr_t>(g) % 16 || reinterpret_cast<uintptr_t>(dw) % 16) return -1;
+    int dev = 0, sms = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+        cudaFuncSetAttribute(conv3d_wgrad_umma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) !=
+            cudaSuccess) {
+        code = -2;
+        return 1;
+    }
+    int per_group = sms / p.unit_groups;
+    if (per_group > p.n_tiles) per_group = p.n_tiles;
+    if (per_group < 1) per_group = 1;
+    conv3d_wgrad_umma_kernel<<<per_group * p.unit_groups, kWgThreads, smem, st>>>(xm, g, dw, db, p);
+    code = launched();
+    return 1;
 }
 
 template <int CPT>
@@ -1196,6 +1288,18 @@ int pmd_conv3d_head(const void* x, const void* w, const float* bias, const float
     return -1;
 }
 
+int pmd_conv3d_wgrad_plan(int n, int d, int h, int wd, int cin, int cout, int* info) {
+    if (!info || n < 1 || d < 1 || h < 1 || wd < 1 || cin < 8 || cin % 8) return -1;
+    ConvShape s{n, d, h, wd, cin, cout, (27 * cin + 63) / 64 * 64};
+    WgConv p;
+    int smem = 0;
+    if (!wg_plan(s, p, smem)) return -1;
+    const int v[8] = {p.tz, p.ncg, p.chunk_groups, p.units, p.unit_groups, p.stages, (int)p.stage_bytes,
+                      (int)p.tmem_cols};
+    for (int i = 0; i < 8; ++i) info[i] = v[i];
+    return 0;
+}
+
 int pmd_conv3d_plan(int n, int d, int h, int wd, int cin, int cout, int* info) {
     if (!info || n < 1 || d < 1 || h < 1 || wd < 1 || cin < 8 || cin % 8) return -1;
     for (int i = 0; i < 8; ++i) info[i] = 0;
@@ -1258,6 +1362,10 @@ int pmd_conv3d_wgrad(const void* x, const void* g, float* dw, float* dbias, int 
     auto X = (const __nv_bfloat16*)x;
     auto G = (const __nv_bfloat16*)g;
     cudaStream_t st = (cudaStream_t)stream;
+    if (g_conv_impl != 1) {  // the tensor-core kernel unless mma.sync is selected
+        int code = 0;
+        if (try_wgrad_umma(X, G, dw, dbias, s, st, code) == 1) return code;
+    }
     switch (cout) {
         case 16: launch_wgrad<16>(X, G, dw, dbias, s, st); break;
         case 32: launch_wgrad<32>(X, G, dw, dbias, s, st); break;

@@ -71,34 +71,67 @@ def test_conv3d_forward_matches_oracle(gpu, shape):
         np.testing.assert_allclose(got, ref, rtol=BF16_REL, atol=1e-5 * np.abs(ref).max())
 
 
-@pytest.mark.parametrize("shape", [(1, 8, 8, 8, 8, 16), (2, 6, 5, 7, 16, 32), (1, 4, 6, 4, 64, 64),
-                                   (1, 4, 4, 4, 192, 64), (1, 4, 4, 8, 48, 16),
-                                   (1, 2, 4, 4, 128, 128)])
+WGRAD_SHAPES = [
+    # every (cin, cout) of the network, partial tiles in d, h and w, one tile
+    # (cin = 8 with its zero partner plane) up to several tiles per CTA, and
+    # tap groups x channel groups for the wide layers
+    (1, 8, 8, 8, 8, 16), (1, 3, 17, 9, 8, 16), (2, 6, 5, 7, 16, 32), (1, 4, 6, 4, 64, 64), (1, 4, 4, 4, 192, 64),
+    (1, 4, 4, 8, 48, 16), (1, 2, 4, 4, 128, 128), (1, 3, 17, 9, 16, 16), (1, 2, 3, 9, 96, 32),
+    (2, 16, 32, 24, 48, 16), (1, 32, 64, 64, 16, 16), (1, 8, 16, 16, 32, 32),
+]
+
+
+def _wgrad_plan(lib, shape):
+    import ctypes
+
+    info = (ctypes.c_int * 8)()
+    return list(info) if lib.pmd_conv3d_wgrad_plan(*shape, info) == 0 else None
+
+
+@pytest.mark.parametrize("shape", WGRAD_SHAPES)
 def test_conv3d_weight_gradient_matches_oracle(gpu, shape):
+    """The tensor-core weight gradient (default) and the mma.sync one
+    (pmd_conv3d_impl(1)) against torch's fp32 conv3d_weight on the same bf16
+    operands."""
     import torch
     from torch.nn.grad import conv3d_weight
 
     n, d, h, w, cin, cout = shape
-    rng = np.random.default_rng(7 + cin + cout)
+    rng = np.random.default_rng(7 + cin + cout + d)
     x = bf16(rng.normal(size=(n, d, h, w, cin)))
     g = bf16(rng.normal(size=(n, d, h, w, cout)))
     kpad = kpad_for(cin)
-    dw = torch.zeros((cout, kpad), dtype=torch.float32, device=gpu)
-    db = torch.zeros(cout, dtype=torch.float32, device=gpu)
+    lib = _lib.load()
+    assert _wgrad_plan(lib, shape) is not None  # the tensor-core kernel covers every layer
     dx, dg = _dev(x, torch.bfloat16), _dev(g, torch.bfloat16)
-    assert _lib.load().pmd_conv3d_wgrad(dx.data_ptr(), dg.data_ptr(), dw.data_ptr(), db.data_ptr(),
-                                        n, d, h, w, cin, cout, kpad, None) == 0
     xt = torch.from_numpy(x.transpose(0, 4, 1, 2, 3).copy())
     gt = torch.from_numpy(g.transpose(0, 4, 1, 2, 3).copy())
-    ref = conv3d_weight(xt, (cout, cin, 3, 3, 3), gt, padding=1)
-    ref_flat = np.zeros((cout, kpad), dtype=np.float32)
+    ref = conv3d_weight(xt.double(), (cout, cin, 3, 3, 3), gt.double(), padding=1)
+    ref_flat = np.zeros((cout, kpad), dtype=np.float64)
     ref_flat[:, :27 * cin] = ref.numpy().transpose(0, 2, 3, 4, 1).reshape(cout, -1)
-    got = dw.cpu().numpy()
+    ref_b = g.astype(np.float64).reshape(-1, cout).sum(0)
     scale = np.abs(ref_flat).max()
-    np.testing.assert_allclose(got, ref_flat, rtol=1e-4, atol=1e-5 * scale)
-    np.testing.assert_allclose(db.cpu().numpy(), g.reshape(-1, cout).sum(0), rtol=1e-4,
-                               atol=1e-4 * np.abs(g).sum(0).max())
-    assert (got[:, 27 * cin:] == 0).all()
+    m = n * d * h * w
+    got = {}
+    previous = lib.pmd_conv3d_impl(-1)
+    try:
+        for impl in (0, 1):
+            lib.pmd_conv3d_impl(impl)
+            dw = torch.zeros((cout, kpad), dtype=torch.float32, device=gpu)
+            db = torch.zeros(cout, dtype=torch.float32, device=gpu)
+            assert lib.pmd_conv3d_wgrad(dx.data_ptr(), dg.data_ptr(), dw.data_ptr(), db.data_ptr(),
+                                        n, d, h, w, cin, cout, kpad, None) == 0
+            got[impl] = (dw.cpu().numpy(), db.cpu().numpy())
+    finally:
+        lib.pmd_conv3d_impl(previous)
+    assert lib.pmd_conv3d_failures() == 0
+    for impl, (gw, gb) in got.items():
+        # fp32 sums of m products of bf16 values in an unfixed order
+        np.testing.assert_allclose(gw, ref_flat, rtol=1e-4, atol=1e-6 * scale * max(1.0, m / 4096),
+                                   err_msg=f"impl {impl}")
+        np.testing.assert_allclose(gb, ref_b, rtol=1e-4, atol=1e-4 * np.abs(g).sum(0).max(),
+                                   err_msg=f"impl {impl}")
+        assert (gw[:, 27 * cin:] == 0).all()
 
 
 @pytest.mark.parametrize("shape", [(1, 8, 8, 8, 16, 16), (2, 6, 5, 7, 48, 16), (1, 4, 6, 4, 96, 32),
