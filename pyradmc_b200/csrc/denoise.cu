@@ -518,7 +518,14 @@ __global__ void loss_kernel(const float* pred, const float* target, const float*
     }
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) local += __shfl_xor_sync(0xffffffffu, local, off);
-    if ((threadIdx.x & 31) == 0) atomicAdd(loss, local * inv_n);
+    __shared__ float part[8];  // one sum per warp of the 256-thread block, one atomic per block
+    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = local;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float v = 0.0f;
+        for (int i = 0; i < (int)(blockDim.x >> 5); ++i) v += part[i];
+        atomicAdd(loss, v * inv_n);
+    }
 }
 
 // Head backward: dF[m][c] = g[m] w[c] (bf16), dW[c] += sum_m g[m] f[m][c], db += sum_m g[m].
@@ -548,16 +555,27 @@ __global__ void head_grad_kernel(const uint4* f, const float* w, const float* g,
             df[m * (C / 8) + c] = pack8(o);
         }
     }
+    // warp sums, then block sums: one atomic per block and parameter (the
+    // launch keeps the grid at a few blocks per SM, so each of the C + 1
+    // addresses sees a few hundred atomics, not one per warp)
+    __shared__ float part[C + 1][8];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 #pragma unroll
     for (int k = 0; k < C; ++k) {
         float v = lw[k];
 #pragma unroll
         for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
-        if ((threadIdx.x & 31) == 0) atomicAdd(dw + k, v);
+        if (lane == 0) part[k][warp] = v;
     }
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) lb += __shfl_xor_sync(0xffffffffu, lb, off);
-    if ((threadIdx.x & 31) == 0) atomicAdd(db, lb);
+    if (lane == 0) part[C][warp] = lb;
+    __syncthreads();
+    if (threadIdx.x <= C) {
+        float v = 0.0f;
+        for (int i = 0; i < (int)(blockDim.x >> 5); ++i) v += part[threadIdx.x][i];
+        atomicAdd(threadIdx.x < C ? dw + threadIdx.x : db, v);
+    }
 }
 
 // Adam on fp32 master parameters; refreshes the bf16 working copy (when given)
@@ -1445,11 +1463,12 @@ int pmd_head_grad(const void* f, const float* w, const float* g, void* df, float
     cudaStream_t st = (cudaStream_t)stream;
     auto F = (const uint4*)f;
     auto DF = (uint4*)df;
+    const int head_grid = grid_for(m) < 148 * 4 ? grid_for(m) : 148 * 4;  // 256 threads = 8 warps
     switch (c) {
-        case 8: head_grad_kernel<8><<<grid_for(m), 256, 0, st>>>(F, w, g, DF, dw, db, m); break;
-        case 16: head_grad_kernel<16><<<grid_for(m), 256, 0, st>>>(F, w, g, DF, dw, db, m); break;
-        case 32: head_grad_kernel<32><<<grid_for(m), 256, 0, st>>>(F, w, g, DF, dw, db, m); break;
-        case 64: head_grad_kernel<64><<<grid_for(m), 256, 0, st>>>(F, w, g, DF, dw, db, m); break;
+        case 8: head_grad_kernel<8><<<head_grid, 256, 0, st>>>(F, w, g, DF, dw, db, m); break;
+        case 16: head_grad_kernel<16><<<head_grid, 256, 0, st>>>(F, w, g, DF, dw, db, m); break;
+        case 32: head_grad_kernel<32><<<head_grid, 256, 0, st>>>(F, w, g, DF, dw, db, m); break;
+        case 64: head_grad_kernel<64><<<head_grid, 256, 0, st>>>(F, w, g, DF, dw, db, m); break;
         default: return -1;
     }
     return launched();
@@ -1457,8 +1476,8 @@ int pmd_head_grad(const void* f, const float* w, const float* g, void* df, float
 
 int pmd_loss(const float* pred, const float* target, const float* weight, float lambda,
              float* grad, float* loss, int64_t m, void* stream) {
-    loss_kernel<<<grid_for(m), 256, 0, (cudaStream_t)stream>>>(pred, target, weight, lambda, grad,
-                                                                loss, m);
+    const int grid = grid_for(m) < 148 * 4 ? grid_for(m) : 148 * 4;
+    loss_kernel<<<grid, 256, 0, (cudaStream_t)stream>>>(pred, target, weight, lambda, grad, loss, m);
     return launched();
 }
 
