@@ -90,11 +90,14 @@ def layout() -> tuple[list[ConvLayer], int, int, int]:
 
 
 def forward_flops_per_voxel() -> float:
-    """Multiply-add FLOPs of one forward pass per full-resolution voxel (the
-    convolutions' 2 * 27 * cin * cout at their level's voxel fraction)."""
+    """Useful multiply-add FLOPs of one forward pass per full-resolution voxel
+    (the convolutions' 2 * 27 * cin * cout at their level's voxel fraction),
+    the input layer counted on its 3 real channels (dose, sigma, density), not
+    the 5 zero channels that pad its voxel rows to 16 bytes."""
     layers, *_ = layout()
     level = {"enc0": 0, "enc1": 1, "enc2": 2, "mid_": 3, "dec2": 2, "dec1": 1, "dec0": 0}
-    return float(sum(2 * 27 * l.cin * l.cout / 8 ** level[l.name[:4]] for l in layers))
+    return float(sum(2 * 27 * (3 if l.name == "enc0a" else l.cin) * l.cout / 8 ** level[l.name[:4]]
+                     for l in layers))
 
 
 def init_parameters(seed: int = 0) -> np.ndarray:
