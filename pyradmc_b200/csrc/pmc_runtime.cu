@@ -98,7 +98,8 @@ struct pmc_engine {
     long long colmax_len = 0;
     DevBuf tile_counts, tile_offsets, col_counts, out_idx, out_dose, out_sigma, col_nhist;
     unsigned long long* d_nnz = nullptr;
-    std::vector<void*> run_allocs;  // per-call generator arrays
+    std::vector<DevBuf> run_pool;  // per-call generator arrays, reused across calls
+    size_t run_used = 0;           // pool slots taken by the current call or group
 
     // graph of the drain loop
     cudaGraph_t graph = nullptr;
@@ -202,14 +203,21 @@ int grid_blocks(long long n) {
     return (int)std::min<long long>(std::max<long long>(b, 1), 148LL * 16);
 }
 
+// A generator array for the current group: the next slot of a pool of device
+// buffers kept across calls (grown only when too small), filled by a copy
+// ordered on the engine's stream — after the kernels of the previous group
+// that read the same slot — with no device-wide synchronization.  (A pageable
+// source is staged before the call returns, so v may go away afterwards.)
 template <typename T>
 int upload_vec(pmc_engine* e, const std::vector<T>& v, const T** out) {
-    void* p = nullptr;
-    PMC_CUDA(e, cudaMalloc(&p, std::max<size_t>(v.size() * sizeof(T), 16)));
-    if (!v.empty()) PMC_CUDA(e, cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
-    e->h2d_bytes += (unsigned long long)(v.size() * sizeof(T));
-    e->run_allocs.push_back(p);
-    *out = (const T*)p;
+    if (e->run_used == e->run_pool.size()) e->run_pool.emplace_back();
+    DevBuf& b = e->run_pool[e->run_used++];
+    const size_t bytes = v.size() * sizeof(T);
+    const int rc = ensure(e, b, bytes);
+    if (rc) return rc;
+    if (!v.empty()) PMC_CUDA(e, cudaMemcpyAsync(b.p, v.data(), bytes, cudaMemcpyHostToDevice, e->stream));
+    e->h2d_bytes += (unsigned long long)bytes;
+    *out = (const T*)b.p;
     return PMC_OK;
 }
 
@@ -223,10 +231,8 @@ int ensure_batch_events(pmc_engine* e, size_t n) {
     return PMC_OK;
 }
 
-void free_run_allocs(pmc_engine* e) {
-    for (void* p : e->run_allocs) cudaFree(p);
-    e->run_allocs.clear();
-}
+// The pool's slots are free for the next group (the buffers stay allocated).
+void free_run_allocs(pmc_engine* e) { e->run_used = 0; }
 
 void free_tables(pmc_engine* e) {
     for (void* p : e->table_allocs) cudaFree(p);
@@ -863,7 +869,9 @@ void pmc_destroy(pmc_engine* e) {
     cudaSetDevice(e->device);
     if (e->stream) cudaStreamSynchronize(e->stream);
     destroy_graph(e);
-    free_run_allocs(e);
+    for (DevBuf& b : e->run_pool)
+        if (b.p) cudaFree(b.p);
+    e->run_pool.clear();
     free_tables(e);
     if (e->d_gs4) cudaFree(e->d_gs4);
     if (e->d_vox) cudaFree(e->d_vox);
@@ -1212,10 +1220,10 @@ int pmc_run_forward(pmc_engine* e, const pmc_source_desc* src, const pmc_run_par
     if (rc) return rc;
     if (G.kind != PMC_PHOTON && G.kind != PMC_ELECTRON && G.type != 3 && G.type != 5)
         return fail(e, PMC_ERR_INVALID, "unknown primary kind %d", G.kind);
-    PMC_CUDA(e, cudaMemcpy(e->d_gen, &G, sizeof G, cudaMemcpyHostToDevice));
+    PMC_CUDA(e, cudaMemcpyAsync(e->d_gen, &G, sizeof G, cudaMemcpyHostToDevice, e->stream));
     e->h2d_bytes += (unsigned long long)(sizeof G);
     const double nh = (double)per_batch;
-    PMC_CUDA(e, cudaMemcpy(e->col_nhist.p, &nh, sizeof nh, cudaMemcpyHostToDevice));
+    PMC_CUDA(e, cudaMemcpyAsync(e->col_nhist.p, &nh, sizeof nh, cudaMemcpyHostToDevice, e->stream));
     e->h2d_bytes += (unsigned long long)(sizeof nh);
 
     rc = reset_counters(e);
@@ -1296,10 +1304,18 @@ int pmc_run_dij(pmc_engine* e, const pmc_beamlet_desc* src, const int64_t* count
     if (rc) return rc;
     const long long n_vox = e->si.n_voxels;
     int group = p->beamlet_group_size > 0 ? p->beamlet_group_size : 0;
+    const int all_cols = std::min(n_beam, 4096);
+    const size_t all_n = (size_t)stride_for(n_vox) * (size_t)all_cols;
+    if (group == 0 && e->edep.bytes >= sizeof(double) * all_n && e->s1.bytes >= sizeof(double) * all_n &&
+        e->s2.bytes >= sizeof(double) * all_n && e->dirty.bytes >= sizeof(unsigned int) * (all_n / kWordEntries) &&
+        e->touched.bytes >= sizeof(unsigned int) * (all_n / kWordEntries))
+        group = all_cols;  // the maps held already cover every column: no memory query
     if (group == 0) {
         // Auto: the largest group whose dense maps (int64 quanta + two float64
         // sums = 24 bytes per entry, plus the two sector bitmaps) fit half of
-        // the free memory, counting the maps this engine already holds.
+        // the free memory, counting the maps this engine already holds.  The
+        // query can take a millisecond or far more on a busy GPU host, hence
+        // the shortcut above.
         size_t free_b = 0, total_b = 0;
         PMC_CUDA(e, cudaMemGetInfo(&free_b, &total_b));
         const double held = (double)(e->edep.bytes + e->s1.bytes + e->s2.bytes + e->dirty.bytes +
@@ -1379,9 +1395,10 @@ int pmc_run_dij(pmc_engine* e, const pmc_beamlet_desc* src, const int64_t* count
             if (!rc) rc = upload_f32(e, spec_cdf, &G.cdf);
         }
         if (rc) return rc;
-        PMC_CUDA(e, cudaMemcpy(e->d_gen, &G, sizeof G, cudaMemcpyHostToDevice));
+        PMC_CUDA(e, cudaMemcpyAsync(e->d_gen, &G, sizeof G, cudaMemcpyHostToDevice, e->stream));
     e->h2d_bytes += (unsigned long long)(sizeof G);
-        PMC_CUDA(e, cudaMemcpy(e->col_nhist.p, nh.data(), sizeof(double) * gs, cudaMemcpyHostToDevice));
+        PMC_CUDA(e, cudaMemcpyAsync(e->col_nhist.p, nh.data(), sizeof(double) * gs, cudaMemcpyHostToDevice,
+                                    e->stream));
     e->h2d_bytes += (unsigned long long)(sizeof(double) * gs);
         rc = begin_maps(e, gs);
         if (!rc) rc = ensure_batch_events(e, 3 * (size_t)p->n_batches);
