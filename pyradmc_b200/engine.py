@@ -174,11 +174,22 @@ def _pinned_array(n: int, dtype) -> np.ndarray:
         try:
             import torch
 
-            tdt = {np.dtype(np.int64): torch.int64, np.dtype(np.float64): torch.float64}[np.dtype(dtype)]
+            tdt = {np.dtype(np.int64): torch.int64, np.dtype(np.float64): torch.float64,
+                   np.dtype(np.float32): torch.float32, np.dtype(np.uint8): torch.uint8}[np.dtype(dtype)]
             return torch.empty(int(n), dtype=tdt, pin_memory=True).numpy()
         except Exception:
             pass
     return np.empty(n, dtype=dtype)
+
+
+def _pinned_copy(a, dtype) -> np.ndarray:
+    """`a` converted to a contiguous `dtype` array in page-locked host memory
+    (same shape): the arrays the engine uploads again on every drop of the
+    device copies then cross the bus by DMA at the full link rate."""
+    a = np.asarray(a)
+    out = _pinned_array(a.size, dtype).reshape(a.shape)
+    np.copyto(out, a, casting="unsafe")
+    return out
 
 
 def column_shards(counts, world: int) -> list[tuple[int, int]]:
@@ -485,8 +496,8 @@ class B200Engine:
         key = ("grid", id(self.grid))
         hit = self._host_arrays.get(key)
         if hit is None:
-            hit = (np.ascontiguousarray(np.asarray(self.grid.density), dtype=np.float32),
-                   np.ascontiguousarray(np.asarray(self.grid.material).astype(np.uint8)))
+            hit = (_pinned_copy(self.grid.density, np.float32),
+                   _pinned_copy(np.asarray(self.grid.material).astype(np.uint8), np.uint8))
             self._host_arrays[key] = hit
         return hit
 
@@ -496,9 +507,8 @@ class B200Engine:
         key = ("mass", id(self.grid))
         hit = self._host_arrays.get(key)
         if hit is None:
-            hit = np.ascontiguousarray(
-                np.asarray(model.ScoringGrid.for_grid(self.grid).voxel_mass).reshape(-1),
-                dtype=np.float64)
+            hit = _pinned_copy(np.asarray(model.ScoringGrid.for_grid(self.grid).voxel_mass).reshape(-1),
+                               np.float64)
             self._host_arrays[key] = hit
         return hit
 
@@ -582,7 +592,10 @@ class B200Engine:
             gs = self._gs_host(host, ecut, e_max)
             gkey2 = id(gs)
             if native.gs_key != gkey2:
-                values = np.ascontiguousarray(np.asarray(gs.values), dtype=np.float32)
+                vkey = ("gs_values", gkey2)
+                values = self._host_arrays.get(vkey)
+                if values is None:  # converted once per GS grid, in page-locked memory
+                    values = self._host_arrays[vkey] = _pinned_copy(gs.values, np.float32)
                 n_eta, n_t2, n_u = values.shape
                 native.check(lib.pmc_upload_gs(native.handle, _lib.ptr(values, C.c_float),
                                                int(gs.ix0), int(gs.iy0), n_eta, n_t2, n_u,
