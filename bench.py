@@ -299,9 +299,11 @@ def denoiser_leg(args, engine, source, counts, stream, device, plain_s_per_dij):
     every rung reports error and signed bias at 50, 10 and 1 % of the maximum
     for both methods.  Plain Monte Carlo at 2 % on a region is its measured s
     per Dij at the benchmark counts times (its error there / 2 %)^2 (1/sqrt(N)).
-    Timed (CUDA events on the engine's stream): ``run_dij_denoised`` at the
-    chosen scale, from transport to the CSC in HBM (device-resident, like
-    ``value``)."""
+    Every rung is denoised with windows DEN_LATERALS voxels across; a region
+    takes the lowest rung where any of them reaches 2 %, with the narrowest
+    such window (the cheaper U-Net).  Timed (CUDA events on the engine's
+    stream): ``run_dij_denoised`` at the chosen scale and window, from
+    transport to the CSC in HBM (device-resident, like ``value``)."""
     import torch
 
     from pyradmc_b200 import _lib
@@ -313,7 +315,8 @@ def denoiser_leg(args, engine, source, counts, stream, device, plain_s_per_dij):
     torch.cuda.empty_cache()  # the engine allocates outside torch's cache
     net = UNet3D.load(DENOISER_WEIGHTS, device=device)
     shape = tuple(engine.grid.shape)
-    window = D.inference_window(shape, 64)
+    windows = {lat: D.inference_window(shape, lat) for lat in DEN_LATERALS}
+    window = windows[DEN_LATERALS[0]]
     rho = torch.from_numpy(np.ascontiguousarray(engine.grid.density, dtype=np.float32).ravel()).to(device)
     ref = engine.run_dij_device(source, REF_HISTORIES, N_BATCHES, SEED + 977, truncation=0.0)
     ref_dose, _, ref_sigma = D.dense_columns(ref, device, with_sigma=True)
@@ -327,16 +330,23 @@ def denoiser_leg(args, engine, source, counts, stream, device, plain_s_per_dij):
         c = np.maximum(N_BATCHES, np.round(counts * g / N_BATCHES).astype(np.int64) * N_BATCHES)
         view = engine.run_dij_device(source, c, N_BATCHES, SEED + 31, truncation=0.0)
         dose, colmax, sg = D.dense_columns(view, device, with_sigma=True)
-        den = D.denoise_dense(net, dose, colmax, rho, shape, sigma=sg, window=window,
-                              directions=D.beam_directions(source), spacing=engine.grid.spacing)
+        by_window = {}
+        for lat, win in windows.items():
+            den = D.denoise_dense(net, dose, colmax, rho, shape, sigma=sg, window=win,
+                                  directions=D.beam_directions(source), spacing=engine.grid.spacing)
+            by_window[lat] = D.error_report(den, ref_dose, ref_sigma)
+            del den
         rung = {"scale": g, "histories": int(c.sum()),
-                "denoised": D.error_report(den, ref_dose, ref_sigma),
+                "denoised": by_window[DEN_LATERALS[0]],
+                "denoised_by_lateral": {str(k): v for k, v in by_window.items()},
                 "plain": D.error_report(dose, ref_dose, ref_sigma)}
         ladder.append(rung)
-        del den, dose, sg
+        del dose, sg
         for t in ("0.5", "0.1"):
-            if t not in chosen and rung["denoised"][t]["sigma_eq"] <= 0.02:
-                chosen[t] = (g, c)
+            # the cheapest window (the narrowest) that reaches 2 % at this rung
+            ok = [lat for lat in DEN_LATERALS if by_window[lat][t]["sigma_eq"] <= 0.02]
+            if t not in chosen and ok:
+                chosen[t] = (g, c, min(ok))
         if len(chosen) == 2:
             break
     del ref_dose, ref_sigma
@@ -344,8 +354,8 @@ def denoiser_leg(args, engine, source, counts, stream, device, plain_s_per_dij):
         return {"reached_2pct": False, "ladder": ladder,
                 "reference_histories_per_beamlet": REF_HISTORIES}
 
-    def timed(c, **extra):
-        kw = dict(n_histories_per_beamlet=c, n_batches=N_BATCHES, seed=SEED, **extra)
+    def timed(c, lateral, **extra):
+        kw = dict(n_histories_per_beamlet=c, n_batches=N_BATCHES, seed=SEED, lateral=lateral, **extra)
         for _ in range(max(1, args.warmup)):
             D.run_dij_denoised(engine, net, source, truncation=1e-3, to_host=False, **kw)
         times, launches0 = [], net.launches
@@ -362,11 +372,11 @@ def denoiser_leg(args, engine, source, counts, stream, device, plain_s_per_dij):
         return float(np.median(times)), (net.launches - launches0) / args.steps, dij
 
     regions = {}
-    for t, (g, c) in chosen.items():
+    for t, (g, c, lat) in chosen.items():
         # one group, and DEN_GROUP-column groups whose denoising overlaps the next
         # group's transport (the same Dij bit for bit); the faster is the method's time
-        s_seq, unet_launches, dij = timed(c)
-        s_pipe, _, _ = timed(c, group_columns=DEN_GROUP, overlap=True)
+        s_seq, unet_launches, dij = timed(c, lat)
+        s_pipe, _, _ = timed(c, lat, group_columns=DEN_GROUP, overlap=True)
         s_den = min(s_seq, s_pipe)
         plain_err = plain_at_counts[t]["sigma_eq"]
         plain_s = plain_s_per_dij * (plain_err / 0.02) ** 2
@@ -374,15 +384,16 @@ def denoiser_leg(args, engine, source, counts, stream, device, plain_s_per_dij):
         regions[t] = {"history_scale": g, "histories_per_dij": int(c.sum()),
                       "s_per_dij_at_2pct": s_den, "plain_sigma_eq_at_benchmark_counts": plain_err,
                       "plain_s_per_dij_at_2pct": plain_s, "speedup_vs_plain": plain_s / s_den,
-                      "denoised": rung["denoised"], "plain_same_histories": rung["plain"],
+                      "lateral": lat, "denoised": rung["denoised_by_lateral"][str(lat)],
+                      "plain_same_histories": rung["plain"],
                       "unet_launches_per_dij": unet_launches, "nnz": int(dij.indptr[-1]),
                       "s_one_group": s_seq, "s_pipelined": s_pipe,
                       "pipelined_group_columns": DEN_GROUP}
     head = regions["0.5"]
-    g, c = chosen["0.5"]
+    g, c, lat = chosen["0.5"]
     stages: dict = {}
     D.run_dij_denoised(engine, net, source, c, N_BATCHES, SEED, truncation=1e-3, to_host=False,
-                       timings=stages)
+                       lateral=lat, timings=stages)
 
     # the dominant convolution (decoder level 0, 48 -> 16 channels, default path)
     lib = _lib.load()
@@ -402,7 +413,7 @@ def denoiser_leg(args, engine, source, counts, stream, device, plain_s_per_dij):
     e1.synchronize()
     conv_s = e0.elapsed_time(e1) / 10 / 1e3
     conv_tflops = 2.0 * b * wx * wy * wz * 27 * 48 * 16 / conv_s / 1e12
-    unet_vox = len(counts) * wx * wy * wz
+    unet_vox = len(counts) * int(np.prod(windows[lat]))  # the timed method's windows
     peaks_path = ROOT / "MEASURED_PEAKS.json"
     peaks = json.loads(peaks_path.read_text()) if peaks_path.exists() else {}
     bf16_peak = float(peaks.get("bf16_tflops", 1590.0))
@@ -420,7 +431,8 @@ def denoiser_leg(args, engine, source, counts, stream, device, plain_s_per_dij):
         "sigma": "per-entry sigma of the denoised Dij is the input Monte Carlo sigma",
         "reference_histories_per_beamlet": REF_HISTORIES,
         "ladder": ladder,
-        "window": list(window),
+        "window": list(windows[lat]),
+        "windows_tried": {str(k): list(v) for k, v in windows.items()},
         "stage_ms": stages,
         "unet_forward_flops_per_dij": forward_flops_per_voxel() * unet_vox,
         "roofline": {"bound": "tensor", "kernel": "conv3d_ws_kernel (decoder level 0, 48->16)",
@@ -593,6 +605,7 @@ def parity_block(device):
 
 
 DEN_GROUP = 25  # columns per group when MC and denoising overlap across groups
+DEN_LATERALS = (64, 48)  # lateral window sizes tried (the network trains on 64); the narrowest reaching 2 % is timed
 PLAN_WINDOW = (64, 64, 128)  # lateral x lateral x depth chunk of the plan's denoising windows
 PLAN_GROUP = 100            # columns whose dense maps are on the device at once
 
