@@ -36,6 +36,19 @@ def _stream(device) -> int:
     return _torch().cuda.current_stream(device).cuda_stream
 
 
+def _device_density(engine, device):
+    """The engine grid's density as float32 [vox] on `device`, converted and
+    uploaded once per (grid, device) and kept on the engine: the conversion
+    and a pageable upload cost milliseconds of host time per Dij."""
+    torch = _torch()
+    key = ("density_on_device", id(engine.grid), str(device))
+    rho = engine._host_arrays.get(key)  # the engine's per-grid cache
+    if rho is None:
+        rho = engine._host_arrays[key] = torch.from_numpy(
+            np.ascontiguousarray(engine.grid.density, dtype=np.float32).ravel()).to(device)
+    return rho
+
+
 def dense_columns(view, device, with_sigma: bool = False):
     """(dose f32 [C, vox], colmax f32 [C], sigma f32 [C, vox] or None) of a
     :class:`DeviceDij` on its device."""
@@ -390,7 +403,7 @@ def inference_window(grid_shape, lateral: int = 64, depth: int | None = None) ->
 
 
 def denoise_dense(net: UNet3D, dose, colmax, density, grid_shape, *, sigma=None, window=None,
-                  chunk: int = 32, out=None, directions=None, spacing=None):
+                  chunk: int = 100, out=None, directions=None, spacing=None):
     """Denoised dense columns, float64 [C, vox]: the Monte Carlo columns
     (float32 dose [C, vox] with their maxima and, optionally, their sigma; or
     `out`, float64, written in place) with every window along each column's
@@ -452,7 +465,7 @@ def compact(mean, sigma, truncation: float, to_host: bool = True):
 
 def run_dij_denoised(engine, net: UNet3D | None, source, n_histories_per_beamlet, n_batches: int,
                      seed: int, *, truncation: float = 1.0e-3, lateral: int = 64,
-                     depth: int | None = None, chunk: int = 32, to_host: bool = True,
+                     depth: int | None = None, chunk: int = 100, to_host: bool = True,
                      timings: dict | None = None, group_columns: int | None = None,
                      overlap: bool = False):
     """A Dij from low-history Monte Carlo plus the denoiser: the engine runs the
@@ -520,8 +533,7 @@ def run_dij_denoised(engine, net: UNet3D | None, source, n_histories_per_beamlet
         mean, sigma = dense_columns_f64(view, device)
         books += np.asarray(view.books, dtype=np.int64)
         if rho is None:
-            rho = torch.from_numpy(np.ascontiguousarray(engine.grid.density, dtype=np.float32)
-                                   .ravel()).to(device)
+            rho = _device_density(engine, device)
         window = inference_window(shape, lateral, depth)
         if pipelined:
             ready = torch.cuda.Event()
