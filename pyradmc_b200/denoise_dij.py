@@ -23,7 +23,7 @@ from dataclasses import dataclass
 import numpy as np
 
 from . import _lib
-from .denoiser import UNet3D, _check
+from .denoiser import LEVELS, UNet3D, _check
 
 
 def _torch():
@@ -402,6 +402,16 @@ def inference_window(grid_shape, lateral: int = 64, depth: int | None = None) ->
     return wa, wa, wd
 
 
+def chunk_windows(n_win: int, window, chunk: int) -> int:
+    """Windows per U-Net pass: at most `chunk`, equal passes (no padded work),
+    and few enough that the network's widest activation — the level-0
+    concatenation, LEVELS[0] + LEVELS[1] channels — stays below 2^31 elements
+    (its element-wise kernels index 32-bit)."""
+    per_window = int(np.prod(window)) * (LEVELS[0] + LEVELS[1])
+    chunk = max(1, min(int(chunk), (2 ** 31 - 1) // per_window, max(1, n_win)))
+    return -(-max(1, n_win) // -(-max(1, n_win) // chunk))
+
+
 def denoise_dense(net: UNet3D, dose, colmax, density, grid_shape, *, sigma=None, window=None,
                   chunk: int = 100, out=None, directions=None, spacing=None):
     """Denoised dense columns, float64 [C, vox]: the Monte Carlo columns
@@ -419,7 +429,7 @@ def denoise_dense(net: UNet3D, dose, colmax, density, grid_shape, *, sigma=None,
         out = dose.to(torch.float64)
     scale = colmax[win[:, 4].to(torch.int64)].contiguous()
     n_win = win.shape[0]
-    chunk = -(-n_win // -(-n_win // chunk))  # equal chunks of at most `chunk` windows: no padded work
+    chunk = chunk_windows(n_win, window, chunk)
     for w0 in range(0, n_win, chunk):
         w1 = min(w0 + chunk, n_win)
         idx = torch.arange(w0, w0 + chunk, device=dose.device).clamp_max(n_win - 1)  # fixed batch shape
@@ -433,6 +443,9 @@ def denoise_dense(net: UNet3D, dose, colmax, density, grid_shape, *, sigma=None,
     return out
 
 
+_COMPACT_CAPACITY: dict = {}  # (columns, voxels, device) -> entries to reserve next time
+
+
 def compact(mean, sigma, truncation: float, to_host: bool = True):
     """Truncation + CSC of dense float64 columns on the device, through the
     allocation-free compaction entry point: (indptr, indices, dose, sigma) on
@@ -442,24 +455,33 @@ def compact(mean, sigma, truncation: float, to_host: bool = True):
     lib = _lib.load()
     n_cols, vox = mean.shape
     dev = mean.device
-    cap = int(torch.count_nonzero(mean).item()) + 1  # kept entries are non-zero
-    counts = torch.zeros(n_cols, dtype=torch.int64, device=dev)
-    idx = torch.empty(cap, dtype=torch.int64, device=dev)
-    dose = torch.empty(cap, dtype=torch.float64, device=dev)
-    sig = torch.empty(cap, dtype=torch.float64, device=dev)
-    nnz = C.c_int64()
-    code = lib.pmc_dij_compact_static(C.c_void_p(mean.data_ptr()), C.c_void_p(sigma.data_ptr()),
-                                      n_cols, vox, float(truncation), cap,
-                                      C.c_void_p(counts.data_ptr()), C.c_void_p(idx.data_ptr()),
-                                      C.c_void_p(dose.data_ptr()), C.c_void_p(sig.data_ptr()),
-                                      C.byref(nnz), C.c_void_p(_stream(dev)))
+    # capacity: the last call's entry count of this shape plus slack (a call
+    # that needs more is told so and runs again with the exact size); no
+    # counting pass over the dense columns
+    key = (n_cols, vox, str(dev))
+    cap = _COMPACT_CAPACITY.get(key, 1 << 20)
+    for _ in range(2):
+        counts = torch.zeros(n_cols, dtype=torch.int64, device=dev)
+        idx = torch.empty(cap, dtype=torch.int64, device=dev)
+        dose = torch.empty(cap, dtype=torch.float64, device=dev)
+        sig = torch.empty(cap, dtype=torch.float64, device=dev)
+        nnz = C.c_int64()
+        code = lib.pmc_dij_compact_static(C.c_void_p(mean.data_ptr()), C.c_void_p(sigma.data_ptr()),
+                                          n_cols, vox, float(truncation), cap,
+                                          C.c_void_p(counts.data_ptr()), C.c_void_p(idx.data_ptr()),
+                                          C.c_void_p(dose.data_ptr()), C.c_void_p(sig.data_ptr()),
+                                          C.byref(nnz), C.c_void_p(_stream(dev)))
+        if code != _lib.PMC_ERR_CAPACITY:
+            break
+        cap = int(nnz.value) + 1  # the size this call needs
     if code != _lib.PMC_OK:
         raise RuntimeError(f"pmc_dij_compact_static failed ({code})")
     k = nnz.value
+    _COMPACT_CAPACITY[key] = k + k // 16 + 1024
     indptr = np.zeros(n_cols + 1, dtype=np.int64)
     np.cumsum(counts.cpu().numpy(), out=indptr[1:])
-    if not to_host:  # copies, so the capacity-sized buffers are freed
-        return indptr, idx[:k].clone(), dose[:k].clone(), sig[:k].clone()
+    if not to_host:  # views: the capacity is at most ~6 % above the entries
+        return indptr, idx[:k], dose[:k], sig[:k]
     return indptr, idx[:k].cpu().numpy(), dose[:k].cpu().numpy(), sig[:k].cpu().numpy()
 
 

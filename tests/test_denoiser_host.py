@@ -183,3 +183,16 @@ def test_oriented_windows_follow_each_beamlet():
     assert win[3].tolist() == [1, 3, 0, 4, 1, 0, 0]  # x 5 - 4, y 7 - 4, full depth, no shear
     one = D.oriented_windows(dose.view(2, -1), shape, dirs, window, starts=np.array([10, 0]))
     assert one.shape == (2, 7) and one[0, 0] == 40 - 26  # one window per column at that depth
+
+
+def test_chunks_respect_the_32_bit_activation_limit():
+    from pyradmc_b200.denoise_dij import chunk_windows
+
+    # 64 x 64 x 128 windows: 48 channels x 524,288 voxels each -> at most 85 per pass
+    assert chunk_windows(100, (64, 64, 128), 100) == 50  # two equal passes
+    assert chunk_windows(100, (48, 48, 128), 100) == 100
+    assert chunk_windows(7, (64, 64, 64), 100) == 7
+    assert chunk_windows(250, (64, 64, 128), 100) == 84  # three passes of <= 85
+    for n in (1, 33, 100, 257):
+        c = chunk_windows(n, (64, 64, 128), 100)
+        assert c * 64 * 64 * 128 * 48 < 2 ** 31 and c >= 1
