@@ -274,6 +274,43 @@ SIGNATURES: dict[str, tuple[object, list]] = {
     ),
 }
 
+# The head pre-solve (include/pyradmc_b200_presolve.h): host arrays throughout.
+_dp = C.POINTER(C.c_double)
+
+
+class HeadStack(C.Structure):
+    _fields_ = [
+        ("n_devices", C.c_int32),
+        ("origin", C.c_double * 3),
+        ("rotation", C.c_double * 9),
+        ("kind", _ip), ("z_top", _dp), ("z_bottom", _dp),
+        ("jaw_axis", _ip), ("jaw_edge_neg", _dp), ("jaw_edge_pos", _dp), ("jaw_focused", _ip),
+        ("mlc_tip_radius", _dp), ("mlc_focused_sides", _ip), ("mlc_n_pairs", _ip),
+        ("mlc_edges_off", _ip), ("mlc_tips_off", _ip),
+        ("leaf_edges_v", _dp), ("n_leaf_edges", C.c_int64),
+        ("tips_neg", _dp), ("tips_pos", _dp), ("n_tips", C.c_int64),
+    ]
+
+
+class HeadMu(C.Structure):
+    _fields_ = [("n_rows", C.c_int32), ("n_table", C.c_int32), ("log_energy", _dp),
+                ("log_total", _dp), ("log_compton", _dp)]
+
+
+class HeadParams(C.Structure):
+    _fields_ = [("first_compton", C.c_int32), ("has_air", C.c_int32), ("air_row", C.c_int32),
+                ("pad_", C.c_int32), ("air_z_start", C.c_double), ("air_z_end", C.c_double),
+                ("exit_z", C.c_double), ("pcut", C.c_double), ("ecut", C.c_double),
+                ("weight_floor", C.c_double), ("seed", C.c_uint64)]
+
+
+SIGNATURES.update({
+    "pmc_head_path_lengths": (C.c_int, [C.POINTER(HeadStack), C.c_int64, _fp, _fp, C.c_int32, _fp]),
+    "pmc_presolve_head": (C.c_int, [C.POINTER(HeadStack), C.POINTER(HeadMu), C.POINTER(HeadParams),
+                                    C.c_int64, _fp, _fp, _fp, _fp, C.c_int64, _ip, _fp, _fp, _fp, _fp,
+                                    _lp, _dp]),
+})
+
 # The denoiser's entry points (include/pyradmc_b200_denoise.h); every pointer is
 # a device address.
 _v = C.c_void_p

@@ -1,8 +1,8 @@
 """Build the sm_100a shared library of the B200 backend, in-tree.
 
 ``python -m pyradmc_b200.build`` compiles each translation unit in ``csrc/``
-(``pmc_runtime.cu``, which includes every transport kernel header, and
-``denoise.cu``) with nvcc for ``sm_100a``, in parallel, and links them into
+(``pmc_runtime.cu``, which includes every transport kernel header,
+``denoise.cu`` and ``pmc_presolve.cu``) with nvcc for ``sm_100a``, in parallel, and links them into
 ``_lib/libpmc_b200.so``.  The library is rebuilt only when a source is newer than
 it, unless ``force`` is set.
 """
@@ -33,7 +33,7 @@ NVCC_FLAGS = [
     "-Xcompiler",
     "-fPIC",
 ]
-UNITS = ("pmc_runtime.cu", "denoise.cu")
+UNITS = ("pmc_runtime.cu", "denoise.cu", "pmc_presolve.cu")
 
 
 def nvcc() -> str:

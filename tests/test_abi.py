@@ -17,10 +17,11 @@ from tests.conftest import ROOT, cuda_available
 
 HEADER = ROOT / "include" / "pyradmc_b200.h"
 DENOISE_HEADER = ROOT / "include" / "pyradmc_b200_denoise.h"
+PRESOLVE_HEADER = ROOT / "include" / "pyradmc_b200_presolve.h"
 
 
 def declared_symbols() -> set[str]:
-    text = HEADER.read_text() + DENOISE_HEADER.read_text()
+    text = HEADER.read_text() + DENOISE_HEADER.read_text() + PRESOLVE_HEADER.read_text()
     return set(re.findall(r"\b(pm[cd]_[a-z0-9_]+)\s*\(", text)) - {"pmc_progress_fn"}
 
 
@@ -52,8 +53,12 @@ def test_ctypes_structs_match_the_c_layout(tmp_path):
         "pmc_run_params": _lib.RunParams,
         "pmc_books": _lib.Books,
         "pmc_counters": _lib.Counters,
+        "pmc_head_stack": _lib.HeadStack,
+        "pmc_head_mu": _lib.HeadMu,
+        "pmc_head_params": _lib.HeadParams,
     }
-    lines = ['#include <stdio.h>', '#include <stddef.h>', f'#include "{HEADER}"', "int main(void){"]
+    lines = ['#include <stdio.h>', '#include <stddef.h>', f'#include "{HEADER}"',
+             f'#include "{PRESOLVE_HEADER}"', "int main(void){"]
     for cname, py in structs.items():
         lines.append(f'printf("{cname} %zu\\n", sizeof({cname}));')
         for field, _ in py._fields_:
