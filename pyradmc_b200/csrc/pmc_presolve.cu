@@ -454,8 +454,7 @@ struct Arena {
         if (d && n && cudaMemcpy(d, src, sizeof(T) * n, cudaMemcpyHostToDevice) != cudaSuccess) return nullptr;
         return d;
     }
-    template <typename T>
-    T* upload_f32(const double* src, size_t n) {  // float64 host array -> float32 device array
+    float* upload_f32(const double* src, size_t n) {  // float64 host array -> float32 device array
         std::vector<float> f(n);
         for (size_t i = 0; i < n; ++i) f[i] = (float)src[i];
         return upload(f.data(), n);
@@ -489,22 +488,22 @@ int upload_stack(Arena& a, const pmc_head_stack* s, Stack& S) {
     for (int k = 0; k < 9; ++k) S.rot[k] = (float)s->rotation[k];
     const size_t n = (size_t)s->n_devices;
     S.kind = a.upload(s->kind, n);
-    S.z_top = a.upload_f32<float>(s->z_top, n);
-    S.z_bottom = a.upload_f32<float>(s->z_bottom, n);
+    S.z_top = a.upload_f32(s->z_top, n);
+    S.z_bottom = a.upload_f32(s->z_bottom, n);
     S.jaw_axis = a.upload(s->jaw_axis, n);
-    S.jaw_neg = a.upload_f32<float>(s->jaw_edge_neg, n);
-    S.jaw_pos = a.upload_f32<float>(s->jaw_edge_pos, n);
+    S.jaw_neg = a.upload_f32(s->jaw_edge_neg, n);
+    S.jaw_pos = a.upload_f32(s->jaw_edge_pos, n);
     S.jaw_focused = a.upload(s->jaw_focused, n);
-    S.tip_radius = a.upload_f32<float>(s->mlc_tip_radius, n);
+    S.tip_radius = a.upload_f32(s->mlc_tip_radius, n);
     S.focused_sides = a.upload(s->mlc_focused_sides, n);
     S.n_pairs = a.upload(s->mlc_n_pairs, n);
     S.edges_off = a.upload(s->mlc_edges_off, n);
     S.tips_off = a.upload(s->mlc_tips_off, n);
     const size_t ne = (size_t)(s->n_leaf_edges > 0 ? s->n_leaf_edges : 0);
     const size_t nt = (size_t)(s->n_tips > 0 ? s->n_tips : 0);
-    S.leaf_edges = ne ? a.upload_f32<float>(s->leaf_edges_v, ne) : a.alloc<float>(1);
-    S.tips_neg = nt ? a.upload_f32<float>(s->tips_neg, nt) : a.alloc<float>(1);
-    S.tips_pos = nt ? a.upload_f32<float>(s->tips_pos, nt) : a.alloc<float>(1);
+    S.leaf_edges = ne ? a.upload_f32(s->leaf_edges_v, ne) : a.alloc<float>(1);
+    S.tips_neg = nt ? a.upload_f32(s->tips_neg, nt) : a.alloc<float>(1);
+    S.tips_pos = nt ? a.upload_f32(s->tips_pos, nt) : a.alloc<float>(1);
     const bool ok = S.kind && S.z_top && S.z_bottom && S.jaw_axis && S.jaw_neg && S.jaw_pos && S.jaw_focused &&
                     S.tip_radius && S.focused_sides && S.n_pairs && S.edges_off && S.tips_off && S.leaf_edges &&
                     S.tips_neg && S.tips_pos;
@@ -559,8 +558,8 @@ extern "C" int pmc_presolve_head(const pmc_head_stack* stack, const pmc_head_mu*
     M.n_table = mu->n_table;
     M.log_e0 = (float)mu->log_energy[0];
     M.inv_dlog = (float)((mu->n_table - 1) / span);
-    M.log_total = a.upload_f32<float>(mu->log_total, (size_t)mu->n_rows * mu->n_table);
-    M.log_compton = a.upload_f32<float>(mu->log_compton, (size_t)mu->n_rows * mu->n_table);
+    M.log_total = a.upload_f32(mu->log_total, (size_t)mu->n_rows * mu->n_table);
+    M.log_compton = a.upload_f32(mu->log_compton, (size_t)mu->n_rows * mu->n_table);
     Params P{};
     P.first_compton = fc;
     P.has_air = air;
