@@ -604,6 +604,52 @@ def parity_block(device):
     return out
 
 
+def presolve_leg(device):
+    """The treatment-head pre-solve (pyradmc_b200.presolve) on the case of
+    tests/golden/presolve_case.py — a jaw pair, a three-pair MLC and an air
+    column in front of a 6 MV-like fan: the reference fixture's totals
+    (pyRadMC's host pre-solve, tests/golden/make_presolve_golden.py) against
+    the GPU's at 1.2e5 primaries, and the throughput of presolve_head_device
+    (host arrays in, phase space out, wall clock) at 4e6 primaries."""
+    import time
+
+    from pyradmc_b200 import presolve as PS
+    from tests.golden import presolve_case as case
+
+    g = np.load(ROOT / "tests" / "golden" / "presolve_golden.npz")
+    names = [f for f in PS.CompiledHeadStack.__dataclass_fields__ if f not in ("materials", "densities", "_keep")]
+    stack = PS.CompiledHeadStack(**{n: g[f"s1_{n}"] for n in names},
+                                 materials=tuple(int(m) for m in g["s1_materials"]),
+                                 densities=tuple(float(d) for d in g["s1_densities"]))
+    mu = PS.HeadMuTables(g["mu_log_energy"], g["mu_log_total"], g["mu_log_compton"])
+    kw = dict(exit_z=case.AIR_EXIT_Z, stack=stack, air=PS.AirColumn(**case.AIR), mode="first_compton",
+              device=device, mu_tables=mu)
+    ps = PS.presolve_head_device(case.FanSource(), n_histories=case.N, seed=case.SEED, **kw)
+    c = ps.columns()
+    w, e = c["weight"].astype(np.float64), c["energy"].astype(np.float64)
+    host = g["air_totals"]
+    parity = {"particles": [len(ps), int(host[0])], "weight": [float(w.sum()), float(host[1])],
+              "weight_energy": [float((w * e).sum()), float(host[2])],
+              "electrons": [int(np.count_nonzero(c["particle_type"] == 2)), int(host[4])]}
+    n = 4_000_000
+    cols = case.FanSource().sample_batch(case.SEED, 0, n)
+
+    class Sampled:  # the same primaries every call: the timing excludes the NumPy sampler
+        max_energy = case.FanSource.max_energy
+
+        def sample_batch(self, seed, offset, m):
+            return cols
+
+    PS.presolve_head_device(Sampled(), n_histories=n, seed=1, **kw)
+    t0 = time.perf_counter()
+    out = PS.presolve_head_device(Sampled(), n_histories=n, seed=2, **kw)
+    seconds = time.perf_counter() - t0
+    return {"case": "jaw pair + 3-pair MLC + air column, first Compton", "parity_vs_host": parity,
+            "primaries": n, "exit_particles": len(out), "seconds": seconds,
+            "primaries_per_s": n / seconds,
+            "reference_host_rate": "~1e5 rays/s with an MLC, one core (geometry/head.py:56-59)"}
+
+
 DEN_GROUP = 25  # columns per group when MC and denoising overlap across groups
 DEN_LATERALS = (64, 48)  # lateral window sizes tried (the network trains on 64); the narrowest reaching 2 % is timed
 PLAN_WINDOW = (64, 64, 128)  # lateral x lateral x depth chunk of the plan's denoising windows
@@ -931,6 +977,7 @@ def b200_arm(args, world, rank, local):
     den = None if args.no_denoiser or world > 1 else denoiser_leg(
         args, engine, source, counts, stream, device, total_ms / args.steps / 1e3)
     parity = parity_block(device) if world == 1 else None
+    presolve = presolve_leg(device) if world == 1 else None
     plan = None
     if not args.no_plan and world == 1:
         engine.drop_uploads()
@@ -977,6 +1024,7 @@ def b200_arm(args, world, rank, local):
         "denoiser": den,
         "plan": plan,
         "parity": parity,
+        "presolve": presolve,
         "e2e": {"value": e2e_value, "unit": "histories/s",
                 "h2d_bytes_per_step": int(np.median(h2d)), "d2h_bytes_per_step": int(np.median(d2h)),
                 "ms_per_step": e2e_total / args.steps},
