@@ -61,6 +61,12 @@ extern "C" {
  * floor(r * n_records), r a 64-bit draw of its own stream, the per-history
  * sampling of PhaseSpaceSource.emit (geometry/phasespace.py:546). */
 #define PMC_SRC_PHASESPACE 4
+/* The same, with the up_* arrays already in the engine device's memory (a
+ * head pre-solve's output, pmc_presolve_head with outputs on the device): no
+ * upload and no host check; every up_kind must be PMC_PHOTON, PMC_ELECTRON or
+ * PMC_POSITRON, and the arrays must stay valid until the call returns (the
+ * hand-off of generate_from_exit_buffer, kernels.py:1963-2032). */
+#define PMC_SRC_PHASESPACE_DEVICE 5
 
 /* Beamlet generators: generate_beamlet_lattice (kernels.py:2248),
  * generate_spectral_beamlets (kernels.py:2322), per-beamlet records (fans and

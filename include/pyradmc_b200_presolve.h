@@ -86,7 +86,8 @@ typedef struct pmc_head_params {
     int32_t first_compton;        /* 0 attenuation only, 1 forced first Compton */
     int32_t has_air;
     int32_t air_row;              /* mu row of the air column */
-    int32_t pad_;
+    int32_t outputs_on_device;    /* 1: the out_* arrays of pmc_presolve_head are device
+                                     pointers of the current device (no copy back) */
     double air_z_start, air_z_end;
     double exit_z;
     double pcut, ecut;
@@ -102,11 +103,11 @@ int pmc_head_path_lengths(const pmc_head_stack* stack, int64_t n, const float* p
                           int32_t from_origin, float* out);
 
 /* The pre-solve of n primaries (host arrays: energy [n], pos [n][3], dir [n][3],
- * weight [n], all photons) into at most `capacity` exit-plane particles (host
- * arrays: kind [capacity] with 1 photon, 2 electron, energy, pos [capacity][3],
- * dir, weight).  *count = particles written; *dropped = dropped weight x
- * energy (MeV).  capacity >= n * (1 + first_compton * (1 + 2 * has_air))
- * always suffices. */
+ * weight [n], all photons) into at most `capacity` exit-plane particles (arrays
+ * kind [capacity] with 1 photon, 2 electron, energy, pos [capacity][3], dir,
+ * weight: host arrays, or device arrays when params->outputs_on_device).
+ * *count = particles written; *dropped = dropped weight x energy (MeV).
+ * capacity >= n * (1 + first_compton * (1 + 2 * has_air)) always suffices. */
 int pmc_presolve_head(const pmc_head_stack* stack, const pmc_head_mu* mu, const pmc_head_params* params,
                       int64_t n, const float* energy, const float* pos, const float* dir,
                       const float* weight, int64_t capacity, int32_t* out_kind, float* out_energy,

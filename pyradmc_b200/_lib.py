@@ -25,6 +25,7 @@ PMC_ERR_CAPACITY = -8
 
 PMC_PHOTON, PMC_ELECTRON, PMC_POSITRON = 0, 1, 2
 PMC_SRC_PENCIL, PMC_SRC_PARALLEL, PMC_SRC_SPECTRAL, PMC_SRC_UPLOAD, PMC_SRC_PHASESPACE = 0, 1, 2, 3, 4
+PMC_SRC_PHASESPACE_DEVICE = 5
 PMC_BEAMLET_LATTICE, PMC_BEAMLET_SPECTRAL, PMC_BEAMLET_RECORDS, PMC_BEAMLET_UPLOAD = 0, 1, 2, 3
 
 _dp = C.POINTER(C.c_double)
@@ -299,7 +300,7 @@ class HeadMu(C.Structure):
 
 class HeadParams(C.Structure):
     _fields_ = [("first_compton", C.c_int32), ("has_air", C.c_int32), ("air_row", C.c_int32),
-                ("pad_", C.c_int32), ("air_z_start", C.c_double), ("air_z_end", C.c_double),
+                ("outputs_on_device", C.c_int32), ("air_z_start", C.c_double), ("air_z_end", C.c_double),
                 ("exit_z", C.c_double), ("pcut", C.c_double), ("ecut", C.c_double),
                 ("weight_floor", C.c_double), ("seed", C.c_uint64)]
 

@@ -609,11 +609,16 @@ extern "C" int pmc_presolve_head(const pmc_head_stack* stack, const pmc_head_mu*
     if (total > capacity) return PMC_ERR_CAPACITY;
     if (total == 0) return PMC_OK;
     if (!out_kind || !out_energy || !out_pos || !out_dir || !out_weight) return PMC_ERR_INVALID;
+    if (cudaMemcpy(d_offsets, offsets.data(), sizeof(long long) * sb, cudaMemcpyHostToDevice) != cudaSuccess)
+        return PMC_ERR_CUDA;
+    if (params->outputs_on_device) {  // straight into the caller's device arrays
+        Out dst{out_kind, out_energy, out_pos, out_dir, out_weight};
+        compact_slots<<<sb, kThreads>>>(slots, n_slots, d_offsets, dst);
+        return cudaGetLastError() == cudaSuccess && cudaDeviceSynchronize() == cudaSuccess ? PMC_OK : PMC_ERR_CUDA;
+    }
     Out packed{a.alloc<int>(total), a.alloc<float>(total), a.alloc<float>(3 * total), a.alloc<float>(3 * total),
                a.alloc<float>(total)};
-    if (!packed.kind || !packed.energy || !packed.pos || !packed.dir || !packed.weight ||
-        cudaMemcpy(d_offsets, offsets.data(), sizeof(long long) * sb, cudaMemcpyHostToDevice) != cudaSuccess)
-        return PMC_ERR_CUDA;
+    if (!packed.kind || !packed.energy || !packed.pos || !packed.dir || !packed.weight) return PMC_ERR_CUDA;
     compact_slots<<<sb, kThreads>>>(slots, n_slots, d_offsets, packed);
     if (cudaGetLastError() != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess) return PMC_ERR_CUDA;
     const bool ok = cudaMemcpy(out_kind, packed.kind, sizeof(int) * total, cudaMemcpyDeviceToHost) == cudaSuccess &&

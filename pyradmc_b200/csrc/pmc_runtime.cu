@@ -1196,6 +1196,20 @@ int pmc_run_forward(pmc_engine* e, const pmc_source_desc* src, const pmc_run_par
             if (!rc) rc = upload_f32(e, w, &G.up_weight);
             break;
         }
+        case PMC_SRC_PHASESPACE_DEVICE: {  // records already on this device
+            G.type = 5;
+            G.book_emitted = 1;
+            if (src->n_records < 1 || !src->up_kind || !src->up_energy || !src->up_pos || !src->up_dir ||
+                !src->up_weight)
+                return fail(e, PMC_ERR_INVALID, "device phase-space source without records");
+            G.n_records = src->n_records;
+            G.up_kind = src->up_kind;
+            G.up_energy = src->up_energy;
+            G.up_pos = src->up_pos;
+            G.up_dir = src->up_dir;
+            G.up_weight = src->up_weight;
+            break;
+        }
         case PMC_SRC_UPLOAD: {
             G.type = 3;
             G.book_emitted = 1;

@@ -788,6 +788,25 @@ class B200Engine:
             src.v_axis[:] = [float(v) for v in source.v_axis]
             src.width_u = float(source.width_u)
             src.width_v = float(source.width_v)
+        elif name == "DevicePhaseSpace" and hasattr(source, "energy"):
+            # a pre-solve's phase space already on the device (presolve.py):
+            # the records are read in place, no copy to the host and back
+            import torch
+
+            dev = torch.device(self.device)
+            if torch.device(source.device) != dev:
+                raise ValueError(f"the phase space lives on {source.device}, the run on {dev}")
+            kind = (source.particle_type - 1).to(torch.int32).contiguous()  # IAEA code -> PMC_* kind
+            cols = [t.contiguous() for t in (source.energy, source.pos, source.dir, source.weight)]
+            keep += [kind, *cols]
+            dptr = lambda t, ct: C.cast(C.c_void_p(t.data_ptr()), C.POINTER(ct))  # noqa: E731
+            src.type = _lib.PMC_SRC_PHASESPACE_DEVICE
+            src.n_records = int(kind.shape[0])
+            src.up_kind = dptr(kind, C.c_int32)
+            src.up_energy = dptr(cols[0], C.c_float)
+            src.up_pos = dptr(cols[1], C.c_float)
+            src.up_dir = dptr(cols[2], C.c_float)
+            src.up_weight = dptr(cols[3], C.c_float)
         elif name in ("PhaseSpaceSource", "InMemoryPhaseSpaceSource") and hasattr(source, "columns"):
             # The whole phase space resident on the device, one record drawn per
             # history from its own stream (PhaseSpaceSource.emit, geometry/phasespace.py:546).

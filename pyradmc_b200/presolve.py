@@ -172,17 +172,46 @@ def resolve_presolve(stack, air, exit_z: float, mode: str) -> str:
     return "first_compton" if mode == "auto" else mode
 
 
+class DevicePhaseSpace:
+    """A pre-solve's exit-plane phase space kept on its GPU (the analogue of
+    pyRadMC's DevicePhaseSpace, backends/warp/presolve.py:710): torch tensors
+    particle_type (IAEA codes, int32), energy, pos [n, 3], dir [n, 3] and
+    weight (float32), already normalized per original primary.  B200Engine.run
+    transports it without a copy to the host; ``columns()`` copies it back."""
+
+    def __init__(self, particle_type, energy, pos, dirs, weight, max_energy: float):
+        self.particle_type, self.energy, self.pos, self.dir, self.weight = (
+            particle_type, energy, pos, dirs, weight)
+        self.max_energy = float(max_energy)
+        self.device = str(energy.device)
+
+    def __len__(self) -> int:
+        return int(self.energy.shape[0])
+
+    def columns(self) -> dict:
+        pos, d = self.pos.cpu().numpy().astype(np.float64), self.dir.cpu().numpy().astype(np.float64)
+        d /= np.linalg.norm(d, axis=1, keepdims=True)
+        return {"particle_type": self.particle_type.cpu().numpy(), "energy": self.energy.cpu().numpy().astype(np.float64),
+                "x": pos[:, 0], "y": pos[:, 1], "z": pos[:, 2], "ux": d[:, 0], "uy": d[:, 1], "uz": d[:, 2],
+                "weight": self.weight.cpu().numpy().astype(np.float64)}
+
+    def to_phase_space(self) -> InMemoryPhaseSpaceSource:
+        return InMemoryPhaseSpaceSource(**self.columns())
+
+
 def presolve_head_device(source, *, cross_sections=None, n_histories: int, seed: int, exit_z: float,
                          stack, air: AirColumn | None = None, mode: str = "auto",
                          device: str = "cuda:0", pcut: float = PCUT_MEV, ecut: float = ECUT_MEV,
                          weight_floor: float = 1.0e-3, e_min: float = 0.010, n_table: int = 512,
-                         mu_tables: HeadMuTables | None = None,
+                         mu_tables: HeadMuTables | None = None, return_device_source: bool = False,
                          return_dropped: bool = False):
     """Pre-solve the head on the GPU and return the exit-plane phase space
     (presolve.py:572-687's arguments and contract; ``device`` selects the
-    CUDA device).  ``mu_tables`` replaces the tables built from
-    ``cross_sections``; ``return_dropped`` also returns the dropped
-    weight x energy (MeV)."""
+    CUDA device).  ``return_device_source`` keeps the population on the device
+    as a :class:`DevicePhaseSpace` that the engine transports with no copy
+    back (the reference's return_device_source).  ``mu_tables`` replaces the
+    tables built from ``cross_sections``; ``return_dropped`` also returns the
+    dropped weight x energy (MeV)."""
     import torch
 
     compiled = stack if isinstance(stack, CompiledHeadStack) else (
@@ -210,33 +239,56 @@ def presolve_head_device(source, *, cross_sections=None, n_histories: int, seed:
     weight = f32(columns["weight"])
     fc = 1 if resolved == "first_compton" else 0
     capacity = n * (1 + fc * (1 + 2 * (air is not None)))
-    out_kind = np.empty(capacity, dtype=np.int32)
-    out_e = np.empty(capacity, dtype=np.float32)
-    out_p = np.empty((capacity, 3), dtype=np.float32)
-    out_d = np.empty((capacity, 3), dtype=np.float32)
-    out_w = np.empty(capacity, dtype=np.float32)
+    if return_device_source:  # the compaction writes straight into these device tensors
+        dev = torch.device(device)
+        t_kind = torch.empty(capacity, dtype=torch.int32, device=dev)
+        t_e = torch.empty(capacity, dtype=torch.float32, device=dev)
+        t_p = torch.empty((capacity, 3), dtype=torch.float32, device=dev)
+        t_d = torch.empty((capacity, 3), dtype=torch.float32, device=dev)
+        t_w = torch.empty(capacity, dtype=torch.float32, device=dev)
+        as_ptr = lambda t, ct: C.cast(C.c_void_p(t.data_ptr()), C.POINTER(ct))  # noqa: E731
+        outs = (as_ptr(t_kind, C.c_int32), as_ptr(t_e, C.c_float), as_ptr(t_p, C.c_float),
+                as_ptr(t_d, C.c_float), as_ptr(t_w, C.c_float))
+    else:
+        out_kind = np.empty(capacity, dtype=np.int32)
+        out_e = np.empty(capacity, dtype=np.float32)
+        out_p = np.empty((capacity, 3), dtype=np.float32)
+        out_d = np.empty((capacity, 3), dtype=np.float32)
+        out_w = np.empty(capacity, dtype=np.float32)
+        outs = (_lib.ptr(out_kind, C.c_int32), _lib.ptr(out_e, C.c_float), _lib.ptr(out_p, C.c_float),
+                _lib.ptr(out_d, C.c_float), _lib.ptr(out_w, C.c_float))
     cs = compiled.to_c()
     mu, keep = mu_tables.to_c()
     params = _lib.HeadParams(first_compton=fc, has_air=int(air is not None), air_row=air_row,
                              air_z_start=float(air.z_start) if air else 0.0,
                              air_z_end=float(air.z_end) if air else 0.0, exit_z=float(exit_z),
                              pcut=float(pcut), ecut=float(ecut), weight_floor=float(weight_floor),
-                             seed=int(seed) & 0xFFFFFFFFFFFFFFFF)
+                             seed=int(seed) & 0xFFFFFFFFFFFFFFFF,
+                             outputs_on_device=int(bool(return_device_source)))
     count, dropped = C.c_int64(), C.c_double()
     lib = _lib.load()
     with torch.cuda.device(torch.device(device)):
         code = lib.pmc_presolve_head(C.byref(cs), C.byref(mu), C.byref(params), n,
                                      _lib.ptr(energy, C.c_float), _lib.ptr(pos, C.c_float),
                                      _lib.ptr(dirs, C.c_float), _lib.ptr(weight, C.c_float), capacity,
-                                     _lib.ptr(out_kind, C.c_int32), _lib.ptr(out_e, C.c_float),
-                                     _lib.ptr(out_p, C.c_float), _lib.ptr(out_d, C.c_float),
-                                     _lib.ptr(out_w, C.c_float), C.byref(count), C.byref(dropped))
+                                     *outs, C.byref(count), C.byref(dropped))
     del keep
     if code != _lib.PMC_OK:
         raise RuntimeError(f"pmc_presolve_head failed ({code})")
     k = int(count.value)
     if k == 0:
         raise ValueError("the pre-solve kept no particles; check the geometry and cutoffs")
+    if return_device_source:
+        # the host path's arithmetic on the device: directions renormalized
+        # and weights scaled per original primary (head.py:296-314) in
+        # float64, then rounded to float32 as the engine's upload rounds them,
+        # so both hand-offs carry the same records bit for bit
+        d64 = t_d[:k].double()
+        n2 = (d64[:, 0] * d64[:, 0] + d64[:, 1] * d64[:, 1]) + d64[:, 2] * d64[:, 2]
+        dps = DevicePhaseSpace(t_kind[:k].clone(), t_e[:k].clone(), t_p[:k].clone(),
+                               (d64 / torch.sqrt(n2).unsqueeze(1)).float(),
+                               (t_w[:k].double() * (k / n)).float(), float(source.max_energy))
+        return (dps, float(dropped.value)) if return_dropped else dps
     d = out_d[:k].astype(np.float64)
     d /= np.linalg.norm(d, axis=1, keepdims=True)  # float32 round-off
     ps = InMemoryPhaseSpaceSource(

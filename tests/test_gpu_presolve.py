@@ -131,3 +131,26 @@ def test_output_is_a_function_of_the_seed_and_the_engine_transports_it(gpu):
     assert res.dose.max() > 0
     balance = res.energy_deposited + res.energy_escaped + res.energy_unscored
     assert balance == pytest.approx(res.energy_emitted, rel=1e-4)
+
+
+def test_device_phase_space_is_transported_in_place_with_the_same_dose(gpu):
+    """return_device_source keeps the population on the GPU; the engine reads it
+    in place (PMC_SRC_PHASESPACE_DEVICE) and scores exactly the dose of the
+    same phase space copied to the host and uploaded again."""
+    from pyradmc_b200 import B200Engine
+    from pyradmc_b200.model import AnalyticWaterTables, VoxelGrid
+
+    g = golden()
+    host = _run(g, gpu, "first_compton", air=True)
+    dev = _run(g, gpu, "first_compton", air=True, return_device_source=True)
+    assert len(dev) == len(host)
+    for name in ("particle_type", "energy", "weight"):
+        np.testing.assert_allclose(dev.columns()[name], host.columns()[name], rtol=1e-6, atol=0)
+    grid = VoxelGrid.uniform_water((16, 16, 16), (1.0, 1.0, 1.0), origin=(0.0, 0.0, -4.5))
+    xs = AnalyticWaterTables(geometry_densities=grid.max_density_by_material())
+    engine = B200Engine(grid, xs, device=gpu)
+    a = engine.run(host, n_histories=40_000, n_batches=4, seed=case.SEED)
+    b = engine.run(dev, n_histories=40_000, n_batches=4, seed=case.SEED)
+    np.testing.assert_array_equal(a.dose, b.dose)
+    np.testing.assert_array_equal(a.dose_sigma, b.dose_sigma)
+    assert a.energy_emitted == b.energy_emitted
