@@ -655,13 +655,18 @@ def presolve_leg(device):
         def sample_batch(self, seed, offset, m):
             return cols
 
-    PS.presolve_head_device(Sampled(), n_histories=n, seed=1, **kw)
-    t0 = time.perf_counter()
-    out = PS.presolve_head_device(Sampled(), n_histories=n, seed=2, **kw)
-    seconds = time.perf_counter() - t0
+    rate = {}
+    for name, on_device in (("to_host", False), ("on_device", True)):
+        PS.presolve_head_device(Sampled(), n_histories=n, seed=1, return_device_source=on_device, **kw)
+        t0 = time.perf_counter()
+        out = PS.presolve_head_device(Sampled(), n_histories=n, seed=2, return_device_source=on_device, **kw)
+        rate[name] = {"seconds": time.perf_counter() - t0, "exit_particles": len(out)}
+        rate[name]["primaries_per_s"] = n / rate[name]["seconds"]
+        del out
     return {"case": "jaw pair + 3-pair MLC + air column, first Compton", "parity_vs_host": parity,
-            "primaries": n, "exit_particles": len(out), "seconds": seconds,
-            "primaries_per_s": n / seconds,
+            "primaries": n, "exit_particles": rate["to_host"]["exit_particles"],
+            "seconds": rate["to_host"]["seconds"], "primaries_per_s": rate["to_host"]["primaries_per_s"],
+            "device_source": rate["on_device"],
             "reference_host_rate": "~1e5 rays/s with an MLC, one core (geometry/head.py:56-59)"}
 
 
