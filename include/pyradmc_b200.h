@@ -67,6 +67,17 @@ extern "C" {
  * PMC_POSITRON, and the arrays must stay valid until the call returns (the
  * hand-off of generate_from_exit_buffer, kernels.py:1963-2032). */
 #define PMC_SRC_PHASESPACE_DEVICE 5
+/* The spectral fan seen through a 0..1 transmission mask on a plane rectangle
+ * (TransmissionMaskSource wrapping SpectralBeamSource, geometry/collimation.py:
+ * 987-1080 and 1205; the device twin generate_spectral_masked_beam,
+ * kernels.py:2137-2244): the four uniforms of PMC_SRC_SPECTRAL, then the ray's
+ * full line meets the mask plane and the primary's weight is the mask value
+ * there, bilinear between pixel centres and clamped in the half-pixel border.
+ * A ray parallel to the plane or crossing it outside the rectangle, or a zero
+ * value, emits nothing (the history still counts in the batch mean).  The
+ * mask_* fields describe the plane; mask[i * mask_n_v + j] is pixel i along
+ * mask_u_axis and j along mask_v_axis, every value finite and in 0..1. */
+#define PMC_SRC_SPECTRAL_MASKED 6
 
 /* Beamlet generators: generate_beamlet_lattice (kernels.py:2248),
  * generate_spectral_beamlets (kernels.py:2322), per-beamlet records (fans and
@@ -147,6 +158,11 @@ typedef struct pmc_source_desc {
     const float* up_dir;    /* [n][3] */
     const float* up_weight;
     int64_t n_records; /* PMC_SRC_PHASESPACE: records in the up_* arrays */
+    /* PMC_SRC_SPECTRAL_MASKED: the mask plane (engine frame, cm; unit axes) */
+    const double* mask; /* [mask_n_u][mask_n_v] */
+    int32_t mask_n_u, mask_n_v;
+    double mask_center[3], mask_u_axis[3], mask_v_axis[3];
+    double mask_width_u, mask_width_v;
 } pmc_source_desc;
 
 /* One beamlet of a PMC_BEAMLET_RECORDS source: a lattice rectangle

@@ -21,6 +21,7 @@ from pyradmc_b200.model import (
     SpectralBeamletSource,
     SpectralBeamSource,
     Spectrum,
+    TransmissionMaskSource,
     TransportResult,
     VoxelGrid,
     ali_rogers_varian_6mv,
@@ -44,6 +45,7 @@ __all__ = [
     "SpectralBeamSource",
     "SpectralBeamletSource",
     "Spectrum",
+    "TransmissionMaskSource",
     "TransportResult",
     "VoxelGrid",
     "ali_rogers_varian_6mv",

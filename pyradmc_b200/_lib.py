@@ -26,6 +26,7 @@ PMC_ERR_CAPACITY = -8
 PMC_PHOTON, PMC_ELECTRON, PMC_POSITRON = 0, 1, 2
 PMC_SRC_PENCIL, PMC_SRC_PARALLEL, PMC_SRC_SPECTRAL, PMC_SRC_UPLOAD, PMC_SRC_PHASESPACE = 0, 1, 2, 3, 4
 PMC_SRC_PHASESPACE_DEVICE = 5
+PMC_SRC_SPECTRAL_MASKED = 6
 PMC_BEAMLET_LATTICE, PMC_BEAMLET_SPECTRAL, PMC_BEAMLET_RECORDS, PMC_BEAMLET_UPLOAD = 0, 1, 2, 3
 
 _dp = C.POINTER(C.c_double)
@@ -109,6 +110,14 @@ class SourceDesc(C.Structure):
         ("up_dir", _fp),
         ("up_weight", _fp),
         ("n_records", C.c_int64),
+        ("mask", _dp),
+        ("mask_n_u", C.c_int32),
+        ("mask_n_v", C.c_int32),
+        ("mask_center", _d3),
+        ("mask_u_axis", _d3),
+        ("mask_v_axis", _d3),
+        ("mask_width_u", C.c_double),
+        ("mask_width_v", C.c_double),
     ]
 
 

@@ -1117,6 +1117,41 @@ int pmc_upload_gs(pmc_engine* e, const float* values, int32_t ix0, int32_t iy0, 
     return PMC_OK;
 }
 
+// The transmission mask of a PMC_SRC_SPECTRAL_MASKED source, checked as
+// _MaskTransmission.__init__ does (geometry/collimation.py:1013-1029) and
+// uploaded in float32, the precision of the Warp twin's mask array.
+static int fill_gen_mask(pmc_engine* e, GenDesc& G, const pmc_source_desc* src) {
+    const long long nu = src->mask_n_u, nv = src->mask_n_v;
+    if (!src->mask || nu < 1 || nv < 1 || nu * nv > (1ll << 28))
+        return fail(e, PMC_ERR_INVALID, "the mask must be a non-empty 2D array, got shape (%lld, %lld)", nu, nv);
+    std::vector<float> m((size_t)(nu * nv));
+    for (long long i = 0; i < nu * nv; ++i) {
+        const double v = src->mask[i];
+        if (!std::isfinite(v) || v < 0.0 || v > 1.0)
+            return fail(e, PMC_ERR_INVALID, "mask values must be finite and within 0..1");
+        m[(size_t)i] = (float)v;
+    }
+    if (!(src->mask_width_u > 0.0) || !(src->mask_width_v > 0.0))
+        return fail(e, PMC_ERR_INVALID, "widths must be positive, got %g, %g", src->mask_width_u, src->mask_width_v);
+    const double* u = src->mask_u_axis;
+    const double* v = src->mask_v_axis;
+    const double nuu = std::sqrt(u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
+    const double nvv = std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+    if (std::fabs(nuu - 1.0) > 1e-9 || std::fabs(nvv - 1.0) > 1e-9)
+        return fail(e, PMC_ERR_INVALID, "mask axes must be unit vectors");
+    if (std::fabs(u[0] * v[0] + u[1] * v[1] + u[2] * v[2]) > 1e-9)
+        return fail(e, PMC_ERR_INVALID, "u_axis and v_axis must be orthogonal");
+    G.masked = 1;
+    G.mask_n_u = (int)nu;
+    G.mask_n_v = (int)nv;
+    G.mcx = (float)src->mask_center[0]; G.mcy = (float)src->mask_center[1]; G.mcz = (float)src->mask_center[2];
+    G.mux = (float)u[0]; G.muy = (float)u[1]; G.muz = (float)u[2];
+    G.mvx = (float)v[0]; G.mvy = (float)v[1]; G.mvz = (float)v[2];
+    G.mask_wu = (float)src->mask_width_u;
+    G.mask_wv = (float)src->mask_width_v;
+    return upload_f32(e, m, &G.mask);
+}
+
 int pmc_run_forward(pmc_engine* e, const pmc_source_desc* src, const pmc_run_params* p,
                     double* dose, double* dose_sigma, pmc_books* books) {
     if (!e || !src || !p || !dose || !dose_sigma) return PMC_ERR_INVALID;
@@ -1159,7 +1194,8 @@ int pmc_run_forward(pmc_engine* e, const pmc_source_desc* src, const pmc_run_par
             if (!rc) rc = upload_f32(e, d, &G.y_ext);
             break;
         }
-        case PMC_SRC_SPECTRAL: {
+        case PMC_SRC_SPECTRAL:
+        case PMC_SRC_SPECTRAL_MASKED: {
             G.type = 2;
             G.kind = PMC_PHOTON;
             G.book_emitted = 1;
@@ -1174,6 +1210,7 @@ int pmc_run_forward(pmc_engine* e, const pmc_source_desc* src, const pmc_run_par
             if (!rc) rc = upload_f32(e, cy, &G.cy);
             if (!rc) rc = upload_f32(e, cz, &G.cz);
             if (!rc) rc = fill_gen_spectrum(e, G, src->n_bins, src->edges, src->cdf);
+            if (!rc && src->type == PMC_SRC_SPECTRAL_MASKED) rc = fill_gen_mask(e, G, src);
             break;
         }
         case PMC_SRC_PHASESPACE: {

@@ -102,6 +102,12 @@ struct GenDesc {
     const BeamletRec* recs;              // records: [group][n_comp]
     const float* comp_cdf;               // records: [n_comp] mixture selection
     int n_comp;
+    int masked;                          // spectral fan through a transmission mask
+    int mask_n_u, mask_n_v;
+    const float* mask;                   // [mask_n_u * mask_n_v]
+    float mcx, mcy, mcz;                 // mask plane centre
+    float mux, muy, muz, mvx, mvy, mvz;  // mask pixel axes
+    float mask_wu, mask_wv;
 };
 
 struct Counters {
@@ -401,10 +407,45 @@ __device__ __forceinline__ bool enter_grid(const TransportParams& P, BlockBooks&
     return true;
 }
 
+// The transmission of a user mask plane along the primary's full line
+// (_MaskTransmission.factors, geometry/collimation.py:1041-1080; device twin
+// kernels.py:2190-2244): zero for a ray parallel to the plane or crossing it
+// outside the rectangle, else the bilinear value between pixel centres,
+// clamped in the half-pixel border, in the incremental form that leaves a
+// plateau of equal pixels exactly at their value.
+__device__ inline float mask_transmission(const GenDesc& G, const Particle& p) {
+    const float nx = G.muy * G.mvz - G.muz * G.mvy;
+    const float ny = G.muz * G.mvx - G.mux * G.mvz;
+    const float nz = G.mux * G.mvy - G.muy * G.mvx;
+    const float den = p.ux * nx + p.uy * ny + p.uz * nz;
+    if (den == 0.0f) return 0.0f;
+    const float t = ((G.mcx - p.x) * nx + (G.mcy - p.y) * ny + (G.mcz - p.z) * nz) / den;
+    const float ox = p.x + t * p.ux - G.mcx;
+    const float oy = p.y + t * p.uy - G.mcy;
+    const float oz = p.z + t * p.uz - G.mcz;
+    const float u = ox * G.mux + oy * G.muy + oz * G.muz;
+    const float v = ox * G.mvx + oy * G.mvy + oz * G.mvz;
+    if (!(fabsf(u) <= 0.5f * G.mask_wu && fabsf(v) <= 0.5f * G.mask_wv)) return 0.0f;
+    const int nu = G.mask_n_u, nv = G.mask_n_v;
+    float pu = (u + 0.5f * G.mask_wu) / (G.mask_wu / (float)nu) - 0.5f;
+    float pv = (v + 0.5f * G.mask_wv) / (G.mask_wv / (float)nv) - 0.5f;
+    pu = fmaxf(0.0f, fminf(pu, (float)(nu - 1)));
+    pv = fmaxf(0.0f, fminf(pv, (float)(nv - 1)));
+    const int i0 = min((int)pu, max(nu - 2, 0));
+    const int j0 = min((int)pv, max(nv - 2, 0));
+    const int i1 = min(i0 + 1, nu - 1);
+    const int j1 = min(j0 + 1, nv - 1);
+    const float fu = pu - (float)i0, fv = pv - (float)j0;
+    const float v00 = __ldg(G.mask + i0 * nv + j0), v10 = __ldg(G.mask + i1 * nv + j0);
+    const float v01 = __ldg(G.mask + i0 * nv + j1), v11 = __ldg(G.mask + i1 * nv + j1);
+    return v00 + fu * (v10 - v00) + fv * (v01 - v00) + fu * fv * (v11 - v10 - v01 + v00);
+}
+
 // ---- primary generation (kernels.py:1888-2401) -------------------------------------
 // Maps primary t of the current batch block to its beamlet and history, seeds
 // the history's stream, and samples the primary exactly as the host sources do
-// (same uniforms, same order).  Returns the particle kind.
+// (same uniforms, same order).  Returns the particle kind, or -1 when the
+// source emits nothing for this history (a masked fan's zero transmission).
 __device__ inline int generate_primary(const TransportParams& P, const GenDesc& G, int batch,
                                        unsigned long long t, Particle& p, BlockBooks& B) {
     // G is the device-resident descriptor, read field by field as needed.
@@ -469,6 +510,10 @@ __device__ inline int generate_primary(const TransportParams& P, const GenDesc& 
         const float inv = 1.0f / sqrtf(dx * dx + dy * dy + dz * dz);
         p.x = G.fx; p.y = G.fy; p.z = G.fz;
         p.ux = dx * inv; p.uy = dy * inv; p.uz = dz * inv;
+        if (G.masked) {
+            p.w = mask_transmission(G, p);
+            if (p.w == 0.0f) return -1;  // nothing emitted; the history still counts
+        }
     } else if (G.type == 4) {  // per-beamlet record (CompositeBeamletSource.emit for mixtures)
         const BeamletRec* r = G.recs + (long long)local * G.n_comp;
         if (G.n_comp > 1) {  // one uniform: the first component whose cdf reaches it
@@ -878,6 +923,7 @@ __global__ void __launch_bounds__(256) generate_kernel(TransportParams P) {
         Particle p;
         ++n_prim;
         const int kind = generate_primary(P, G, batch, t, p, B);
+        if (kind < 0) continue;
         if (kind == kPhoton) {
             if (enter_grid(P, B, p, 0.0f)) queue_suspend(P, q_ph, p, n_push);
         } else {  // charged primary: to the electron queue unchanged (it enters there)

@@ -772,12 +772,29 @@ class B200Engine:
             src.y_lo = float(source.y_range[0])
             src.y_extent = float(source.y_range[1] - source.y_range[0])
             energy_emitted = n_histories * source.max_energy
-        elif name == "SpectralBeamSource":
+        elif name == "SpectralBeamSource" or (
+                name == "TransmissionMaskSource" and _type_name(source.inner) == "SpectralBeamSource"):
+            # a spectral fan, or one seen through a transmission mask (the Warp
+            # engine's generate_spectral_masked_beam): generated in-kernel
+            masked = name == "TransmissionMaskSource"
+            if masked:
+                mask = np.ascontiguousarray(source.mask, dtype=np.float64)
+                if mask.ndim != 2:
+                    raise ValueError(f"the mask must be a non-empty 2D array, got shape {mask.shape}")
+                keep.append(mask)
+                src.mask = _lib.ptr(mask, C.c_double)
+                src.mask_n_u, src.mask_n_v = (int(n) for n in mask.shape)
+                src.mask_center[:] = [float(c) for c in source.plane_center]
+                src.mask_u_axis[:] = [float(c) for c in source.u_axis]
+                src.mask_v_axis[:] = [float(c) for c in source.v_axis]
+                src.mask_width_u = float(source.width_u)
+                src.mask_width_v = float(source.width_v)
+                source = source.inner
             spectrum = source.spectrum
             edges = np.ascontiguousarray(spectrum.edges, dtype=np.float64)
             cdf = np.ascontiguousarray(spectrum.cdf, dtype=np.float64)
             keep += [edges, cdf]
-            src.type = _lib.PMC_SRC_SPECTRAL
+            src.type = _lib.PMC_SRC_SPECTRAL_MASKED if masked else _lib.PMC_SRC_SPECTRAL
             src.kind = _lib.PMC_PHOTON
             src.n_bins = int(cdf.size)
             src.edges = _lib.ptr(edges, C.c_double)

@@ -58,6 +58,7 @@ __all__ = [
     "SpectralBeamSource",
     "SpectralBeamletSource",
     "Spectrum",
+    "TransmissionMaskSource",
     "TransportResult",
     "VoxelGrid",
     "ali_rogers_varian_6mv",
@@ -475,6 +476,50 @@ class SpectralBeamletSource:
     width_v = property(lambda self: self._fan.width_v)
     u_axis = property(lambda self: self._fan.u_axis)
     v_axis = property(lambda self: self._fan.v_axis)
+
+
+class TransmissionMaskSource:
+    """A source shaped by a 0..1 transmission mask on a plane rectangle
+    (geometry/collimation.py:1205, the model :987-1080): each primary of
+    ``inner`` carries the mask value where its full line crosses the plane as
+    its weight; ``mask[i, j]`` is pixel i along ``u_axis`` and j along
+    ``v_axis``.  The engine generates it in-kernel when ``inner`` is a
+    SpectralBeamSource, as pyRadMC's Warp engine does."""
+
+    def __init__(self, inner, *, mask, plane_center, width_u, width_v,
+                 u_axis=(1.0, 0.0, 0.0), v_axis=(0.0, 1.0, 0.0)) -> None:
+        values = np.array(mask, dtype=np.float64)
+        if values.ndim != 2 or values.size == 0:
+            raise ValueError(f"the mask must be a non-empty 2D array, got shape {values.shape}")
+        if not np.all(np.isfinite(values)) or values.min() < 0.0 or values.max() > 1.0:
+            raise ValueError("mask values must be finite and within 0..1")
+        if width_u <= 0.0 or width_v <= 0.0:
+            raise ValueError(f"widths must be positive, got {width_u}, {width_v}")
+        u = _unit(u_axis, "u_axis")
+        v = _unit(v_axis, "v_axis")
+        if abs(u[0] * v[0] + u[1] * v[1] + u[2] * v[2]) > 1.0e-9:
+            raise ValueError("u_axis and v_axis must be orthogonal")
+        self._inner = inner
+        self._mask = values
+        self._center = tuple(float(c) for c in plane_center)
+        self._widths = (float(width_u), float(width_v))
+        self._axes = (u, v)
+
+    inner = property(lambda self: self._inner)
+    max_energy = property(lambda self: self._inner.max_energy)
+    mask = property(lambda self: self._mask)
+    plane_center = property(lambda self: self._center)
+    width_u = property(lambda self: self._widths[0])
+    width_v = property(lambda self: self._widths[1])
+    u_axis = property(lambda self: self._axes[0])
+    v_axis = property(lambda self: self._axes[1])
+
+
+def _unit(v, name: str) -> tuple[float, float, float]:
+    n = math.sqrt(sum(float(c) * float(c) for c in v))
+    if n <= 0.0:
+        raise ValueError(f"{name} must be a nonzero vector")
+    return (float(v[0]) / n, float(v[1]) / n, float(v[2]) / n)
 
 
 def _selection_cdf(weights) -> np.ndarray:

@@ -87,7 +87,8 @@ def build_case(name: str):
 
     ns = SimpleNamespace(**{name: getattr(P, name) for name in (
         "PencilBeamSource", "ParallelBeamSource", "SpectralBeamSource", "BeamletGridSource",
-        "SpectralBeamletSource", "CompositeBeamletSource")}, spectrum=P.ali_rogers_varian_6mv,
+        "SpectralBeamletSource", "CompositeBeamletSource", "TransmissionMaskSource")},
+        spectrum=P.ali_rogers_varian_6mv,
         PhaseSpaceSource=PhaseSpaceSource)
     src = make_source(case["source"], ns)
     if case.get("cross_sections") == "water_bone":

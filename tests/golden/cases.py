@@ -121,6 +121,26 @@ CASES: dict[str, dict] = {
                     width_u=1.5, width_v=1.5, u_axis=(0.0, 1.0, 0.0), v_axis=(0.0, 0.0, 1.0)),
         run=dict(n_histories_per_beamlet=8000, n_batches=8, seed=SEED, truncation=0.0),
     ),
+    # A spectral fan through a transmission mask (TransmissionMaskSource,
+    # geometry/collimation.py:1205): a 6 x 5 pixel mask with exact zeros and
+    # ones on a plane halfway to the focal spot, its u axis along y, and a
+    # rectangle narrower than the fan there, so the rim of the fan is cut.
+    "spectral_masked": dict(
+        grid=dict(shape=(16, 16, 16), spacing=(0.5, 0.5, 0.5)),
+        source=dict(kind="masked",
+                    inner=dict(kind="spectral", focal_point=(4.0, 4.0, -100.0), center=(4.0, 4.0, 0.0),
+                               width_u=6.0, width_v=6.0),
+                    mask=((1.0, 0.9, 0.6, 0.3, 0.0),
+                          (1.0, 1.0, 0.7, 0.2, 0.0),
+                          (0.8, 1.0, 1.0, 0.5, 0.1),
+                          (0.5, 0.7, 1.0, 1.0, 0.4),
+                          (0.2, 0.4, 0.8, 1.0, 1.0),
+                          (0.0, 0.1, 0.5, 0.9, 1.0)),
+                    plane_center=(4.0, 4.0, -50.0), width_u=2.4, width_v=2.4,
+                    u_axis=(0.0, 1.0, 0.0), v_axis=(1.0, 0.0, 0.0)),
+        run=dict(n_histories=80_000, n_batches=10, seed=SEED),
+        shards=10,
+    ),
     # A per-beamlet mixture (CompositeBeamletSource): beamlet j is 60 % the
     # lattice rectangle j, 40 % the spectral fan j.
     "dij_composite": dict(
@@ -140,7 +160,8 @@ def make_source(s: dict, ns):
     """A case's source built from the classes of `ns` (pyRadMC's modules or this
     package): PencilBeamSource, ParallelBeamSource, SpectralBeamSource,
     BeamletGridSource, SpectralBeamletSource, CompositeBeamletSource,
-    PhaseSpaceSource and a 6 MV spectrum factory ``spectrum()``."""
+    TransmissionMaskSource, PhaseSpaceSource and a 6 MV spectrum factory
+    ``spectrum()``."""
     kind = s["kind"]
     if kind == "parallel":
         return ns.ParallelBeamSource(s["energy"], s["z"], s["x_range"], s["y_range"])
@@ -155,6 +176,12 @@ def make_source(s: dict, ns):
         axes = {k: s[k] for k in ("u_axis", "v_axis") if k in s}
         return ns.SpectralBeamletSource(ns.spectrum(), s["focal_point"], s["centers"], s["width_u"],
                                         s["width_v"], **axes)
+    if kind == "masked":
+        import numpy as np
+
+        return ns.TransmissionMaskSource(make_source(s["inner"], ns), mask=np.asarray(s["mask"]),
+                                         plane_center=s["plane_center"], width_u=s["width_u"],
+                                         width_v=s["width_v"], u_axis=s["u_axis"], v_axis=s["v_axis"])
     if kind == "composite":
         return ns.CompositeBeamletSource([(make_source(c, ns), w) for c, w in s["components"]])
     if kind == "phasespace":

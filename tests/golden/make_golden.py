@@ -60,6 +60,7 @@ def _reference_sources():
     from types import SimpleNamespace
 
     import pyradmc.geometry.source as S
+    from pyradmc.geometry.collimation import TransmissionMaskSource
     from pyradmc.geometry.spectrum import ali_rogers_mv
 
     return SimpleNamespace(
@@ -67,6 +68,7 @@ def _reference_sources():
         SpectralBeamSource=S.SpectralBeamSource, BeamletGridSource=S.BeamletGridSource,
         SpectralBeamletSource=S.SpectralBeamletSource,
         CompositeBeamletSource=S.CompositeBeamletSource,
+        TransmissionMaskSource=TransmissionMaskSource,
         PhaseSpaceSource=_reference_phsp,
         spectrum=lambda: ali_rogers_mv("varian-6mv", e_min=0.1))
 

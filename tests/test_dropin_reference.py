@@ -166,3 +166,32 @@ def test_reference_beamlet_sources_give_the_mirror_descriptors(pyradmc):
     # the reference spectrum object and the packed one are the same histogram
     np.testing.assert_array_equal(np.asarray(ref_fan.spectrum.edges), fan.spectrum.edges)
     np.testing.assert_array_equal(np.asarray(ref_fan.spectrum.cdf), fan.spectrum.cdf)
+
+
+def test_mask_source_mirror_matches_the_reference_class(pyradmc):
+    """The engine reads a TransmissionMaskSource (geometry/collimation.py:1205)
+    through its properties alone: the mirror exposes the same values and
+    refuses the same masks with the same messages."""
+    from pyradmc.geometry.collimation import TransmissionMaskSource as Ref
+    from pyradmc.geometry.source import SpectralBeamSource
+    from pyradmc.geometry.spectrum import ali_rogers_mv
+
+    import pyradmc_b200 as P
+
+    inner_ref = SpectralBeamSource(ali_rogers_mv("varian-6mv", e_min=0.1), (4.0, 4.0, -100.0),
+                                   (4.0, 4.0, 0.0), 6.0, 6.0)
+    inner = P.SpectralBeamSource(P.ali_rogers_varian_6mv(), (4.0, 4.0, -100.0), (4.0, 4.0, 0.0), 6.0, 6.0)
+    good = dict(mask=np.linspace(0.0, 1.0, 12).reshape(3, 4), plane_center=(4.0, 4.0, -50.0),
+                width_u=2.4, width_v=3.0, u_axis=(0.0, 2.0, 0.0), v_axis=(1.0, 0.0, 0.0))
+    a, b = Ref(inner_ref, **good), P.TransmissionMaskSource(inner, **good)
+    np.testing.assert_array_equal(a.mask, b.mask)
+    for name in ("plane_center", "width_u", "width_v", "u_axis", "v_axis"):
+        assert getattr(a, name) == getattr(b, name), name
+    assert a.max_energy == b.max_energy
+    for bad in (dict(mask=np.zeros(3)), dict(mask=np.full((2, 2), 1.5)), dict(width_u=0.0),
+                dict(u_axis=(0.0, 0.0, 0.0)), dict(v_axis=(0.0, 1.0, 0.0))):
+        kw = {**good, **bad}
+        with pytest.raises(ValueError) as ref_err:
+            Ref(inner_ref, **kw)
+        with pytest.raises(ValueError, match=str(ref_err.value).replace("(", r"\(").replace(")", r"\)")):
+            P.TransmissionMaskSource(inner, **kw)

@@ -181,3 +181,67 @@ def test_resident_phase_space_is_bit_inert_to_scheduling(gpu):
     np.testing.assert_array_equal(a.dose, b.dose)
     np.testing.assert_array_equal(a.dose_sigma, b.dose_sigma)
     assert a.energy_emitted == b.energy_emitted
+
+
+def _masked(fan, mask, width=4.0, **kw):
+    axes = dict(u_axis=(0.0, 1.0, 0.0), v_axis=(1.0, 0.0, 0.0))
+    axes.update(kw)
+    return P.TransmissionMaskSource(fan, mask=mask, plane_center=(4.0, 4.0, -50.0), width_u=width,
+                                    width_v=width, **axes)
+
+
+def test_an_open_mask_is_bit_inert_and_a_closed_one_emits_nothing(gpu):
+    """The spectral fan through a transmission mask (the Warp engine's
+    generate_spectral_masked_beam, kernels.py:2137-2244).  An all-ones mask
+    whose rectangle holds the whole fan leaves every primary at weight exactly
+    1 (the incremental bilinear form is exact on a plateau), so the run is the
+    unmasked fan's bit for bit; an all-zeros mask, or a rectangle the fan
+    misses, emits nothing; a constant mask c books c times the emitted
+    energy.  The masked dose itself is pinned against pyRadMC's
+    ReferenceEngine in test_gpu_transport.py (``spectral_masked``)."""
+    grid, xs = _water()
+    engine = P.B200Engine(grid, xs)
+    fan = P.SpectralBeamSource(P.ali_rogers_varian_6mv(), (4.0, 4.0, -100.0), (4.0, 4.0, 0.0), 6.0, 6.0)
+    kw = dict(n_histories=40_000, n_batches=8, seed=SEED)
+    plain = engine.run(fan, **kw)
+    # the fan is 3 cm wide at the plane: a 4 cm rectangle holds all of it
+    opened = engine.run(_masked(fan, np.ones((7, 3))), **kw)
+    np.testing.assert_array_equal(opened.dose, plain.dose)
+    np.testing.assert_array_equal(opened.dose_sigma, plain.dose_sigma)
+    assert opened.energy_emitted == plain.energy_emitted
+    assert opened.energy_deposited == plain.energy_deposited
+    for closed in (_masked(fan, np.zeros((2, 2))),
+                   P.TransmissionMaskSource(fan, mask=np.ones((2, 2)), plane_center=(20.0, 4.0, -50.0),
+                                            width_u=4.0, width_v=4.0)):
+        res = engine.run(closed, **kw)
+        assert not res.dose.any() and res.energy_emitted == 0.0 and res.energy_deposited == 0.0
+    half = engine.run(_masked(fan, np.full((3, 4), 0.5)), **kw)
+    assert half.energy_emitted == pytest.approx(0.5 * plain.energy_emitted, rel=1e-8)
+
+
+def test_the_native_path_rejects_a_bad_mask(gpu):
+    """The C-ABI checks the mask as _MaskTransmission.__init__ does
+    (geometry/collimation.py:1013-1023), whatever object the caller hands in:
+    PMC_ERR_INVALID, a ValueError."""
+    grid, xs = _water()
+    engine = P.B200Engine(grid, xs)
+    fan = P.SpectralBeamSource(P.ali_rogers_varian_6mv(), (4.0, 4.0, -100.0), (4.0, 4.0, 0.0), 6.0, 6.0)
+
+    class TransmissionMaskSource:  # duck-typed, unchecked on the host
+        inner = fan
+        max_energy = fan.max_energy
+        plane_center = (4.0, 4.0, -50.0)
+        width_u = width_v = 4.0
+        u_axis, v_axis = (1.0, 0.0, 0.0), (0.0, 1.0, 0.0)
+
+        def __init__(self, mask, **kw):
+            self.mask = mask
+            self.__dict__.update(kw)
+
+    kw = dict(n_histories=1000, n_batches=1, seed=SEED)
+    for bad, match in ((TransmissionMaskSource(np.full((2, 2), 1.5)), "within 0..1"),
+                       (TransmissionMaskSource(np.full((2, 2), np.nan)), "within 0..1"),
+                       (TransmissionMaskSource(np.ones((2, 2)), width_u=0.0), "widths"),
+                       (TransmissionMaskSource(np.ones((2, 2)), v_axis=(0.6, 0.8, 0.0)), "orthogonal")):
+        with pytest.raises(ValueError, match=match):
+            engine.run(bad, **kw)
