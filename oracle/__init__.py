@@ -65,7 +65,10 @@ class _Source(C.Structure):
                 ("x_lo", _dp), ("x_extent", _dp), ("y_lo", _dp), ("y_extent", _dp),
                 ("n_bins", C.c_int), ("edges", _dp), ("cdf", _dp), ("focal", _d3),
                 ("u_axis", _d3), ("v_axis", _d3), ("width_u", C.c_double),
-                ("width_v", C.c_double), ("centers", _dp)]
+                ("width_v", C.c_double), ("centers", _dp), ("mask", _dp),
+                ("mask_n_u", C.c_int), ("mask_n_v", C.c_int), ("mask_center", _d3),
+                ("mask_u", _d3), ("mask_v", _d3), ("mask_width_u", C.c_double),
+                ("mask_width_v", C.c_double)]
 
 
 class _Params(C.Structure):
@@ -128,7 +131,7 @@ def run(grid, tables, gs, source, *, counts, n_batches, seed, forward=True, pcut
 
     ``grid`` needs shape/spacing/origin/density/material; ``tables`` the
     CrossSectionTables fields; ``gs`` values/ix0/iy0/bins_per_log; ``source`` is a
-    pencil, parallel, lattice, spectral or spectral-beamlet source (the same
+    pencil, parallel, lattice, spectral (optionally masked) or spectral-beamlet source (the same
     classes the engine takes).  ``counts`` gives each column's histories.
     """
     lib = load()
@@ -169,6 +172,17 @@ def run(grid, tables, gs, source, *, counts, n_batches, seed, forward=True, pcut
         keep.append(a)
         return a.ctypes.data_as(_dp)
 
+    if name == "TransmissionMaskSource" and type(source.inner).__name__ == "SpectralBeamSource":
+        # the spectral fan, its primaries weighted by the mask
+        mask = _d(source.mask)
+        keep.append(mask)
+        s.mask = mask.ctypes.data_as(_dp)
+        s.mask_n_u, s.mask_n_v = (int(n) for n in mask.shape)
+        s.mask_center[:] = list(map(float, source.plane_center))
+        s.mask_u[:] = list(map(float, source.u_axis))
+        s.mask_v[:] = list(map(float, source.v_axis))
+        s.mask_width_u, s.mask_width_v = float(source.width_u), float(source.width_v)
+        source, name = source.inner, "SpectralBeamSource"
     if name == "PencilBeamSource":
         s.type = 0
         s.energy = float(source.energy)

@@ -72,7 +72,7 @@ typedef struct {
 
 /* Source of one call: forward (one column) or a Dij group of n_cols beamlets. */
 typedef struct {
-    int type; /* 0 pencil, 1 parallel/lattice, 2 spectral fan */
+    int type; /* 0 pencil, 1 parallel/lattice, 2 spectral fan (optionally masked) */
     int kind; /* PHOTON or ELECTRON */
     double energy;
     double position[3], direction[3];
@@ -83,7 +83,45 @@ typedef struct {
     double focal[3], u_axis[3], v_axis[3];
     double width_u, width_v;
     const double* centers; /* [n_cols][3] */
+    /* spectral fan through a transmission mask (mask != NULL) */
+    const double* mask; /* [mask_n_u][mask_n_v] */
+    int mask_n_u, mask_n_v;
+    double mask_center[3], mask_u[3], mask_v[3];
+    double mask_width_u, mask_width_v;
 } o_source;
+
+/* _MaskTransmission.factors (geometry/collimation.py:1041-1080), one ray, in
+ * float64: zero off the plane's rectangle or parallel to the plane, else the
+ * clamped bilinear value between pixel centres. */
+static double mask_factor(const o_source* s, const double p[3], const double d[3]) {
+    const double* a = s->mask_u;
+    const double* b = s->mask_v;
+    const double n[3] = {a[1] * b[2] - a[2] * b[1], a[2] * b[0] - a[0] * b[2], a[0] * b[1] - a[1] * b[0]};
+    const double den = d[0] * n[0] + d[1] * n[1] + d[2] * n[2];
+    if (den == 0.0) return 0.0;
+    const double t = ((s->mask_center[0] - p[0]) * n[0] + (s->mask_center[1] - p[1]) * n[1] +
+                      (s->mask_center[2] - p[2]) * n[2]) / den;
+    double off[3];
+    for (int k = 0; k < 3; ++k) off[k] = p[k] + t * d[k] - s->mask_center[k];
+    const double u = off[0] * a[0] + off[1] * a[1] + off[2] * a[2];
+    const double v = off[0] * b[0] + off[1] * b[1] + off[2] * b[2];
+    if (!(fabs(u) <= s->mask_width_u / 2.0 && fabs(v) <= s->mask_width_v / 2.0)) return 0.0;
+    const int nu = s->mask_n_u, nv = s->mask_n_v;
+    double pu = (u + s->mask_width_u / 2.0) / (s->mask_width_u / nu) - 0.5;
+    double pv = (v + s->mask_width_v / 2.0) / (s->mask_width_v / nv) - 0.5;
+    pu = pu < 0.0 ? 0.0 : (pu > nu - 1 ? nu - 1 : pu);
+    pv = pv < 0.0 ? 0.0 : (pv > nv - 1 ? nv - 1 : pv);
+    int i0 = (int)pu, j0 = (int)pv;
+    const int ci = nu - 2 > 0 ? nu - 2 : 0, cj = nv - 2 > 0 ? nv - 2 : 0;
+    if (i0 > ci) i0 = ci;
+    if (j0 > cj) j0 = cj;
+    const int i1 = i0 + 1 < nu - 1 ? i0 + 1 : nu - 1;
+    const int j1 = j0 + 1 < nv - 1 ? j0 + 1 : nv - 1;
+    const double fu = pu - i0, fv = pv - j0;
+    const double v00 = s->mask[i0 * nv + j0], v10 = s->mask[i1 * nv + j0];
+    const double v01 = s->mask[i0 * nv + j1], v11 = s->mask[i1 * nv + j1];
+    return v00 + fu * (v10 - v00) + fv * (v01 - v00) + fu * fv * (v11 - v10 - v01 + v00);
+}
 
 typedef struct {
     int forward;
@@ -678,7 +716,11 @@ static void history(ctx_t* c, const o_source* s, int col, uint64_t key) {
         for (int a = 0; a < 3; ++a) pr.u[a] = d[a] / norm;
         memcpy(pr.p, s->focal, sizeof pr.p);
         pr.kind = PHOTON;
-        int64_t q = (int64_t)floor(pr.e * INV_QUANTUM + 0.5);
+        if (s->mask) {  /* TransmissionMaskSource: a zero factor emits nothing */
+            pr.w = mask_factor(s, pr.p, pr.u);
+            if (pr.w == 0.0) return;
+        }
+        int64_t q = (int64_t)floor(pr.w * pr.e * INV_QUANTUM + 0.5);
         __atomic_fetch_add(&c->emitted, q, __ATOMIC_RELAXED);
     }
     stack[n++] = pr;
