@@ -138,6 +138,9 @@ typedef struct pmc_scoring_desc {
 } pmc_scoring_desc;
 
 /* Open-field primary source (WarpEngine.run, engine.py:454). */
+struct pmc_head_stack;
+struct pmc_head_mu;
+
 typedef struct pmc_source_desc {
     int32_t type; /* PMC_SRC_* */
     int32_t kind; /* PMC_PHOTON or PMC_ELECTRON for the analytic beams */
@@ -163,6 +166,14 @@ typedef struct pmc_source_desc {
     int32_t mask_n_u, mask_n_v;
     double mask_center[3], mask_u_axis[3], mask_v_axis[3];
     double mask_width_u, mask_width_v;
+    /* Optional (NULL: none): a beam-limiting stack the primaries are seen
+     * through, CollimatedSource (geometry/collimation.py:1154): each analytic
+     * primary's weight is multiplied by exp(-sum_j mu_j(E) t_j), t_j the chord
+     * of its full line through device j, mu_j row j of stack_mu's log_total
+     * (macroscopic, density included; the log energies log-uniform).  A zero
+     * transmission emits nothing.  Types declared in pyradmc_b200_presolve.h. */
+    const struct pmc_head_stack* stack;
+    const struct pmc_head_mu* stack_mu;
 } pmc_source_desc;
 
 /* One beamlet of a PMC_BEAMLET_RECORDS source: a lattice rectangle
@@ -219,6 +230,11 @@ typedef struct pmc_beamlet_desc {
     /* PMC_BEAMLET_UPLOAD */
     pmc_sample_fn sample;
     void* sample_user;
+    /* Optional stack transmission of every in-kernel beamlet primary, the
+     * same fields as in pmc_source_desc: CollimatedBeamletSource,
+     * geometry/collimation.py:1185 */
+    const struct pmc_head_stack* stack;
+    const struct pmc_head_mu* stack_mu;
 } pmc_beamlet_desc;
 
 /* Run options: the keyword arguments of WarpEngine.run / run_dij plus the

@@ -6,6 +6,7 @@ and Dij compaction running as hand-written sm_100a CUDA behind the C-ABI of
 ``include/pyradmc_b200.h``.
 """
 
+from pyradmc_b200.collimation import CollimatedBeamletSource, CollimatedSource
 from pyradmc_b200.engine import B200Engine
 from pyradmc_b200.model import (
     AnalyticWaterTables,
@@ -34,6 +35,8 @@ __all__ = [
     "AnalyticWaterTables",
     "B200Engine",
     "BeamletGridSource",
+    "CollimatedBeamletSource",
+    "CollimatedSource",
     "CompositeBeamletSource",
     "ConcatenatedBeamletSource",
     "CylindricalScoringGrid",

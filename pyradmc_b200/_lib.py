@@ -118,6 +118,8 @@ class SourceDesc(C.Structure):
         ("mask_v_axis", _d3),
         ("mask_width_u", C.c_double),
         ("mask_width_v", C.c_double),
+        ("stack", C.c_void_p),
+        ("stack_mu", C.c_void_p),
     ]
 
 
@@ -174,6 +176,8 @@ class BeamletDesc(C.Structure):
         ("spectrum_cdf", _dp),
         ("sample", SAMPLE_FN),
         ("sample_user", C.c_void_p),
+        ("stack", C.c_void_p),
+        ("stack_mu", C.c_void_p),
     ]
 
 

@@ -21,6 +21,7 @@
 #include <vector>
 
 #include "../../include/pyradmc_b200.h"
+#include "../../include/pyradmc_b200_presolve.h"
 #include "pmc_common.cuh"
 #include "pmc_reduce.cuh"
 #include "pmc_transport.cuh"
@@ -1117,6 +1118,78 @@ int pmc_upload_gs(pmc_engine* e, const float* values, int32_t ix0, int32_t iy0, 
     return PMC_OK;
 }
 
+// The beam-limiting stack of a collimated source and its attenuation rows,
+// checked and uploaded in float32 (the generator's precision).  The table's
+// energies must be log-uniform (np.geomspace, as _StackTransmission builds
+// them, geometry/collimation.py:961-969).
+static int fill_gen_stack(pmc_engine* e, GenDesc& G, const pmc_head_stack* st, const pmc_head_mu* mu) {
+    if (!st) return PMC_OK;
+    const int n = st->n_devices;
+    if (n < 1 || n > pmc_head::kMaxDevices || !mu || mu->n_rows < n || mu->n_table < 2 || !mu->log_energy ||
+        !mu->log_total || !st->kind || !st->z_top || !st->z_bottom)
+        return fail(e, PMC_ERR_INVALID, "bad collimation stack or attenuation table");
+    const int nt = mu->n_table;
+    const double l0 = mu->log_energy[0], l1 = mu->log_energy[nt - 1];
+    if (!(l1 > l0)) return fail(e, PMC_ERR_INVALID, "attenuation table energies must ascend");
+    const double step = (l1 - l0) / (nt - 1);
+    for (int k = 0; k < nt; ++k)
+        if (std::fabs(mu->log_energy[k] - (l0 + k * step)) > 1e-6 * std::max(1.0, std::fabs(step)))
+            return fail(e, PMC_ERR_INVALID, "attenuation table energies must be log-uniform");
+    long long n_edges = 0, n_tips = 0;
+    for (int j = 0; j < n; ++j) {
+        if (st->kind[j] != 0 && st->kind[j] != 1) return fail(e, PMC_ERR_INVALID, "unknown device kind");
+        if (st->kind[j] == 1) {
+            const long long np_ = st->mlc_n_pairs[j];
+            n_edges = std::max(n_edges, (long long)st->mlc_edges_off[j] + np_ + 1);
+            n_tips = std::max(n_tips, (long long)st->mlc_tips_off[j] + np_);
+            if (np_ < 1 || st->mlc_edges_off[j] < 0 || st->mlc_tips_off[j] < 0)
+                return fail(e, PMC_ERR_INVALID, "bad leaf offsets");
+        }
+    }
+    if (n_edges > st->n_leaf_edges || n_tips > st->n_tips)
+        return fail(e, PMC_ERR_INVALID, "leaf offsets beyond the leaf arrays");
+    auto f32 = [](const double* a, long long m) {
+        std::vector<float> v((size_t)std::max(m, 1ll), 0.0f);
+        for (long long i = 0; i < m; ++i) v[(size_t)i] = a ? (float)a[i] : 0.0f;
+        return v;
+    };
+    auto i32 = [](const int32_t* a, long long m) {
+        std::vector<int> v((size_t)std::max(m, 1ll), 0);
+        for (long long i = 0; i < m; ++i) v[(size_t)i] = a ? a[i] : 0;
+        return v;
+    };
+    pmc_head::Stack& S = G.stack;
+    S.n = n;
+    for (int k = 0; k < 3; ++k) S.origin[k] = (float)st->origin[k];
+    for (int k = 0; k < 9; ++k) S.rot[k] = (float)st->rotation[k];
+    int rc = upload_vec(e, i32(st->kind, n), &S.kind);
+    if (!rc) rc = upload_f32(e, f32(st->z_top, n), &S.z_top);
+    if (!rc) rc = upload_f32(e, f32(st->z_bottom, n), &S.z_bottom);
+    if (!rc) rc = upload_vec(e, i32(st->jaw_axis, n), &S.jaw_axis);
+    if (!rc) rc = upload_f32(e, f32(st->jaw_edge_neg, n), &S.jaw_neg);
+    if (!rc) rc = upload_f32(e, f32(st->jaw_edge_pos, n), &S.jaw_pos);
+    if (!rc) rc = upload_vec(e, i32(st->jaw_focused, n), &S.jaw_focused);
+    if (!rc) rc = upload_f32(e, f32(st->mlc_tip_radius, n), &S.tip_radius);
+    if (!rc) rc = upload_vec(e, i32(st->mlc_focused_sides, n), &S.focused_sides);
+    if (!rc) rc = upload_vec(e, i32(st->mlc_n_pairs, n), &S.n_pairs);
+    if (!rc) rc = upload_vec(e, i32(st->mlc_edges_off, n), &S.edges_off);
+    if (!rc) rc = upload_vec(e, i32(st->mlc_tips_off, n), &S.tips_off);
+    if (!rc) rc = upload_f32(e, f32(st->leaf_edges_v, st->n_leaf_edges), &S.leaf_edges);
+    if (!rc) rc = upload_f32(e, f32(st->tips_neg, st->n_tips), &S.tips_neg);
+    if (!rc) rc = upload_f32(e, f32(st->tips_pos, st->n_tips), &S.tips_pos);
+    pmc_head::Mu& M = G.stack_mu;
+    M.n_rows = n;
+    M.n_table = nt;
+    M.log_e0 = (float)l0;
+    M.inv_dlog = (float)(1.0 / step);
+    if (!rc) rc = upload_f32(e, f32(mu->log_total, (long long)n * nt), &M.log_total);
+    M.log_compton = M.log_total;
+    if (rc) return rc;
+    G.stacked = 1;
+    G.book_emitted = 1;  // weighted primaries: the emitted energy is booked one by one
+    return PMC_OK;
+}
+
 // The transmission mask of a PMC_SRC_SPECTRAL_MASKED source, checked as
 // _MaskTransmission.__init__ does (geometry/collimation.py:1013-1029) and
 // uploaded in float32, the precision of the Warp twin's mask array.
@@ -1268,6 +1341,7 @@ int pmc_run_forward(pmc_engine* e, const pmc_source_desc* src, const pmc_run_par
         default:
             return fail(e, PMC_ERR_INVALID, "unknown source type %d", src->type);
     }
+    if (!rc) rc = fill_gen_stack(e, G, src->stack, src->stack_mu);
     if (rc) return rc;
     if (G.kind != PMC_PHOTON && G.kind != PMC_ELECTRON && G.type != 3 && G.type != 5)
         return fail(e, PMC_ERR_INVALID, "unknown primary kind %d", G.kind);
@@ -1444,6 +1518,7 @@ int pmc_run_dij(pmc_engine* e, const pmc_beamlet_desc* src, const int64_t* count
             if (!rc) rc = upload_f32(e, comp_cdf, &G.comp_cdf);
             if (!rc) rc = upload_f32(e, spec_edges, &G.edges);
             if (!rc) rc = upload_f32(e, spec_cdf, &G.cdf);
+            if (!rc) rc = fill_gen_stack(e, G, src->stack, src->stack_mu);
         }
         if (rc) return rc;
         PMC_CUDA(e, cudaMemcpyAsync(e->d_gen, &G, sizeof G, cudaMemcpyHostToDevice, e->stream));

@@ -22,6 +22,7 @@
 #include "pmc_common.cuh"
 #include "pmc_physics.cuh"
 #include "pmc_reduce.cuh"
+#include "pmc_stack.cuh"
 
 namespace pmc {
 
@@ -108,6 +109,9 @@ struct GenDesc {
     float mcx, mcy, mcz;                 // mask plane centre
     float mux, muy, muz, mvx, mvy, mvz;  // mask pixel axes
     float mask_wu, mask_wv;
+    int stacked;                         // collimated: weight by the stack transmission
+    pmc_head::Stack stack;
+    pmc_head::Mu stack_mu;               // macroscopic attenuation, one row per device
 };
 
 struct Counters {
@@ -441,6 +445,23 @@ __device__ inline float mask_transmission(const GenDesc& G, const Particle& p) {
     return v00 + fu * (v10 - v00) + fv * (v01 - v00) + fu * fv * (v11 - v10 - v01 + v00);
 }
 
+// Narrow-beam transmission of a collimated source (_StackTransmission.factors,
+// geometry/collimation.py:927-985): exp(-sum_j mu_j(E) t_j), t_j the chord of
+// the primary's full line through device j and mu_j that device's macroscopic
+// total attenuation on its log-log table.  A ray trapped in a slab has an
+// infinite chord and a zero transmission.
+__device__ inline float stack_transmission(const GenDesc& G, const Particle& p) {
+    const float x[3] = {p.x, p.y, p.z}, u[3] = {p.ux, p.uy, p.uz};
+    float lp[3], ld[3];
+    pmc_head::to_local(G.stack, x, u, lp, ld);
+    float tau = 0.0f;
+    for (int j = 0; j < G.stack.n; ++j) {
+        const float t = pmc_head::device_len(G.stack, j, lp, ld, 0);
+        if (t > 0.0f) tau += pmc_head::mu_at(G.stack_mu, G.stack_mu.log_total, j, p.e) * t;
+    }
+    return expf(-tau);
+}
+
 // ---- primary generation (kernels.py:1888-2401) -------------------------------------
 // Maps primary t of the current batch block to its beamlet and history, seeds
 // the history's stream, and samples the primary exactly as the host sources do
@@ -577,6 +598,10 @@ __device__ inline int generate_primary(const TransportParams& P, const GenDesc& 
         p.ux = __ldg(G.up_dir + 3 * ri);
         p.uy = __ldg(G.up_dir + 3 * ri + 1);
         p.uz = __ldg(G.up_dir + 3 * ri + 2);
+    }
+    if (G.stacked && G.type != 3 && G.type != 5) {  // host records carry their own weights
+        p.w *= stack_transmission(G, p);
+        if (p.w == 0.0f) return -1;
     }
     if (G.book_emitted) {
         const float latent = p.kind == kPositron ? 2.0f * kElectronMass : 0.0f;

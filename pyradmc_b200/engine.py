@@ -362,9 +362,49 @@ def _fill_general_desc(desc, source, records, sl: slice, seed: int, keep: list) 
     desc.sample = callback
 
 
+def _forward_in_kernel(source) -> bool:
+    name = _type_name(source)
+    return name in ("PencilBeamSource", "ParallelBeamSource", "SpectralBeamSource") or (
+        name == "TransmissionMaskSource" and _type_name(source.inner) == "SpectralBeamSource")
+
+
+def _attach_stack(desc, source, keep: list):
+    """Point `desc` (a pmc_source_desc or pmc_beamlet_desc) at the stack
+    transmission of a collimated `source`; the structures go into `keep`."""
+    from .collimation import stack_transmission_tables
+
+    _, stack, log_energy, log_total = stack_transmission_tables(source)
+    hs = stack.to_c()
+    arrs = [np.ascontiguousarray(log_energy, dtype=np.float64),
+            np.ascontiguousarray(log_total, dtype=np.float64)]
+    mu = _lib.HeadMu(n_rows=int(arrs[1].shape[0]), n_table=int(arrs[0].size),
+                     log_energy=_lib.ptr(arrs[0], C.c_double), log_total=_lib.ptr(arrs[1], C.c_double),
+                     log_compton=_lib.ptr(arrs[1], C.c_double))
+    keep += [stack, hs, mu, arrs]
+    desc.stack = C.cast(C.pointer(hs), C.c_void_p)
+    desc.stack_mu = C.cast(C.pointer(mu), C.c_void_p)
+
+
+def _collimated_inner(source, in_kernel):
+    """The inner source of a collimated `source` when `in_kernel(inner)` says
+    the engine generates it on the device, else None."""
+    from .collimation import stack_transmission_tables
+
+    found = stack_transmission_tables(source)
+    return found[0] if found is not None and in_kernel(found[0]) else None
+
+
+def _beamlets_in_kernel(source) -> bool:
+    name = _type_name(source)
+    return name in ("BeamletGridSource", "SpectralBeamletSource") or _records_plan(source) is not None
+
+
 def beamlet_arrays(source):
     """(per-beamlet arrays of a built-in generator or None, records plan or None):
     the host-side flattening of a beamlet source for ``pmc_run_dij``."""
+    inner = _collimated_inner(source, _beamlets_in_kernel)
+    if inner is not None:
+        return beamlet_arrays(inner)
     name = _type_name(source)
     n = int(source.n_beamlets)
     if name == "BeamletGridSource":
@@ -382,6 +422,11 @@ def beamlet_arrays(source):
 def beamlet_descriptor(source, sl: slice, seed: int, keep: list, per=None, records=None):
     """The ``pmc_beamlet_desc`` of columns `sl` of `source` (the arrays it
     points to are appended to `keep`, which must outlive the call)."""
+    inner = _collimated_inner(source, _beamlets_in_kernel)
+    if inner is not None:  # the inner generator, its primaries weighted by the stack
+        desc = beamlet_descriptor(inner, sl, seed, keep, per, records)
+        _attach_stack(desc, source, keep)
+        return desc
     if per is None and records is None:
         per, records = beamlet_arrays(source)
     desc = _lib.BeamletDesc(n_beamlets=sl.stop - sl.start)
@@ -740,6 +785,9 @@ class B200Engine:
                 f"n_histories={n_histories} not divisible by n_batches={n_batches}; "
                 "unequal batches would weight batch means inconsistently"
             )
+        collimated = source
+        source = _collimated_inner(source, _forward_in_kernel) or source
+        collimated = collimated if source is not collimated else None
         name = _type_name(source)
         in_kernel = name in ("PencilBeamSource", "ParallelBeamSource")
         if in_kernel and primary_kind not in ("photon", "electron"):
@@ -861,6 +909,9 @@ class B200Engine:
             src.up_weight = _lib.ptr(weight, C.c_float)
         else:
             raise ValueError(f"unsupported source type {name}")
+        if collimated is not None:  # weights from the stack: emitted energy booked per primary
+            _attach_stack(src, collimated, keep)
+            energy_emitted = None
 
         params = self._params(
             n_histories=n_histories, n_batches=n_batches, seed=seed, pcut=pcut, ecut=ecut,

@@ -67,6 +67,22 @@ def gpu():
     return "cuda:0"
 
 
+def collimated(inner, beamlets: bool):
+    """`inner` seen through the collimated cases' stack, with the stack and
+    transmission table pyRadMC built (tests/golden/collimation.npz)."""
+    import pyradmc_b200 as P
+    from pyradmc_b200.presolve import CompiledHeadStack
+
+    with np.load(GOLDEN / "collimation.npz") as z:
+        f = {k: z[k] for k in z.files}
+    names = [n for n in CompiledHeadStack.__dataclass_fields__ if n not in ("materials", "densities", "_keep")]
+    stack = CompiledHeadStack(**{n: f[f"stack_{n}"] for n in names},
+                              materials=tuple(int(m) for m in f["stack_materials"]),
+                              densities=tuple(float(d) for d in f["stack_densities"]))
+    cls = P.CollimatedBeamletSource if beamlets else P.CollimatedSource
+    return cls.from_tables(inner, stack, f["log_energy"], f["log_total"])
+
+
 def build_case(name: str):
     """(grid, cross_sections, source, run kwargs) of a golden case, on this package's types."""
     import pyradmc_b200 as P
@@ -89,7 +105,7 @@ def build_case(name: str):
         "PencilBeamSource", "ParallelBeamSource", "SpectralBeamSource", "BeamletGridSource",
         "SpectralBeamletSource", "CompositeBeamletSource", "TransmissionMaskSource")},
         spectrum=P.ali_rogers_varian_6mv,
-        PhaseSpaceSource=PhaseSpaceSource)
+        PhaseSpaceSource=PhaseSpaceSource, collimated=collimated)
     src = make_source(case["source"], ns)
     if case.get("cross_sections") == "water_bone":
         xs = P.PackedCrossSections(GOLDEN / "pack_water_bone.npz")

@@ -141,6 +141,27 @@ CASES: dict[str, dict] = {
         run=dict(n_histories=80_000, n_batches=10, seed=SEED),
         shards=10,
     ),
+    # A spectral fan seen through a beam-limiting stack (CollimatedSource,
+    # geometry/collimation.py:1154): the stack of COLLIMATION weights every
+    # primary by its narrow-beam transmission.
+    "collimated_spectral": dict(
+        grid=dict(shape=(16, 16, 16), spacing=(0.5, 0.5, 0.5)),
+        source=dict(kind="collimated",
+                    inner=dict(kind="spectral", focal_point=(4.0, 4.0, -100.0), center=(4.0, 4.0, 0.0),
+                               width_u=6.0, width_v=6.0)),
+        run=dict(n_histories=80_000, n_batches=10, seed=SEED),
+        shards=10,
+    ),
+    # Four spectral beamlets through the same stack (CollimatedBeamletSource,
+    # :1185): each column carries its own transmission pattern.
+    "dij_collimated": dict(
+        grid=dict(shape=(16, 16, 16), spacing=(0.5, 0.5, 0.5)),
+        source=dict(kind="collimated_beamlets",
+                    inner=dict(kind="spectral_beamlets", focal_point=(4.0, 4.0, -100.0),
+                               centers=((3.0, 3.0, 0.0), (5.0, 3.0, 0.0), (3.0, 5.0, 0.0), (5.0, 5.0, 0.0)),
+                               width_u=2.0, width_v=2.0)),
+        run=dict(n_histories_per_beamlet=8000, n_batches=8, seed=SEED, truncation=0.0),
+    ),
     # A per-beamlet mixture (CompositeBeamletSource): beamlet j is 60 % the
     # lattice rectangle j, 40 % the spectral fan j.
     "dij_composite": dict(
@@ -156,12 +177,26 @@ CASES: dict[str, dict] = {
 }
 
 
+# The beam-limiting stack of the collimated cases, in a beam frame at the
+# focal spot (w along +z): a jaw pair closing the +x side beyond u = 0.4 cm
+# at 42.5 cm from the focus, and a three-pair MLC whose middle pair is shut.
+# The analytic cross sections know water only, so the devices are water at
+# 3 g/cc.
+COLLIMATION = dict(
+    focal=(4.0, 4.0, -100.0),
+    jaw=dict(axis="u", z_top=40.0, z_bottom=45.0, edge_neg=-1000.0, edge_pos=0.4, material=0, density=3.0),
+    mlc=dict(z_top=50.0, z_bottom=56.0, leaf_edges_v=(-1.5, -0.5, 0.5, 1.5), tips_neg=(-1.0, 0.1, -1.0),
+             tips_pos=(1.0, 0.1, 1.0), tip_radius=8.0, material=0, density=3.0),
+)
+
+
 def make_source(s: dict, ns):
     """A case's source built from the classes of `ns` (pyRadMC's modules or this
     package): PencilBeamSource, ParallelBeamSource, SpectralBeamSource,
     BeamletGridSource, SpectralBeamletSource, CompositeBeamletSource,
-    TransmissionMaskSource, PhaseSpaceSource and a 6 MV spectrum factory
-    ``spectrum()``."""
+    TransmissionMaskSource, PhaseSpaceSource, a 6 MV spectrum factory
+    ``spectrum()`` and ``collimated(inner, beamlets)``, the inner source seen
+    through the COLLIMATION stack."""
     kind = s["kind"]
     if kind == "parallel":
         return ns.ParallelBeamSource(s["energy"], s["z"], s["x_range"], s["y_range"])
@@ -176,6 +211,8 @@ def make_source(s: dict, ns):
         axes = {k: s[k] for k in ("u_axis", "v_axis") if k in s}
         return ns.SpectralBeamletSource(ns.spectrum(), s["focal_point"], s["centers"], s["width_u"],
                                         s["width_v"], **axes)
+    if kind in ("collimated", "collimated_beamlets"):
+        return ns.collimated(make_source(s["inner"], ns), kind == "collimated_beamlets")
     if kind == "masked":
         import numpy as np
 

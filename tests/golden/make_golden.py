@@ -46,6 +46,7 @@ sys.path.insert(0, str(HERE))
 
 from cases import (  # noqa: E402
     CASES,
+    COLLIMATION,
     CT_CASE,
     layered_density,
     layered_material,
@@ -70,7 +71,46 @@ def _reference_sources():
         CompositeBeamletSource=S.CompositeBeamletSource,
         TransmissionMaskSource=TransmissionMaskSource,
         PhaseSpaceSource=_reference_phsp,
-        spectrum=lambda: ali_rogers_mv("varian-6mv", e_min=0.1))
+        spectrum=lambda: ali_rogers_mv("varian-6mv", e_min=0.1),
+        collimated=_reference_collimated)
+
+
+def _reference_stack():
+    from pyradmc.geometry.collimation import MLC, BeamFrame, BeamLimitingStack, JawPair
+
+    c = COLLIMATION
+    return BeamLimitingStack(frame=BeamFrame(origin=c["focal"]), devices=(JawPair(**c["jaw"]), MLC(**c["mlc"])))
+
+
+def _reference_collimated(inner, beamlets: bool):
+    from pyradmc.data.analytic import AnalyticCrossSections
+    from pyradmc.geometry.collimation import CollimatedBeamletSource, CollimatedSource
+
+    cls = CollimatedBeamletSource if beamlets else CollimatedSource
+    return cls(inner, _reference_stack(), AnalyticCrossSections())
+
+
+def make_collimation() -> None:
+    """tests/golden/collimation.npz: the COLLIMATION stack flattened
+    (BeamLimitingStack.flatten) and the transmission table that pyRadMC's
+    CollimatedSource builds for the 6 MV spectrum (_StackTransmission,
+    geometry/collimation.py:945-969), so the tests need no reference code."""
+    from pyradmc.geometry.source import SpectralBeamSource
+    from pyradmc.geometry.spectrum import ali_rogers_mv
+
+    inner = SpectralBeamSource(ali_rogers_mv("varian-6mv", e_min=0.1), COLLIMATION["focal"], (4.0, 4.0, 0.0),
+                               6.0, 6.0)
+    src = _reference_collimated(inner, False)
+    model = src._model
+    stack = _reference_stack()
+    c = stack.flatten()
+    out = {f"stack_{n}": np.asarray(getattr(c, n)) for n in c.__dataclass_fields__}
+    out["stack_materials"] = np.asarray(stack.materials)
+    out["stack_densities"] = np.asarray(stack.densities)
+    out["log_energy"] = np.asarray(model._log_energies)
+    out["log_total"] = np.asarray(model._log_mu) + np.log(np.asarray(model._densities))[:, None]
+    np.savez_compressed(HERE / "collimation.npz", **out)
+    print("collimation written", flush=True)
 
 
 def _reference_phsp(path):
@@ -395,7 +435,7 @@ if __name__ == "__main__":
         raise SystemExit("usage: python tests/golden/make_golden.py /path/to/pyRadMC [case ...]")
     REFERENCE = sys.argv[1]
     sys.path.insert(0, REFERENCE)
-    names = sys.argv[2:] or ["reduction", "bone_pack", "phsp_file", *CASES, "ct_beamlets"]
+    names = sys.argv[2:] or ["reduction", "bone_pack", "phsp_file", "collimation", *CASES, "ct_beamlets"]
     for name in names:
         if name == "reduction":
             make_reduction()
@@ -403,6 +443,8 @@ if __name__ == "__main__":
             make_bone_pack()
         elif name == "phsp_file":
             make_phsp_file()
+        elif name == "collimation":
+            make_collimation()
         elif name == "ct_beamlets":
             run_ct()
         else:

@@ -20,7 +20,7 @@ import pytest
 
 import pyradmc_b200 as P
 from oracle import stats
-from tests.conftest import SEED, build_case
+from tests.conftest import GOLDEN, SEED, build_case
 
 pytestmark = pytest.mark.gpu
 
@@ -245,3 +245,55 @@ def test_the_native_path_rejects_a_bad_mask(gpu):
                        (TransmissionMaskSource(np.ones((2, 2)), v_axis=(0.6, 0.8, 0.0)), "orthogonal")):
         with pytest.raises(ValueError, match=match):
             engine.run(bad, **kw)
+
+
+def _open_stack():
+    """One jaw pair whose edges stand far outside every beam: zero chords."""
+    from pyradmc_b200.presolve import CompiledHeadStack
+
+    z = np.load(GOLDEN / "collimation.npz")
+    stack = CompiledHeadStack(
+        origin=z["stack_origin"], rotation=z["stack_rotation"], kind=np.array([0]), z_top=np.array([40.0]),
+        z_bottom=np.array([45.0]), jaw_axis=np.array([0]), jaw_edge_neg=np.array([-1000.0]),
+        jaw_edge_pos=np.array([1000.0]), jaw_focused=np.array([0]), mlc_tip_radius=np.zeros(1),
+        mlc_focused_sides=np.zeros(1, dtype=np.int32), mlc_n_pairs=np.zeros(1, dtype=np.int32),
+        mlc_edges_off=np.zeros(1, dtype=np.int32), mlc_tips_off=np.zeros(1, dtype=np.int32),
+        leaf_edges_v=np.zeros(0), tips_neg=np.zeros(0), tips_pos=np.zeros(0), materials=(0,),
+        densities=(3.0,))
+    return stack, z["log_energy"], z["log_total"][:1]
+
+
+def test_an_open_stack_is_bit_inert_and_a_closed_stack_attenuates(gpu):
+    """Collimated sources (CollimatedSource / CollimatedBeamletSource,
+    geometry/collimation.py:1154-1204) weight each in-kernel primary by the
+    stack's transmission.  A stack no ray crosses transmits exactly 1, so the
+    forward run and the Dij are the plain sources' bit for bit; the cases'
+    stack (a jaw and a three-pair MLC of 3 g/cc water) books less emitted
+    energy than the open fan and no more than it.  The collimated dose itself
+    is pinned against pyRadMC's ReferenceEngine in test_gpu_transport.py
+    (``collimated_spectral``, ``dij_collimated``)."""
+    from tests.conftest import collimated
+
+    grid, xs = _water()
+    engine = P.B200Engine(grid, xs)
+    fan = P.SpectralBeamSource(P.ali_rogers_varian_6mv(), (4.0, 4.0, -100.0), (4.0, 4.0, 0.0), 6.0, 6.0)
+    stack, log_e, log_total = _open_stack()
+    kw = dict(n_histories=40_000, n_batches=8, seed=SEED)
+    plain = engine.run(fan, **kw)
+    opened = engine.run(P.CollimatedSource.from_tables(fan, stack, log_e, log_total), **kw)
+    np.testing.assert_array_equal(opened.dose, plain.dose)
+    assert opened.energy_emitted == plain.energy_emitted
+    closed = engine.run(collimated(fan, False), **kw)
+    assert 0.2 * plain.energy_emitted < closed.energy_emitted < 0.95 * plain.energy_emitted
+
+    beams = _fan((4.0, 4.0, -100.0), ((3.0, 3.0, 0.0), (5.0, 3.0, 0.0), (3.0, 5.0, 0.0)), width=2.0)
+    dkw = dict(n_histories_per_beamlet=4000, n_batches=4, seed=SEED, truncation=0.0)
+    a = engine.run_dij(beams, **dkw)
+    b = engine.run_dij(P.CollimatedBeamletSource.from_tables(beams, stack, log_e, log_total), **dkw)
+    np.testing.assert_array_equal(a.indptr, b.indptr)
+    np.testing.assert_array_equal(a.dose, b.dose)
+    np.testing.assert_array_equal(a.sigma, b.sigma)
+    lattice = P.BeamletGridSource(6.0, -1.0, (2.0, 6.0), (2.0, 6.0), 2, 2)
+    c = engine.run_dij(lattice, **dkw)
+    d = engine.run_dij(P.CollimatedBeamletSource.from_tables(lattice, stack, log_e, log_total), **dkw)
+    np.testing.assert_array_equal(c.dose, d.dose)

@@ -70,11 +70,12 @@ def _oracle_case(name, mult, seed_offset=1, n_threads=None):
 
 
 # The C oracle restates the built-in generators on the analytic water source
-# and the voxel scoring grid only; mixtures, phase spaces, the packed
-# multi-material source and cylindrical scoring are pinned on the GPU against
-# the reference fixtures directly.
+# and the voxel scoring grid only; mixtures, phase spaces, collimated sources,
+# the packed multi-material source and cylindrical scoring are pinned on the
+# GPU against the reference fixtures directly.
 ORACLE_CASES = [n for n, c in CASES.items()
-                if c["source"]["kind"] not in ("composite", "phasespace") and "cross_sections" not in c
+                if c["source"]["kind"] not in ("composite", "phasespace", "collimated", "collimated_beamlets")
+                and "cross_sections" not in c
                 and "scoring" not in c]
 
 
