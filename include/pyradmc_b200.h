@@ -161,7 +161,9 @@ typedef struct pmc_source_desc {
     const float* up_dir;    /* [n][3] */
     const float* up_weight;
     int64_t n_records; /* PMC_SRC_PHASESPACE: records in the up_* arrays */
-    /* PMC_SRC_SPECTRAL_MASKED: the mask plane (engine frame, cm; unit axes) */
+    /* PMC_SRC_SPECTRAL_MASKED: the mask plane (engine frame, cm; unit axes).
+     * A non-NULL mask on PMC_SRC_PENCIL, _PARALLEL or _SPECTRAL weights those
+     * primaries the same way (TransmissionMaskSource over any built-in). */
     const double* mask; /* [mask_n_u][mask_n_v] */
     int32_t mask_n_u, mask_n_v;
     double mask_center[3], mask_u_axis[3], mask_v_axis[3];
@@ -235,6 +237,13 @@ typedef struct pmc_beamlet_desc {
      * geometry/collimation.py:1185 */
     const struct pmc_head_stack* stack;
     const struct pmc_head_mu* stack_mu;
+    /* Optional (NULL: none) transmission mask of every in-kernel beamlet
+     * primary, the fields of pmc_source_desc's mask:
+     * TransmissionMaskBeamletSource, geometry/collimation.py:1264 */
+    const double* mask;
+    int32_t mask_n_u, mask_n_v;
+    double mask_center[3], mask_u_axis[3], mask_v_axis[3];
+    double mask_width_u, mask_width_v;
 } pmc_beamlet_desc;
 
 /* Run options: the keyword arguments of WarpEngine.run / run_dij plus the

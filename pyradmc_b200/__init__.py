@@ -22,6 +22,7 @@ from pyradmc_b200.model import (
     SpectralBeamletSource,
     SpectralBeamSource,
     Spectrum,
+    TransmissionMaskBeamletSource,
     TransmissionMaskSource,
     TransportResult,
     VoxelGrid,
@@ -48,6 +49,7 @@ __all__ = [
     "SpectralBeamSource",
     "SpectralBeamletSource",
     "Spectrum",
+    "TransmissionMaskBeamletSource",
     "TransmissionMaskSource",
     "TransportResult",
     "VoxelGrid",

@@ -178,6 +178,14 @@ class BeamletDesc(C.Structure):
         ("sample_user", C.c_void_p),
         ("stack", C.c_void_p),
         ("stack_mu", C.c_void_p),
+        ("mask", _dp),
+        ("mask_n_u", C.c_int32),
+        ("mask_n_v", C.c_int32),
+        ("mask_center", _d3),
+        ("mask_u_axis", _d3),
+        ("mask_v_axis", _d3),
+        ("mask_width_u", C.c_double),
+        ("mask_width_v", C.c_double),
     ]
 
 

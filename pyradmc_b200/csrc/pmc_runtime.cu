@@ -1193,8 +1193,19 @@ static int fill_gen_stack(pmc_engine* e, GenDesc& G, const pmc_head_stack* st, c
 // The transmission mask of a PMC_SRC_SPECTRAL_MASKED source, checked as
 // _MaskTransmission.__init__ does (geometry/collimation.py:1013-1029) and
 // uploaded in float32, the precision of the Warp twin's mask array.
-static int fill_gen_mask(pmc_engine* e, GenDesc& G, const pmc_source_desc* src) {
-    const long long nu = src->mask_n_u, nv = src->mask_n_v;
+struct MaskFields {
+    const double* mask;
+    long long nu, nv;
+    const double *center, *u, *v;
+    double wu, wv;
+};
+#define PMC_MASK_FIELDS(d) \
+    MaskFields { (d)->mask, (d)->mask_n_u, (d)->mask_n_v, (d)->mask_center, (d)->mask_u_axis, \
+                 (d)->mask_v_axis, (d)->mask_width_u, (d)->mask_width_v }
+
+static int fill_gen_mask(pmc_engine* e, GenDesc& G, const MaskFields& f) {
+    const MaskFields* src = &f;
+    const long long nu = src->nu, nv = src->nv;
     if (!src->mask || nu < 1 || nv < 1 || nu * nv > (1ll << 28))
         return fail(e, PMC_ERR_INVALID, "the mask must be a non-empty 2D array, got shape (%lld, %lld)", nu, nv);
     std::vector<float> m((size_t)(nu * nv));
@@ -1204,10 +1215,10 @@ static int fill_gen_mask(pmc_engine* e, GenDesc& G, const pmc_source_desc* src) 
             return fail(e, PMC_ERR_INVALID, "mask values must be finite and within 0..1");
         m[(size_t)i] = (float)v;
     }
-    if (!(src->mask_width_u > 0.0) || !(src->mask_width_v > 0.0))
-        return fail(e, PMC_ERR_INVALID, "widths must be positive, got %g, %g", src->mask_width_u, src->mask_width_v);
-    const double* u = src->mask_u_axis;
-    const double* v = src->mask_v_axis;
+    if (!(src->wu > 0.0) || !(src->wv > 0.0))
+        return fail(e, PMC_ERR_INVALID, "widths must be positive, got %g, %g", src->wu, src->wv);
+    const double* u = src->u;
+    const double* v = src->v;
     const double nuu = std::sqrt(u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
     const double nvv = std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
     if (std::fabs(nuu - 1.0) > 1e-9 || std::fabs(nvv - 1.0) > 1e-9)
@@ -1217,11 +1228,12 @@ static int fill_gen_mask(pmc_engine* e, GenDesc& G, const pmc_source_desc* src) 
     G.masked = 1;
     G.mask_n_u = (int)nu;
     G.mask_n_v = (int)nv;
-    G.mcx = (float)src->mask_center[0]; G.mcy = (float)src->mask_center[1]; G.mcz = (float)src->mask_center[2];
+    G.mcx = (float)src->center[0]; G.mcy = (float)src->center[1]; G.mcz = (float)src->center[2];
     G.mux = (float)u[0]; G.muy = (float)u[1]; G.muz = (float)u[2];
     G.mvx = (float)v[0]; G.mvy = (float)v[1]; G.mvz = (float)v[2];
-    G.mask_wu = (float)src->mask_width_u;
-    G.mask_wv = (float)src->mask_width_v;
+    G.mask_wu = (float)src->wu;
+    G.mask_wv = (float)src->wv;
+    G.book_emitted = 1;  // weighted primaries: the emitted energy is booked one by one
     return upload_f32(e, m, &G.mask);
 }
 
@@ -1283,7 +1295,8 @@ int pmc_run_forward(pmc_engine* e, const pmc_source_desc* src, const pmc_run_par
             if (!rc) rc = upload_f32(e, cy, &G.cy);
             if (!rc) rc = upload_f32(e, cz, &G.cz);
             if (!rc) rc = fill_gen_spectrum(e, G, src->n_bins, src->edges, src->cdf);
-            if (!rc && src->type == PMC_SRC_SPECTRAL_MASKED) rc = fill_gen_mask(e, G, src);
+            if (!rc && src->type == PMC_SRC_SPECTRAL_MASKED) rc = fill_gen_mask(e, G, PMC_MASK_FIELDS(src));
+            if (!rc && src->type == PMC_SRC_SPECTRAL && src->mask) rc = fill_gen_mask(e, G, PMC_MASK_FIELDS(src));
             break;
         }
         case PMC_SRC_PHASESPACE: {
@@ -1341,6 +1354,8 @@ int pmc_run_forward(pmc_engine* e, const pmc_source_desc* src, const pmc_run_par
         default:
             return fail(e, PMC_ERR_INVALID, "unknown source type %d", src->type);
     }
+    if (!rc && src->mask && (src->type == PMC_SRC_PENCIL || src->type == PMC_SRC_PARALLEL))
+        rc = fill_gen_mask(e, G, PMC_MASK_FIELDS(src));
     if (!rc) rc = fill_gen_stack(e, G, src->stack, src->stack_mu);
     if (rc) return rc;
     if (G.kind != PMC_PHOTON && G.kind != PMC_ELECTRON && G.type != 3 && G.type != 5)
@@ -1519,6 +1534,7 @@ int pmc_run_dij(pmc_engine* e, const pmc_beamlet_desc* src, const int64_t* count
             if (!rc) rc = upload_f32(e, spec_edges, &G.edges);
             if (!rc) rc = upload_f32(e, spec_cdf, &G.cdf);
             if (!rc) rc = fill_gen_stack(e, G, src->stack, src->stack_mu);
+            if (!rc && src->mask) rc = fill_gen_mask(e, G, PMC_MASK_FIELDS(src));
         }
         if (rc) return rc;
         PMC_CUDA(e, cudaMemcpyAsync(e->d_gen, &G, sizeof G, cudaMemcpyHostToDevice, e->stream));

@@ -531,10 +531,6 @@ __device__ inline int generate_primary(const TransportParams& P, const GenDesc& 
         const float inv = 1.0f / sqrtf(dx * dx + dy * dy + dz * dz);
         p.x = G.fx; p.y = G.fy; p.z = G.fz;
         p.ux = dx * inv; p.uy = dy * inv; p.uz = dz * inv;
-        if (G.masked) {
-            p.w = mask_transmission(G, p);
-            if (p.w == 0.0f) return -1;  // nothing emitted; the history still counts
-        }
     } else if (G.type == 4) {  // per-beamlet record (CompositeBeamletSource.emit for mixtures)
         const BeamletRec* r = G.recs + (long long)local * G.n_comp;
         if (G.n_comp > 1) {  // one uniform: the first component whose cdf reaches it
@@ -599,8 +595,10 @@ __device__ inline int generate_primary(const TransportParams& P, const GenDesc& 
         p.uy = __ldg(G.up_dir + 3 * ri + 1);
         p.uz = __ldg(G.up_dir + 3 * ri + 2);
     }
-    if (G.stacked && G.type != 3 && G.type != 5) {  // host records carry their own weights
-        p.w *= stack_transmission(G, p);
+    if (G.type != 3 && G.type != 5) {  // host records carry their own weights
+        // a zero weight emits nothing; the history still counts in the batch mean
+        if (G.masked) p.w *= mask_transmission(G, p);
+        if (G.stacked && p.w != 0.0f) p.w *= stack_transmission(G, p);
         if (p.w == 0.0f) return -1;
     }
     if (G.book_emitted) {

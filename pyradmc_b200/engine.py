@@ -364,8 +364,9 @@ def _fill_general_desc(desc, source, records, sl: slice, seed: int, keep: list) 
 
 def _forward_in_kernel(source) -> bool:
     name = _type_name(source)
-    return name in ("PencilBeamSource", "ParallelBeamSource", "SpectralBeamSource") or (
-        name == "TransmissionMaskSource" and _type_name(source.inner) == "SpectralBeamSource")
+    if name in ("PencilBeamSource", "ParallelBeamSource", "SpectralBeamSource"):
+        return True
+    return _collimated_inner(source, _forward_in_kernel) is not None
 
 
 def _attach_stack(desc, source, keep: list):
@@ -385,18 +386,51 @@ def _attach_stack(desc, source, keep: list):
     desc.stack_mu = C.cast(C.pointer(mu), C.c_void_p)
 
 
+_MASKS = ("TransmissionMaskSource", "TransmissionMaskBeamletSource")
+
+
 def _collimated_inner(source, in_kernel):
-    """The inner source of a collimated `source` when `in_kernel(inner)` says
-    the engine generates it on the device, else None."""
+    """The inner source of a collimated or masked `source` when
+    `in_kernel(inner)` says the engine generates it on the device, else None."""
     from .collimation import stack_transmission_tables
 
+    if _type_name(source) in _MASKS:
+        inner = source.inner
+        return inner if in_kernel(inner) else None
     found = stack_transmission_tables(source)
     return found[0] if found is not None and in_kernel(found[0]) else None
 
 
 def _beamlets_in_kernel(source) -> bool:
     name = _type_name(source)
-    return name in ("BeamletGridSource", "SpectralBeamletSource") or _records_plan(source) is not None
+    if name in ("BeamletGridSource", "SpectralBeamletSource") or _records_plan(source) is not None:
+        return True
+    return _collimated_inner(source, _beamlets_in_kernel) is not None
+
+
+def _attach_mask(desc, source, keep: list) -> None:
+    """Point `desc` at the transmission mask of a TransmissionMask(Beamlet)Source
+    (geometry/collimation.py:987-1080, 1205-1284)."""
+    if desc.mask:
+        raise ValueError("one transmission mask per source: nested masks are not supported")
+    mask = np.ascontiguousarray(source.mask, dtype=np.float64)
+    if mask.ndim != 2:
+        raise ValueError(f"the mask must be a non-empty 2D array, got shape {mask.shape}")
+    keep.append(mask)
+    desc.mask = _lib.ptr(mask, C.c_double)
+    desc.mask_n_u, desc.mask_n_v = (int(n) for n in mask.shape)
+    desc.mask_center[:] = [float(c) for c in source.plane_center]
+    desc.mask_u_axis[:] = [float(c) for c in source.u_axis]
+    desc.mask_v_axis[:] = [float(c) for c in source.v_axis]
+    desc.mask_width_u = float(source.width_u)
+    desc.mask_width_v = float(source.width_v)
+
+
+def _attach_weights(desc, source, keep: list) -> None:
+    if _type_name(source) in _MASKS:
+        _attach_mask(desc, source, keep)
+    else:
+        _attach_stack(desc, source, keep)
 
 
 def beamlet_arrays(source):
@@ -423,9 +457,9 @@ def beamlet_descriptor(source, sl: slice, seed: int, keep: list, per=None, recor
     """The ``pmc_beamlet_desc`` of columns `sl` of `source` (the arrays it
     points to are appended to `keep`, which must outlive the call)."""
     inner = _collimated_inner(source, _beamlets_in_kernel)
-    if inner is not None:  # the inner generator, its primaries weighted by the stack
+    if inner is not None:  # the inner generator, its primaries weighted by the stack or mask
         desc = beamlet_descriptor(inner, sl, seed, keep, per, records)
-        _attach_stack(desc, source, keep)
+        _attach_weights(desc, source, keep)
         return desc
     if per is None and records is None:
         per, records = beamlet_arrays(source)
@@ -785,9 +819,10 @@ class B200Engine:
                 f"n_histories={n_histories} not divisible by n_batches={n_batches}; "
                 "unequal batches would weight batch means inconsistently"
             )
-        collimated = source
-        source = _collimated_inner(source, _forward_in_kernel) or source
-        collimated = collimated if source is not collimated else None
+        wrappers = []  # stack and mask wrappers around an in-kernel source, outermost first
+        while (inner := _collimated_inner(source, _forward_in_kernel)) is not None:
+            wrappers.append(source)
+            source = inner
         name = _type_name(source)
         in_kernel = name in ("PencilBeamSource", "ParallelBeamSource")
         if in_kernel and primary_kind not in ("photon", "electron"):
@@ -820,29 +855,12 @@ class B200Engine:
             src.y_lo = float(source.y_range[0])
             src.y_extent = float(source.y_range[1] - source.y_range[0])
             energy_emitted = n_histories * source.max_energy
-        elif name == "SpectralBeamSource" or (
-                name == "TransmissionMaskSource" and _type_name(source.inner) == "SpectralBeamSource"):
-            # a spectral fan, or one seen through a transmission mask (the Warp
-            # engine's generate_spectral_masked_beam): generated in-kernel
-            masked = name == "TransmissionMaskSource"
-            if masked:
-                mask = np.ascontiguousarray(source.mask, dtype=np.float64)
-                if mask.ndim != 2:
-                    raise ValueError(f"the mask must be a non-empty 2D array, got shape {mask.shape}")
-                keep.append(mask)
-                src.mask = _lib.ptr(mask, C.c_double)
-                src.mask_n_u, src.mask_n_v = (int(n) for n in mask.shape)
-                src.mask_center[:] = [float(c) for c in source.plane_center]
-                src.mask_u_axis[:] = [float(c) for c in source.u_axis]
-                src.mask_v_axis[:] = [float(c) for c in source.v_axis]
-                src.mask_width_u = float(source.width_u)
-                src.mask_width_v = float(source.width_v)
-                source = source.inner
+        elif name == "SpectralBeamSource":
             spectrum = source.spectrum
             edges = np.ascontiguousarray(spectrum.edges, dtype=np.float64)
             cdf = np.ascontiguousarray(spectrum.cdf, dtype=np.float64)
             keep += [edges, cdf]
-            src.type = _lib.PMC_SRC_SPECTRAL_MASKED if masked else _lib.PMC_SRC_SPECTRAL
+            src.type = _lib.PMC_SRC_SPECTRAL
             src.kind = _lib.PMC_PHOTON
             src.n_bins = int(cdf.size)
             src.edges = _lib.ptr(edges, C.c_double)
@@ -909,8 +927,9 @@ class B200Engine:
             src.up_weight = _lib.ptr(weight, C.c_float)
         else:
             raise ValueError(f"unsupported source type {name}")
-        if collimated is not None:  # weights from the stack: emitted energy booked per primary
-            _attach_stack(src, collimated, keep)
+        for wrapper in wrappers:  # weights from a stack or a mask (the Warp engine's
+            # generate_spectral_masked_beam for a masked fan): emitted energy booked per primary
+            _attach_weights(src, wrapper, keep)
             energy_emitted = None
 
         params = self._params(

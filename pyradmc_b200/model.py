@@ -58,6 +58,7 @@ __all__ = [
     "SpectralBeamSource",
     "SpectralBeamletSource",
     "Spectrum",
+    "TransmissionMaskBeamletSource",
     "TransmissionMaskSource",
     "TransportResult",
     "VoxelGrid",
@@ -483,8 +484,9 @@ class TransmissionMaskSource:
     (geometry/collimation.py:1205, the model :987-1080): each primary of
     ``inner`` carries the mask value where its full line crosses the plane as
     its weight; ``mask[i, j]`` is pixel i along ``u_axis`` and j along
-    ``v_axis``.  The engine generates it in-kernel when ``inner`` is a
-    SpectralBeamSource, as pyRadMC's Warp engine does."""
+    ``v_axis``.  The engine weights the primaries in-kernel when it generates
+    ``inner`` there (pencil, parallel or spectral fan; pyRadMC's Warp engine
+    does so for the spectral fan)."""
 
     def __init__(self, inner, *, mask, plane_center, width_u, width_v,
                  u_axis=(1.0, 0.0, 0.0), v_axis=(0.0, 1.0, 0.0)) -> None:
@@ -513,6 +515,14 @@ class TransmissionMaskSource:
     width_v = property(lambda self: self._widths[1])
     u_axis = property(lambda self: self._axes[0])
     v_axis = property(lambda self: self._axes[1])
+
+
+class TransmissionMaskBeamletSource(TransmissionMaskSource):
+    """A beamlet source shaped by a 0..1 transmission mask
+    (geometry/collimation.py:1264): every beamlet's primaries are weighted by
+    the mask value where their rays cross its plane."""
+
+    n_beamlets = property(lambda self: self._inner.n_beamlets)
 
 
 def _unit(v, name: str) -> tuple[float, float, float]:

@@ -103,7 +103,8 @@ def build_case(name: str):
 
     ns = SimpleNamespace(**{name: getattr(P, name) for name in (
         "PencilBeamSource", "ParallelBeamSource", "SpectralBeamSource", "BeamletGridSource",
-        "SpectralBeamletSource", "CompositeBeamletSource", "TransmissionMaskSource")},
+        "SpectralBeamletSource", "CompositeBeamletSource", "TransmissionMaskSource",
+        "TransmissionMaskBeamletSource")},
         spectrum=P.ali_rogers_varian_6mv,
         PhaseSpaceSource=PhaseSpaceSource, collimated=collimated)
     src = make_source(case["source"], ns)

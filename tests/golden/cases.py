@@ -162,6 +162,25 @@ CASES: dict[str, dict] = {
                                width_u=2.0, width_v=2.0)),
         run=dict(n_histories_per_beamlet=8000, n_batches=8, seed=SEED, truncation=0.0),
     ),
+    # Four spectral beamlets through a transmission mask
+    # (TransmissionMaskBeamletSource, geometry/collimation.py:1264): the mask
+    # of spectral_masked on a 3 x 3 cm rectangle halfway to the focus.
+    "dij_masked": dict(
+        grid=dict(shape=(16, 16, 16), spacing=(0.5, 0.5, 0.5)),
+        source=dict(kind="masked_beamlets",
+                    inner=dict(kind="spectral_beamlets", focal_point=(4.0, 4.0, -100.0),
+                               centers=((3.0, 3.0, 0.0), (5.0, 3.0, 0.0), (3.0, 5.0, 0.0), (5.0, 5.0, 0.0)),
+                               width_u=2.0, width_v=2.0),
+                    mask=((1.0, 0.9, 0.6, 0.3, 0.0),
+                          (1.0, 1.0, 0.7, 0.2, 0.0),
+                          (0.8, 1.0, 1.0, 0.5, 0.1),
+                          (0.5, 0.7, 1.0, 1.0, 0.4),
+                          (0.2, 0.4, 0.8, 1.0, 1.0),
+                          (0.0, 0.1, 0.5, 0.9, 1.0)),
+                    plane_center=(4.0, 4.0, -50.0), width_u=3.0, width_v=3.0,
+                    u_axis=(0.0, 1.0, 0.0), v_axis=(1.0, 0.0, 0.0)),
+        run=dict(n_histories_per_beamlet=8000, n_batches=8, seed=SEED, truncation=0.0),
+    ),
     # A per-beamlet mixture (CompositeBeamletSource): beamlet j is 60 % the
     # lattice rectangle j, 40 % the spectral fan j.
     "dij_composite": dict(
@@ -194,7 +213,7 @@ def make_source(s: dict, ns):
     """A case's source built from the classes of `ns` (pyRadMC's modules or this
     package): PencilBeamSource, ParallelBeamSource, SpectralBeamSource,
     BeamletGridSource, SpectralBeamletSource, CompositeBeamletSource,
-    TransmissionMaskSource, PhaseSpaceSource, a 6 MV spectrum factory
+    TransmissionMaskSource, TransmissionMaskBeamletSource, PhaseSpaceSource, a 6 MV spectrum factory
     ``spectrum()`` and ``collimated(inner, beamlets)``, the inner source seen
     through the COLLIMATION stack."""
     kind = s["kind"]
@@ -213,10 +232,11 @@ def make_source(s: dict, ns):
                                         s["width_v"], **axes)
     if kind in ("collimated", "collimated_beamlets"):
         return ns.collimated(make_source(s["inner"], ns), kind == "collimated_beamlets")
-    if kind == "masked":
+    if kind in ("masked", "masked_beamlets"):
         import numpy as np
 
-        return ns.TransmissionMaskSource(make_source(s["inner"], ns), mask=np.asarray(s["mask"]),
+        cls = ns.TransmissionMaskSource if kind == "masked" else ns.TransmissionMaskBeamletSource
+        return cls(make_source(s["inner"], ns), mask=np.asarray(s["mask"]),
                                          plane_center=s["plane_center"], width_u=s["width_u"],
                                          width_v=s["width_v"], u_axis=s["u_axis"], v_axis=s["v_axis"])
     if kind == "composite":

@@ -61,7 +61,7 @@ def _reference_sources():
     from types import SimpleNamespace
 
     import pyradmc.geometry.source as S
-    from pyradmc.geometry.collimation import TransmissionMaskSource
+    from pyradmc.geometry.collimation import TransmissionMaskBeamletSource, TransmissionMaskSource
     from pyradmc.geometry.spectrum import ali_rogers_mv
 
     return SimpleNamespace(
@@ -70,6 +70,7 @@ def _reference_sources():
         SpectralBeamletSource=S.SpectralBeamletSource,
         CompositeBeamletSource=S.CompositeBeamletSource,
         TransmissionMaskSource=TransmissionMaskSource,
+        TransmissionMaskBeamletSource=TransmissionMaskBeamletSource,
         PhaseSpaceSource=_reference_phsp,
         spectrum=lambda: ali_rogers_mv("varian-6mv", e_min=0.1),
         collimated=_reference_collimated)

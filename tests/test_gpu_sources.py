@@ -297,3 +297,29 @@ def test_an_open_stack_is_bit_inert_and_a_closed_stack_attenuates(gpu):
     c = engine.run_dij(lattice, **dkw)
     d = engine.run_dij(P.CollimatedBeamletSource.from_tables(lattice, stack, log_e, log_total), **dkw)
     np.testing.assert_array_equal(c.dose, d.dose)
+
+
+def test_open_masks_are_bit_inert_on_every_in_kernel_source(gpu):
+    """A mask of ones whose rectangle holds every ray weights nothing: a masked
+    parallel field and masked beamlets (TransmissionMaskBeamletSource,
+    geometry/collimation.py:1264) are the plain sources' runs bit for bit.  The
+    masked Dij itself is pinned against pyRadMC's ReferenceEngine in
+    test_gpu_transport.py (``dij_masked``)."""
+    grid, xs = _water()
+    engine = P.B200Engine(grid, xs)
+    field = P.ParallelBeamSource(6.0, -1.0, (1.0, 7.0), (1.0, 7.0))
+    kw = dict(n_histories=20_000, n_batches=4, seed=SEED)
+    plain = engine.run(field, **kw)
+    masked = engine.run(P.TransmissionMaskSource(field, mask=np.ones((3, 3)), plane_center=(4.0, 4.0, -50.0),
+                                                 width_u=20.0, width_v=20.0), **kw)
+    np.testing.assert_array_equal(masked.dose, plain.dose)
+    assert masked.energy_emitted == pytest.approx(plain.energy_emitted, rel=1e-12)
+    beams = _fan((4.0, 4.0, -100.0), ((3.0, 3.0, 0.0), (5.0, 3.0, 0.0), (3.0, 5.0, 0.0)), width=2.0)
+    dkw = dict(n_histories_per_beamlet=4000, n_batches=4, seed=SEED, truncation=0.0)
+    a = engine.run_dij(beams, **dkw)
+    b = engine.run_dij(P.TransmissionMaskBeamletSource(beams, mask=np.ones((2, 5)),
+                                                       plane_center=(4.0, 4.0, -50.0), width_u=4.0,
+                                                       width_v=4.0), **dkw)
+    np.testing.assert_array_equal(a.indptr, b.indptr)
+    np.testing.assert_array_equal(a.dose, b.dose)
+    np.testing.assert_array_equal(a.sigma, b.sigma)

@@ -74,7 +74,8 @@ def _oracle_case(name, mult, seed_offset=1, n_threads=None):
 # the packed multi-material source and cylindrical scoring are pinned on the
 # GPU against the reference fixtures directly.
 ORACLE_CASES = [n for n, c in CASES.items()
-                if c["source"]["kind"] not in ("composite", "phasespace", "collimated", "collimated_beamlets")
+                if c["source"]["kind"] not in ("composite", "phasespace", "collimated", "collimated_beamlets",
+                                         "masked_beamlets")
                 and "cross_sections" not in c
                 and "scoring" not in c]
 
