@@ -92,4 +92,5 @@ def stack_transmission_tables(source):
     if model is None or not hasattr(model, "_log_mu"):
         return None
     log_total = np.asarray(model._log_mu) + np.log(np.asarray(model._densities, dtype=np.float64))[:, None]
-    return source.inner, _compiled(model._stack), np.asarray(model._log_energies), log_total
+    inner = getattr(source, "inner", None) or source._inner  # the beamlet wrapper keeps it private
+    return inner, _compiled(model._stack), np.asarray(model._log_energies), log_total

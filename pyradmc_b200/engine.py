@@ -389,14 +389,31 @@ def _attach_stack(desc, source, keep: list):
 _MASKS = ("TransmissionMaskSource", "TransmissionMaskBeamletSource")
 
 
+def _wrapped(source):
+    """The source a weight wrapper wraps (pyRadMC's beamlet wrappers keep it
+    private, geometry/collimation.py:1126-1128)."""
+    return getattr(source, "inner", None) or getattr(source, "_inner", None)
+
+
+def _mask_params(source):
+    """(mask, centre, width_u, width_v, u_axis, v_axis) of a mask wrapper: its
+    properties, or the _MaskTransmission model of pyRadMC's beamlet wrapper
+    (geometry/collimation.py:1024-1029), which exposes none."""
+    if hasattr(source, "mask"):
+        return (source.mask, source.plane_center, source.width_u, source.width_v, source.u_axis,
+                source.v_axis)
+    m = source._model
+    return m._mask, m._center, m._widths[0], m._widths[1], m._u_axis, m._v_axis
+
+
 def _collimated_inner(source, in_kernel):
     """The inner source of a collimated or masked `source` when
     `in_kernel(inner)` says the engine generates it on the device, else None."""
     from .collimation import stack_transmission_tables
 
     if _type_name(source) in _MASKS:
-        inner = source.inner
-        return inner if in_kernel(inner) else None
+        inner = _wrapped(source)
+        return inner if inner is not None and in_kernel(inner) else None
     found = stack_transmission_tables(source)
     return found[0] if found is not None and in_kernel(found[0]) else None
 
@@ -413,17 +430,18 @@ def _attach_mask(desc, source, keep: list) -> None:
     (geometry/collimation.py:987-1080, 1205-1284)."""
     if desc.mask:
         raise ValueError("one transmission mask per source: nested masks are not supported")
-    mask = np.ascontiguousarray(source.mask, dtype=np.float64)
+    values, center, width_u, width_v, u_axis, v_axis = _mask_params(source)
+    mask = np.ascontiguousarray(values, dtype=np.float64)
     if mask.ndim != 2:
         raise ValueError(f"the mask must be a non-empty 2D array, got shape {mask.shape}")
     keep.append(mask)
     desc.mask = _lib.ptr(mask, C.c_double)
     desc.mask_n_u, desc.mask_n_v = (int(n) for n in mask.shape)
-    desc.mask_center[:] = [float(c) for c in source.plane_center]
-    desc.mask_u_axis[:] = [float(c) for c in source.u_axis]
-    desc.mask_v_axis[:] = [float(c) for c in source.v_axis]
-    desc.mask_width_u = float(source.width_u)
-    desc.mask_width_v = float(source.width_v)
+    desc.mask_center[:] = [float(c) for c in center]
+    desc.mask_u_axis[:] = [float(c) for c in u_axis]
+    desc.mask_v_axis[:] = [float(c) for c in v_axis]
+    desc.mask_width_u = float(width_u)
+    desc.mask_width_v = float(width_v)
 
 
 def _attach_weights(desc, source, keep: list) -> None:

@@ -195,3 +195,61 @@ def test_mask_source_mirror_matches_the_reference_class(pyradmc):
             Ref(inner_ref, **kw)
         with pytest.raises(ValueError, match=str(ref_err.value).replace("(", r"\(").replace(")", r"\)")):
             P.TransmissionMaskSource(inner, **kw)
+
+
+def test_collimated_wrappers_read_the_reference_stack_and_table(pyradmc):
+    """pyRadMC's CollimatedSource / CollimatedBeamletSource
+    (geometry/collimation.py:1154-1204) hand the engine the same compiled stack
+    and attenuation rows as this package's wrappers built from the same stack
+    and cross sections: the Dij-compatible collimation route with the
+    reference's own objects."""
+    from pyradmc.data.analytic import AnalyticCrossSections
+    from pyradmc.geometry.collimation import MLC, BeamFrame, BeamLimitingStack, CollimatedBeamletSource, JawPair
+    from pyradmc.geometry.source import SpectralBeamletSource
+    from pyradmc.geometry.spectrum import ali_rogers_mv
+
+    import pyradmc_b200 as P
+    from pyradmc_b200.collimation import stack_transmission_tables
+    from tests.golden.cases import COLLIMATION as c
+
+    stack = BeamLimitingStack(frame=BeamFrame(origin=c["focal"]), devices=(JawPair(**c["jaw"]), MLC(**c["mlc"])))
+    xs = AnalyticCrossSections()
+    inner = SpectralBeamletSource(ali_rogers_mv("varian-6mv", e_min=0.1), c["focal"], ((3.0, 3.0, 0.0),), 2.0, 2.0)
+    ref = stack_transmission_tables(CollimatedBeamletSource(inner, stack, xs))
+    mine = stack_transmission_tables(P.CollimatedBeamletSource(inner, stack, xs))
+    assert ref[0] is inner and mine[0] is inner
+    for name in ("kind", "z_top", "z_bottom", "jaw_edge_pos", "leaf_edges_v", "tips_neg", "tips_pos"):
+        np.testing.assert_array_equal(getattr(ref[1], name), getattr(mine[1], name))
+    assert ref[1].densities == mine[1].densities == (3.0, 3.0)
+    np.testing.assert_array_equal(ref[2], mine[2])
+    np.testing.assert_allclose(mine[3], ref[3], rtol=0, atol=1e-12)
+    with pytest.raises(ValueError, match="e_min < e_max"):
+        P.CollimatedBeamletSource(inner, stack, xs, e_min=10.0)
+
+
+def test_reference_mask_beamlet_source_gives_the_mirror_descriptor(pyradmc):
+    """pyRadMC's TransmissionMaskBeamletSource (geometry/collimation.py:1264)
+    exposes neither its inner source nor its mask; the engine reads them from
+    the wrapper's model and builds the descriptor the mirror class gives."""
+    from pyradmc.geometry.collimation import TransmissionMaskBeamletSource
+    from pyradmc.geometry.source import SpectralBeamletSource
+    from pyradmc.geometry.spectrum import ali_rogers_mv
+
+    import pyradmc_b200 as P
+    from pyradmc_b200.engine import beamlet_descriptor
+
+    spectrum = ali_rogers_mv("varian-6mv", e_min=0.1)
+    kw = dict(mask=np.linspace(0.0, 1.0, 6).reshape(2, 3), plane_center=(4.0, 4.0, -50.0), width_u=3.0,
+              width_v=2.0, u_axis=(0.0, 1.0, 0.0), v_axis=(1.0, 0.0, 0.0))
+    centers = ((3.0, 3.0, 0.0), (5.0, 3.0, 0.0))
+    ref = TransmissionMaskBeamletSource(SpectralBeamletSource(spectrum, (4.0, 4.0, -100.0), centers, 2.0, 2.0),
+                                        **kw)
+    mine = P.TransmissionMaskBeamletSource(
+        P.SpectralBeamletSource(P.ali_rogers_varian_6mv(), (4.0, 4.0, -100.0), centers, 2.0, 2.0), **kw)
+    keep: list = []
+    a, b = beamlet_descriptor(ref, slice(0, 2), 1, keep), beamlet_descriptor(mine, slice(0, 2), 1, keep)
+    assert a.type == b.type and a.mask_n_u == b.mask_n_u == 2 and a.mask_n_v == b.mask_n_v == 3
+    for name in ("mask_center", "mask_u_axis", "mask_v_axis"):
+        assert list(getattr(a, name)) == list(getattr(b, name))
+    assert (a.mask_width_u, a.mask_width_v) == (b.mask_width_u, b.mask_width_v) == (3.0, 2.0)
+    assert [a.mask[i] for i in range(6)] == [b.mask[i] for i in range(6)]
